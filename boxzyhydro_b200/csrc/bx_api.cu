@@ -1,0 +1,677 @@
+// bx_api.cu -- the C ABI of include/boxzy_gpu.h.
+//
+// A handle holds one reference grid in two interchangeable device forms:
+//  * the reference's module arrays (cons, cons_old, u, p, adindx) for the
+//    per-phase kernels, and
+//  * the fused form: conserved planes only (velocity and pressure are
+//    recomputed from them), advanced by two stage kernels per step.
+// A step runs fused when the grid's ghost fill resolves to interior cells
+// within the two consecutive fills the main loop performs and the previous
+// step left u == m/rho and no low-density cell; the stage kernels raise a
+// flag when the velocity limiter or the low-density EOS branch would fire, and
+// the step is then redone from its (untouched) input with the per-phase
+// kernels, which follow the reference's data flow exactly.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "bx_internal.h"
+
+using namespace bx;
+
+namespace bx {
+size_t stage_smem_bytes();
+int stage_blocks_per_sm(int stage, bool pow2, bool threed);
+}  // namespace bx
+
+struct bx_handle {
+  bx_params P{};
+  Geom g{};
+  GhostTable T;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  double* buf[3] = {nullptr, nullptr, nullptr};
+  int cur = 0;
+  int nsrc = 1;
+  PhaseArrays pa{};
+  int nghost = 0;
+  int32_t *d_dst = nullptr, *d_src1 = nullptr, *d_src2 = nullptr;
+  uint8_t *d_sgn1 = nullptr, *d_sgn2 = nullptr;
+  Geom* d_geom = nullptr;
+  Tile* d_tiles = nullptr;
+  int ntiles = 0;
+  Ctrl* d_ctrl = nullptr;
+  Ctrl* h_ctrl = nullptr;  // pinned mirror
+  Ctrl clock{};            // host copy of the clock after the last completed call
+  int mode = 0;            // 0 = reference arrays current, 1 = fused planes current
+  bool eligible = false;
+  bool gforce_set = false;
+  uint32_t status = 0;
+  int last_path = 0;
+  // profiling: CUDA events around the stage launches, accumulated per step
+  bool prof = false;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  double ms_stage[2] = {0.0, 0.0};
+  long long n_stage = 0;
+  long long launches = 0;  // kernels of this library launched on the handle's stream
+  std::string err;
+};
+
+static std::string g_create_err;
+
+#define CK(expr)                                                                  \
+  do {                                                                            \
+    cudaError_t e_ = (expr);                                                      \
+    if (e_ != cudaSuccess) {                                                      \
+      h->err = std::string(#expr) + ": " + cudaGetErrorString(e_);                \
+      return BX_ERR_CUDA;                                                         \
+    }                                                                             \
+  } while (0)
+
+#define CHECK_H()                    \
+  do {                               \
+    if (!h) return BX_ERR_ARG;       \
+  } while (0)
+
+static int set_err(bx_handle* h, int code, const std::string& m) {
+  if (h) h->err = m;
+  else g_create_err = m;
+  return code;
+}
+
+static cudaError_t dalloc(void** p, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  return cudaMalloc(p, bytes);
+}
+
+// ---- tiles: 32x8 column tiles times z chunks sized so the launch fills the GPU
+static std::vector<Tile> make_tiles(const Geom& g, int box, int slots) {
+  const int NAx = g.ax1 - g.ax0, NAy = g.ay1 - g.ay0, NAz = g.az1 - g.az0;
+  const int tx = (NAx + TX - 1) / TX, ty = (NAy + TY - 1) / TY;
+  const long long cols = (long long)tx * ty;
+  int best = NAz;
+  double best_cost = 1e300;
+  for (int zc = 1; zc <= NAz; ++zc) {
+    const long long chunks = (NAz + zc - 1) / zc;
+    const long long blocks = cols * chunks;
+    const long long waves = (blocks + slots - 1) / slots;
+    const double per = g.threed ? zc + 1.0 : (double)zc;
+    const double cost = waves * per;
+    if (cost < best_cost - 1e-9) {
+      best_cost = cost;
+      best = zc;
+    }
+  }
+  std::vector<Tile> tiles;
+  for (int z = 0; z < NAz; z += best)
+    for (int y = 0; y < ty; ++y)
+      for (int x = 0; x < tx; ++x) tiles.push_back(Tile{box, x * TX, y * TY, z, std::min(NAz, z + best)});
+  return tiles;
+}
+
+extern "C" {
+
+const char* bx_version(void) { return "boxzy-b200 1.0 (sm_100a, FP64)"; }
+
+const char* bx_last_error(bx_handle* h) {
+  if (!h) return g_create_err.c_str();
+  return h->err.c_str();
+}
+
+int bx_create(const bx_params* params, bx_handle** out) {
+  if (!params || !out) return set_err(nullptr, BX_ERR_ARG, "null argument");
+  const bx_params& P = *params;
+  if (P.h2stat != -1)
+    return set_err(nullptr, BX_ERR_UNSUPPORTED, "only H2STAT=-1 (fixed gamma) is supported");
+  if (P.fluxangmom)
+    return set_err(nullptr, BX_ERR_UNSUPPORTED, "fluxangmom=.true. is not supported");
+  if (P.nx < 5 || P.ny < 5 || P.nz < 1 || (P.nz >= 6 && P.nz < 5))
+    return set_err(nullptr, BX_ERR_ARG, "grid too small: need nx,ny>=5");
+  if ((long long)P.nx * P.ny * P.nz >= (1ll << 31))
+    return set_err(nullptr, BX_ERR_ARG, "grid exceeds 2^31 cells");
+  if (!(P.dx > 0 && P.dy > 0 && P.dz > 0 && P.gammafix > 1.0 && P.cfl > 0))
+    return set_err(nullptr, BX_ERR_ARG, "dx,dy,dz,cfl must be >0 and gammafix>1");
+  bx_handle* h = new bx_handle();
+  h->P = P;
+  fill_geom(P, h->g);
+  build_ghost_tables(P, h->T);
+  h->eligible = h->T.resolved2 && h->T.face_rule_ok && !(P.flags & BX_FLAG_PHASE_ONLY);
+  const long long ng = h->g.ng;
+  h->nghost = (int)h->T.dst.size();
+  auto fail = [&](int code) {
+    g_create_err = h->err;
+    bx_destroy(h);
+    return code;
+  };
+#define CKC(expr)                                                               \
+  do {                                                                          \
+    cudaError_t e_ = (expr);                                                    \
+    if (e_ != cudaSuccess) {                                                    \
+      h->err = std::string(#expr) + ": " + cudaGetErrorString(e_);              \
+      return fail(e_ == cudaErrorMemoryAllocation ? BX_ERR_NOMEM : BX_ERR_CUDA); \
+    }                                                                           \
+  } while (0)
+  CKC(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+  h->own_stream = true;
+  for (int k = 0; k < 3; ++k) CKC(dalloc((void**)&h->buf[k], 5 * ng * sizeof(double)));
+  CKC(dalloc((void**)&h->pa.cons, 5 * ng * sizeof(double)));
+  CKC(dalloc((void**)&h->pa.cons_old, 5 * ng * sizeof(double)));
+  CKC(dalloc((void**)&h->pa.u, 3 * ng * sizeof(double)));
+  CKC(dalloc((void**)&h->pa.p, ng * sizeof(double)));
+  CKC(dalloc((void**)&h->pa.adindx, ng * sizeof(double)));
+  CKC(dalloc((void**)&h->pa.gtmp, 5 * (size_t)h->nghost * sizeof(double)));
+  CKC(cudaMemset(h->pa.cons, 0, 5 * ng * sizeof(double)));
+  CKC(cudaMemset(h->pa.u, 0, 3 * ng * sizeof(double)));
+  CKC(cudaMemset(h->pa.p, 0, ng * sizeof(double)));
+  const int n = h->nghost;
+  CKC(dalloc((void**)&h->d_dst, n * sizeof(int32_t)));
+  CKC(dalloc((void**)&h->d_src1, n * sizeof(int32_t)));
+  CKC(dalloc((void**)&h->d_src2, n * sizeof(int32_t)));
+  CKC(dalloc((void**)&h->d_sgn1, n));
+  CKC(dalloc((void**)&h->d_sgn2, n));
+  if (n) {
+    CKC(cudaMemcpy(h->d_dst, h->T.dst.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(h->d_src1, h->T.src1.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(h->d_src2, h->T.src2.data(), n * sizeof(int32_t), cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(h->d_sgn1, h->T.sgn1.data(), n, cudaMemcpyHostToDevice));
+    CKC(cudaMemcpy(h->d_sgn2, h->T.sgn2.data(), n, cudaMemcpyHostToDevice));
+  }
+  CKC(dalloc((void**)&h->d_geom, sizeof(Geom)));
+  CKC(cudaMemcpy(h->d_geom, &h->g, sizeof(Geom), cudaMemcpyHostToDevice));
+  int dev = 0, sms = 148;
+  CKC(cudaGetDevice(&dev));
+  CKC(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const int per_sm = std::max(1, stage_blocks_per_sm(1, h->g.pow2, h->g.threed));
+  std::vector<Tile> tiles = make_tiles(h->g, 0, sms * per_sm);
+  h->ntiles = (int)tiles.size();
+  CKC(dalloc((void**)&h->d_tiles, tiles.size() * sizeof(Tile)));
+  CKC(cudaMemcpy(h->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+  CKC(dalloc((void**)&h->d_ctrl, sizeof(Ctrl)));
+  CKC(cudaMallocHost((void**)&h->h_ctrl, sizeof(Ctrl)));
+  std::memset(&h->clock, 0, sizeof(Ctrl));
+  h->clock.cfl = P.cfl;
+  h->clock.endtime = 0.0;
+  h->clock.max_step = (1ll << 62);
+  CKC(cudaMemcpy(h->d_ctrl, &h->clock, sizeof(Ctrl), cudaMemcpyHostToDevice));
+#undef CKC
+  *out = h;
+  return BX_OK;
+}
+
+int bx_destroy(bx_handle* h) {
+  if (!h) return BX_OK;
+  if (h->stream) cudaStreamSynchronize(h->stream);
+  for (int k = 0; k < 3; ++k) cudaFree(h->buf[k]);
+  cudaFree(h->pa.cons);
+  cudaFree(h->pa.cons_old);
+  cudaFree(h->pa.u);
+  cudaFree(h->pa.p);
+  cudaFree(h->pa.adindx);
+  cudaFree(h->pa.gforce);
+  cudaFree(h->pa.states);
+  cudaFree(h->pa.gtmp);
+  cudaFree(h->d_dst);
+  cudaFree(h->d_src1);
+  cudaFree(h->d_src2);
+  cudaFree(h->d_sgn1);
+  cudaFree(h->d_sgn2);
+  cudaFree(h->d_geom);
+  cudaFree(h->d_tiles);
+  cudaFree(h->d_ctrl);
+  if (h->h_ctrl) cudaFreeHost(h->h_ctrl);
+  for (int k = 0; k < 3; ++k)
+    if (h->ev[k]) cudaEventDestroy(h->ev[k]);
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  delete h;
+  return BX_OK;
+}
+
+int bx_set_stream(bx_handle* h, void* s) {
+  CHECK_H();
+  CK(cudaStreamSynchronize(h->stream));
+  if (h->own_stream && h->stream) cudaStreamDestroy(h->stream);
+  if (s) {
+    h->stream = (cudaStream_t)s;
+    h->own_stream = false;
+  } else {
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    h->own_stream = true;
+  }
+  return BX_OK;
+}
+
+// device -> host clock mirror (synchronises the stream)
+static int pull_clock(bx_handle* h) {
+  CK(cudaMemcpyAsync(h->h_ctrl, h->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->clock = *h->h_ctrl;
+  return BX_OK;
+}
+static int push_clock(bx_handle* h) {
+  *h->h_ctrl = h->clock;
+  CK(cudaMemcpyAsync(h->d_ctrl, h->h_ctrl, sizeof(Ctrl), cudaMemcpyHostToDevice, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return BX_OK;
+}
+
+static int ensure_states(bx_handle* h) {
+  if (!h->pa.states) CK(dalloc((void**)&h->pa.states, 42 * h->g.ng * sizeof(double)));
+  return BX_OK;
+}
+
+static int bx_adindx_fill(bx_handle* h) {
+  // adindx(:) = gammafix, as state() sets it (state.f90:50)
+  std::vector<double> gam(h->g.ng, h->P.gammafix);
+  CK(cudaMemcpyAsync(h->pa.adindx, gam.data(), h->g.ng * sizeof(double), cudaMemcpyHostToDevice,
+                     h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return BX_OK;
+}
+
+// make the reference arrays current (from the fused planes if needed)
+static int to_phase(bx_handle* h) {
+  if (h->mode == 0) return BX_OK;
+  CK(fused_to_phase(h->g, h->buf[h->cur], h->nsrc, h->pa, h->nghost, h->d_dst, h->d_src2,
+                    h->d_sgn2, h->stream));
+  h->mode = 0;
+  return BX_OK;
+}
+
+// staging buffer for the AoS<->SoA transposes: a fused plane set that does not
+// hold the current state
+static double* staging(bx_handle* h) { return h->buf[(h->cur + 1) % 3]; }
+
+static int enter_fused(bx_handle* h);
+
+int bx_upload(bx_handle* h, const double* cons, const double* u, const double* p) {
+  CHECK_H();
+  if (!cons) return set_err(h, BX_ERR_ARG, "cons is required");
+  const long long n = h->g.ng;
+  double* tmp = staging(h);
+  cudaStream_t s = h->stream;
+  CK(cudaMemcpyAsync(tmp, cons, 5 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(aos_to_soa(tmp, h->pa.cons, n, 5, s));
+  if (u) {
+    CK(cudaMemcpyAsync(tmp, u, 3 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+    CK(aos_to_soa(tmp, h->pa.u, n, 3, s));
+  } else {
+    CK(cudaMemsetAsync(h->pa.u, 0, 3 * n * sizeof(double), s));
+  }
+  if (p) CK(cudaMemcpyAsync(h->pa.p, p, n * sizeof(double), cudaMemcpyHostToDevice, s));
+  else CK(cudaMemsetAsync(h->pa.p, 0, n * sizeof(double), s));
+  h->launches += 2;
+  h->mode = 0;
+  // a state the fused stages reproduce exactly (as left by a previous step)
+  // continues on them; anything else starts on the per-phase kernels
+  if (h->eligible && !h->gforce_set) {
+    if (int r = pull_clock(h)) return r;
+    h->clock.flags = 0;
+    if (int r = push_clock(h)) return r;
+    CK(check_clean(h->g, h->pa, h->nghost, h->d_dst, h->d_src2, h->d_sgn2, h->d_ctrl, s));
+    h->launches += 2;
+    if (int r = pull_clock(h)) return r;
+    const bool clean = !(h->clock.flags & kFlagNotClean);
+    h->clock.flags = 0;
+    if (int r = push_clock(h)) return r;
+    if (clean) {
+      // adindx = gammafix is what state() leaves; set it like the other path does
+      return enter_fused(h);
+    }
+  }
+  return bx_adindx_fill(h);
+}
+
+int bx_download(bx_handle* h, double* cons, double* u, double* p) {
+  CHECK_H();
+  const long long n = h->g.ng;
+  cudaStream_t s = h->stream;
+  if (h->mode == 1) {
+    CK(fused_to_phase(h->g, h->buf[h->cur], h->nsrc, h->pa, h->nghost, h->d_dst, h->d_src2,
+                      h->d_sgn2, s));
+    h->launches += 3;
+  }
+  double* tmp = staging(h);
+  if (cons) {
+    CK(soa_to_aos(h->pa.cons, tmp, n, 5, s));
+    CK(cudaMemcpyAsync(cons, tmp, 5 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    h->launches += 1;
+  }
+  if (u) {
+    // the transpose of u must not overwrite cons before its copy is done: the
+    // stream orders them
+    CK(soa_to_aos(h->pa.u, tmp + 5 * n - 3 * n, n, 3, s));
+    CK(cudaMemcpyAsync(u, tmp + 5 * n - 3 * n, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, s));
+    h->launches += 1;
+  }
+  if (p) CK(cudaMemcpyAsync(p, h->pa.p, n * sizeof(double), cudaMemcpyDeviceToHost, s));
+  CK(cudaStreamSynchronize(s));
+  return BX_OK;
+}
+
+int bx_set_clock(bx_handle* h, double time, double dtold, int64_t step) {
+  CHECK_H();
+  if (int r = pull_clock(h)) return r;
+  h->clock.time = time;
+  h->clock.dtold = dtold;
+  h->clock.step = step;
+  return push_clock(h);
+}
+
+int bx_get_clock(bx_handle* h, double* time, double* dt, double* dtold, int64_t* step) {
+  CHECK_H();
+  if (int r = pull_clock(h)) return r;
+  if (time) *time = h->clock.time;
+  if (dt) *dt = h->clock.dt;
+  if (dtold) *dtold = h->clock.dtold;
+  if (step) *step = h->clock.step;
+  return BX_OK;
+}
+
+int bx_set_dt(bx_handle* h, double dt) {
+  CHECK_H();
+  if (int r = pull_clock(h)) return r;
+  h->clock.dt = dt;
+  return push_clock(h);
+}
+
+// ---- per-phase entry points
+int bx_state(bx_handle* h) {
+  CHECK_H();
+  if (int r = to_phase(h)) return r;
+  CK(phase_state(h->g, h->pa, h->d_ctrl, h->stream));
+  return pull_clock(h);
+}
+int bx_velocity(bx_handle* h) {
+  CHECK_H();
+  if (int r = to_phase(h)) return r;
+  CK(phase_velocity(h->g, h->pa, h->d_ctrl, h->stream));
+  return pull_clock(h);
+}
+int bx_courant(bx_handle* h, double* dt) {
+  CHECK_H();
+  if (int r = to_phase(h)) return r;
+  CK(cudaMemsetAsync(&h->d_ctrl->rate_bits, 0, sizeof(unsigned long long), h->stream));
+  CK(phase_courant(h->g, h->pa, h->d_ctrl, h->stream));
+  CK(phase_courant_finish(h->d_ctrl, h->stream));
+  if (int r = pull_clock(h)) return r;
+  if (dt) *dt = h->clock.dt;
+  return BX_OK;
+}
+int bx_ghost(bx_handle* h) {
+  CHECK_H();
+  if (int r = to_phase(h)) return r;
+  CK(phase_ghost(h->nghost, h->d_dst, h->d_src1, h->d_sgn1, h->pa, h->g.ng, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return BX_OK;
+}
+int bx_source(bx_handle* h, int32_t siter) {
+  CHECK_H();
+  (void)siter;
+  if (int r = to_phase(h)) return r;
+  CK(phase_source(h->g, h->pa, h->d_ctrl, 1.0, h->stream));
+  CK(phase_ghost(h->nghost, h->d_dst, h->d_src1, h->d_sgn1, h->pa, h->g.ng, h->stream));
+  return pull_clock(h);
+}
+int bx_flux(bx_handle* h, int32_t avg) {
+  CHECK_H();
+  if (avg != 0 && avg != 1) return set_err(h, BX_ERR_ARG, "avg must be 0 or 1");
+  if (int r = to_phase(h)) return r;
+  if (int r = ensure_states(h)) return r;
+  CK(phase_flux(h->g, h->pa, h->d_ctrl, avg, h->stream));
+  CK(phase_ghost(h->nghost, h->d_dst, h->d_src1, h->d_sgn1, h->pa, h->g.ng, h->stream));
+  return pull_clock(h);
+}
+int bx_avisc(bx_handle* h) {
+  CHECK_H();
+  return BX_OK;
+}
+int bx_save_cons_old(bx_handle* h) {
+  CHECK_H();
+  if (int r = to_phase(h)) return r;
+  CK(phase_copy_old(h->g, h->pa, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  return BX_OK;
+}
+
+int bx_set_gforce(bx_handle* h, const double* gforce) {
+  CHECK_H();
+  const long long n = h->g.ng;
+  if (!gforce) {
+    h->gforce_set = false;
+    cudaFree(h->pa.gforce);
+    h->pa.gforce = nullptr;
+    return BX_OK;
+  }
+  if (!h->pa.gforce) CK(dalloc((void**)&h->pa.gforce, 3 * n * sizeof(double)));
+  if (int r = to_phase(h)) return r;
+  double* tmp = staging(h);
+  CK(cudaMemcpyAsync(tmp, gforce, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(aos_to_soa(tmp, h->pa.gforce, n, 3, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->gforce_set = true;
+  return BX_OK;
+}
+
+int bx_status(bx_handle* h, uint32_t* bits, int32_t* last_path) {
+  CHECK_H();
+  if (bits) *bits = h->status;
+  if (last_path) *last_path = h->last_path;
+  h->status = 0;
+  return BX_OK;
+}
+
+int bx_device_cons(bx_handle* h, double** cons_soa, int64_t* ngrid) {
+  CHECK_H();
+  if (h->mode == 1)
+    CK(fused_to_phase(h->g, h->buf[h->cur], h->nsrc, h->pa, h->nghost, h->d_dst, h->d_src2,
+                      h->d_sgn2, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  if (cons_soa) *cons_soa = h->pa.cons;
+  if (ngrid) *ngrid = h->g.ng;
+  return BX_OK;
+}
+
+// ---- whole steps
+static int ghost1(bx_handle* h) {
+  CK(phase_ghost(h->nghost, h->d_dst, h->d_src1, h->d_sgn1, h->pa, h->g.ng, h->stream));
+  return BX_OK;
+}
+
+// main.f90:212-545 with the per-phase kernels (reference data flow)
+static int phase_step(bx_handle* h) {
+  if (int r = ensure_states(h)) return r;
+  Geom& g = h->g;
+  PhaseArrays& a = h->pa;
+  cudaStream_t s = h->stream;
+  Ctrl* c = h->d_ctrl;
+  CK(phase_state(g, a, c, s));
+  CK(cudaMemsetAsync(&c->rate_bits, 0, sizeof(unsigned long long), s));
+  CK(phase_courant(g, a, c, s));
+  CK(launch_dt(c, 1, s));
+  CK(phase_source(g, a, c, 0.5, s));   // source(time,0) with dt/2
+  if (int r = ghost1(h)) return r;
+  if (int r = ghost1(h)) return r;     // main.f90:312
+  CK(phase_state(g, a, c, s));
+  CK(phase_velocity(g, a, c, s));
+  CK(phase_copy_old(g, a, s));
+  CK(phase_flux(g, a, c, 0, s));
+  if (int r = ghost1(h)) return r;     // flux.f90:231
+  if (int r = ghost1(h)) return r;     // main.f90:351
+  CK(phase_state(g, a, c, s));
+  CK(phase_velocity(g, a, c, s));
+  CK(phase_flux(g, a, c, 1, s));
+  if (int r = ghost1(h)) return r;
+  if (int r = ghost1(h)) return r;     // main.f90:374
+  CK(phase_state(g, a, c, s));
+  CK(phase_velocity(g, a, c, s));
+  CK(phase_source(g, a, c, 0.5, s));   // source(time+dt,1) with dt/2
+  if (int r = ghost1(h)) return r;
+  if (int r = ghost1(h)) return r;     // main.f90:511
+  CK(phase_state(g, a, c, s));
+  CK(phase_velocity(g, a, c, s));
+  CK(launch_end(c, 1, s));
+  h->launches += 46;
+  return BX_OK;
+}
+
+static int fused_launch(bx_handle* h) {
+  const int X = h->cur, Y = (h->cur + 1) % 3, Z = (h->cur + 2) % 3;
+  StageArgs a{};
+  a.ctrl = h->d_ctrl;
+  a.geom = h->d_geom;
+  a.tiles = h->d_tiles;
+  a.ncells_total = h->g.ng;
+  a.nsrc = h->nsrc;
+  const bool p2 = h->g.pow2 != 0, t3 = h->g.threed != 0;
+  CK(launch_dt(h->d_ctrl, 1, h->stream));
+  a.X = h->buf[X];
+  a.Y = nullptr;
+  a.out = h->buf[Y];
+  if (h->prof) CK(cudaEventRecord(h->ev[0], h->stream));
+  CK(launch_stage(0, p2, t3, a, h->ntiles, h->stream));
+  if (h->prof) CK(cudaEventRecord(h->ev[1], h->stream));
+  a.Y = h->buf[Y];
+  a.out = h->buf[Z];
+  CK(launch_stage(1, p2, t3, a, h->ntiles, h->stream));
+  if (h->prof) CK(cudaEventRecord(h->ev[2], h->stream));
+  CK(launch_end(h->d_ctrl, 1, h->stream));
+  h->launches += 4;
+  return BX_OK;
+}
+
+// switch to the fused form after a clean per-phase step: the planes take the
+// reference cons (sources of this step already applied: nsrc=1) and the Courant
+// rate of the next step's state()/courant() is accumulated now.
+static int enter_fused(bx_handle* h) {
+  if (int r = bx_adindx_fill(h)) return r;
+  CK(cudaMemcpyAsync(h->buf[h->cur], h->pa.cons, 5 * h->g.ng * sizeof(double),
+                     cudaMemcpyDeviceToDevice, h->stream));
+  CK(phase_state(h->g, h->pa, h->d_ctrl, h->stream));
+  CK(cudaMemsetAsync(&h->d_ctrl->rate_bits, 0, sizeof(unsigned long long), h->stream));
+  CK(phase_courant(h->g, h->pa, h->d_ctrl, h->stream));
+  h->launches += 2;
+  h->nsrc = 1;
+  h->mode = 1;
+  return pull_clock(h);
+}
+
+int bx_step(bx_handle* h, double endtime, int32_t* ran) {
+  CHECK_H();
+  if (ran) *ran = 0;
+  if (h->gforce_set && h->mode == 1) {
+    if (int r = to_phase(h)) return r;
+  }
+  if (!(h->clock.time < endtime) || h->clock.step >= 1000000) return BX_OK;
+  if (h->clock.endtime != endtime) {
+    h->clock.endtime = endtime;
+    if (int r = push_clock(h)) return r;
+  }
+  const Ctrl before = h->clock;
+  if (h->mode == 1) {
+    if (int r = fused_launch(h)) return r;
+    if (int r = pull_clock(h)) return r;
+    const unsigned f = h->clock.flags;
+    if (f & kFlagNonFinite) {
+      h->status |= f;
+      return set_err(h, BX_ERR_STATE, "non-finite state produced by the step");
+    }
+    if (h->prof) {
+      float t0 = 0.f, t1 = 0.f;
+      CK(cudaEventElapsedTime(&t0, h->ev[0], h->ev[1]));
+      CK(cudaEventElapsedTime(&t1, h->ev[1], h->ev[2]));
+      h->ms_stage[0] += t0;
+      h->ms_stage[1] += t1;
+      h->n_stage += 1;
+    }
+    if (!(f & (kFlagVlimit | kFlagLowRho))) {
+      h->cur = (h->cur + 2) % 3;
+      h->nsrc = 2;
+      h->clock.flags = 0;
+      if (int r = push_clock(h)) return r;
+      h->last_path = 1;
+      if (ran) *ran = 1;
+      return BX_OK;
+    }
+    // the limiter or the low-density branch fires in this step: redo it from
+    // its untouched input with the reference data flow
+    h->status |= f & (kFlagVlimit | kFlagLowRho);
+    h->clock = before;
+    h->clock.rate_bits = 0;
+    if (int r = push_clock(h)) return r;
+    if (int r = to_phase(h)) return r;
+  }
+  if (int r = phase_step(h)) return r;
+  if (int r = pull_clock(h)) return r;
+  const unsigned f = h->clock.flags;
+  h->status |= f;
+  h->last_path = 0;
+  if (ran) *ran = 1;
+  h->clock.flags = 0;
+  if (int r = push_clock(h)) return r;
+  if (f & kFlagNonFinite) return set_err(h, BX_ERR_STATE, "non-finite state produced by the step");
+  if (h->eligible && !h->gforce_set && !(f & (kFlagVlimit | kFlagLowRho)))
+    return enter_fused(h);
+  return BX_OK;
+}
+
+int bx_profile(bx_handle* h, int32_t enable) {
+  CHECK_H();
+  if (enable && !h->ev[0])
+    for (int k = 0; k < 3; ++k) CK(cudaEventCreate(&h->ev[k]));
+  h->prof = enable != 0;
+  h->ms_stage[0] = h->ms_stage[1] = 0.0;
+  h->n_stage = 0;
+  h->launches = 0;
+  return BX_OK;
+}
+
+int bx_profile_read(bx_handle* h, double* ms_stage0, double* ms_stage1, int64_t* fused_steps,
+                    int64_t* launches) {
+  CHECK_H();
+  if (ms_stage0) *ms_stage0 = h->ms_stage[0];
+  if (ms_stage1) *ms_stage1 = h->ms_stage[1];
+  if (fused_steps) *fused_steps = h->n_stage;
+  if (launches) *launches = h->launches;
+  return BX_OK;
+}
+
+int bx_ghost_plan(const bx_params* params, int64_t* nghost, int32_t* dst, int32_t* src1,
+                  uint8_t* sgn1, int32_t* src2, uint8_t* sgn2, int32_t* fused_ok) {
+  if (!params || !nghost) return set_err(nullptr, BX_ERR_ARG, "null argument");
+  const bx_params& P = *params;
+  if (P.nx < 5 || P.ny < 5 || P.nz < 1) return set_err(nullptr, BX_ERR_ARG, "grid too small");
+  GhostTable T;
+  build_ghost_tables(P, T);
+  const size_t n = T.dst.size();
+  if (dst) {
+    if ((size_t)*nghost < n) return set_err(nullptr, BX_ERR_ARG, "output arrays too small");
+    std::memcpy(dst, T.dst.data(), n * sizeof(int32_t));
+    if (src1) std::memcpy(src1, T.src1.data(), n * sizeof(int32_t));
+    if (sgn1) std::memcpy(sgn1, T.sgn1.data(), n);
+    if (src2) std::memcpy(src2, T.src2.data(), n * sizeof(int32_t));
+    if (sgn2) std::memcpy(sgn2, T.sgn2.data(), n);
+  }
+  *nghost = (int64_t)n;
+  if (fused_ok)
+    *fused_ok = (T.resolved2 && T.face_rule_ok && !(P.flags & BX_FLAG_PHASE_ONLY)) ? 1 : 0;
+  return BX_OK;
+}
+
+int bx_run(bx_handle* h, double endtime, int64_t nsteps, int64_t* steps_taken) {
+  CHECK_H();
+  int64_t n = 0;
+  int rc = BX_OK;
+  while (n < nsteps) {
+    int32_t ran = 0;
+    rc = bx_step(h, endtime, &ran);
+    if (rc != BX_OK || !ran) break;
+    ++n;
+  }
+  if (steps_taken) *steps_taken = n;
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,139 @@
+// bx_internal.h -- device data layout and launch interfaces of the hydro step.
+//
+// HBM layout: every grid is held as five SoA planes of FP64 (rho, m1, m2, m3, E),
+// each ng = nx*ny*nz doubles in the reference's cell order (x fastest), so a
+// warp touching 32 consecutive x cells moves 256 contiguous bytes per field.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/boxzy_gpu.h"
+
+namespace bx {
+
+// status bits raised on the device (BX_STATUS_* mirror these in the C header)
+enum : unsigned {
+  kFlagVlimit = 1u << 0,   // |u_i| > vlimit somewhere: velocity limiter rewrites cons
+  kFlagLowRho = 1u << 1,   // rho < 1e-4 somewhere: low-density EOS branch
+  kFlagNonFinite = 1u << 2,
+  kFlagZeroWave = 1u << 3, // ap+am == 0 in an HLL face (reference divides by zero)
+  kFlagNotClean = 1u << 4, // uploaded arrays are not a state the fused stages can start from
+};
+
+// main.f90 clock held on the device (time, dt, dtold, step) plus the Courant
+// accumulator and guard flags of the step in flight.
+struct Ctrl {
+  double time;
+  double dt;          // full step dt (main.f90:342)
+  double dtold;       // main.f90:270-271
+  double endtime;
+  double rate;        // last reduced dtrate (courant.f90:175)
+  unsigned long long rate_bits;  // atomicMax accumulator (bit image of a double >= 0)
+  long long step;
+  long long max_step;
+  unsigned int flags;
+  int active;         // 1 while the step in flight is to be taken
+  double cfl;
+  double pad[2];
+};
+
+// Geometry and constants of one box (one reference grid).
+struct Geom {
+  int nx, ny, nz;          // with ghosts
+  int ax0, ax1, ay0, ay1, az0, az1;  // interior [a0,a1) per axis (0-based)
+  long long sy, sz;        // strides (1, nx, nx*ny)
+  long long ng;            // cells
+  long long base;          // offset of this box's cells in the pooled buffers
+  int wall[6];             // reflective wall flags xl,xr,yl,yr,zl,zr (after nz<6 rule)
+  int threed;              // nz >= 6
+  int pow2;                // dx,dy,dz all powers of two
+  double dx, dy, dz, idx, idy, idz;
+  double ayz, axz, axy, vol, ivol;
+  double gam, gm1, small_rho, small_eps, vlimit, cfl;
+  double muc, rgas;
+};
+
+// Work item of the tiled stage kernel: one 32x8 column tile and a z range of a box.
+struct Tile {
+  int box;
+  int x0, y0;     // interior-relative tile origin
+  int z0, z1;     // interior-relative z range [z0,z1) (for nz<6: plane range)
+};
+
+constexpr int TX = 32;
+constexpr int TY = 8;
+
+// ghost-fill tables: per ghost (index order), destination cell, source cell and
+// momentum sign mask (bit0: m1, bit1: m2, bit2: m3 negated).
+struct GhostTable {
+  std::vector<int32_t> dst;
+  std::vector<int32_t> src1;   // single fill, sources read before the fill
+  std::vector<uint8_t> sgn1;
+  std::vector<int32_t> src2;   // two consecutive fills, resolved to interior cells
+  std::vector<uint8_t> sgn2;
+  bool resolved2 = false;      // every src2 is an interior cell
+  bool face_rule_ok = false;   // face ghosts follow the fixed donor rule of the stage kernels
+};
+
+void build_ghost_tables(const bx_params& P, GhostTable& T);
+void fill_geom(const bx_params& P, Geom& g);
+bool is_pow2(double x);
+
+// ---- kernels (bx_kernels.cu)
+struct StageArgs {
+  const double* X;   // step input planes (C2 if nsrc==2, C3 if nsrc==1)
+  const double* Y;   // stage-1 input: C1
+  double* out;       // stage output planes (interior cells written)
+  Ctrl* ctrl;        // per box control blocks
+  const Geom* geom;  // per box geometry (device)
+  const Tile* tiles;
+  long long ncells_total;  // plane stride of the pooled buffers
+  int nsrc;
+};
+
+cudaError_t launch_stage(int stage, bool pow2, bool threed, const StageArgs& a, int ntiles,
+                         cudaStream_t s);
+cudaError_t launch_dt(Ctrl* ctrl, int nbox, cudaStream_t s);
+cudaError_t launch_end(Ctrl* ctrl, int nbox, cudaStream_t s);
+
+// phase kernels (one reference subroutine each, full arrays)
+struct PhaseArrays {
+  double* cons;     // 5*ng SoA
+  double* cons_old; // 5*ng
+  double* u;        // 3*ng
+  double* p;        // ng
+  double* adindx;   // ng
+  double* gforce;   // 3*ng or null (zero force)
+  double* states;   // 42*ng scratch for flux
+  double* gtmp;     // 5*nghost scratch for the ghost fill
+};
+
+cudaError_t phase_state(const Geom& g, PhaseArrays& a, Ctrl* ctrl, cudaStream_t s);
+cudaError_t phase_velocity(const Geom& g, PhaseArrays& a, Ctrl* ctrl, cudaStream_t s);
+cudaError_t phase_courant(const Geom& g, PhaseArrays& a, Ctrl* ctrl, cudaStream_t s);
+cudaError_t phase_source(const Geom& g, PhaseArrays& a, Ctrl* ctrl, double mult, cudaStream_t s);
+cudaError_t phase_ghost(int nghost, const int32_t* dst, const int32_t* src, const uint8_t* sgn,
+                        PhaseArrays& a, long long ng, cudaStream_t s);
+cudaError_t phase_flux(const Geom& g, PhaseArrays& a, Ctrl* ctrl, int avg, cudaStream_t s);
+cudaError_t phase_courant_finish(Ctrl* ctrl, cudaStream_t s);
+cudaError_t phase_copy_old(const Geom& g, PhaseArrays& a, cudaStream_t s);
+
+// fused <-> phase representation changes
+cudaError_t fused_to_phase(const Geom& g, const double* X, int nsrc, PhaseArrays& a, int nghost,
+                           const int32_t* dst, const int32_t* src2, const uint8_t* sgn2,
+                           cudaStream_t s);
+
+
+// does the uploaded reference state equal what the fused form reproduces
+// (u == m/rho, rho >= 1e-4 everywhere, ghosts == two-sweep fill of the interior)?
+cudaError_t check_clean(const Geom& g, const PhaseArrays& a, int nghost, const int32_t* dst,
+                        const int32_t* src2, const uint8_t* sgn2, Ctrl* ctrl, cudaStream_t s);
+
+// AoS host layout <-> SoA device layout
+cudaError_t aos_to_soa(const double* aos, double* soa, long long n, int k, cudaStream_t s);
+cudaError_t soa_to_aos(const double* soa, double* aos, long long n, int k, cudaStream_t s);
+
+}  // namespace bx

@@ -1,0 +1,912 @@
+// bx_kernels.cu -- sm_100a FP64 kernels of the hydro step.
+//
+// Two kernel families compute the same reference step:
+//
+//  * Fused stage kernels (k_stage<0|1>): one launch per SSP-RK2 stage.  A block
+//    owns a 32x8 column tile of interior cells and marches through a z range.
+//    For each z plane it stages primitives of the tile plus a two-cell x/y halo
+//    in shared memory, builds the limited MUSCL face states once per cell and
+//    direction, computes every x/y face flux once, carries the z-direction
+//    states, face fluxes and primitives of its own column in registers, and
+//    updates the conserved variables in the epilogue.  Sources, the EOS, the
+//    velocity update and the CFL max-reduction of the following step are fused
+//    into the stage kernels; ghost cells are not stored but read through a
+//    fixed donor rule (validated per grid on the host), so each conserved plane
+//    crosses HBM about once per stage.
+//
+//  * Phase kernels: one kernel per reference subroutine (state, velocity,
+//    courant, source, set_ghost_cells, flux) on full arrays, exactly the
+//    reference's data flow including its stored velocity and pressure arrays.
+//    They serve the bisection entry points, the first step after an upload, and
+//    steps where the velocity limiter or the low-density EOS branch fires.
+#include <cuda_runtime.h>
+
+#include "bx_internal.h"
+#include "bx_math.cuh"
+
+namespace bx {
+
+namespace {
+
+__device__ __forceinline__ double ldg(const double* p) { return __ldg(p); }
+
+// donor of a coordinate along one axis for a face ghost (fused path)
+__device__ __forceinline__ int remap_axis(int c, int a0, int a1, int wl, int wr, bool& flip) {
+  if (c < a0) {
+    if (wl) { flip = true; return 2 * a0 - 1 - c; }
+    return a0;
+  }
+  if (c >= a1) {
+    if (wr) { flip = true; return 2 * a1 - 1 - c; }
+    return a1 - 1;
+  }
+  return c;
+}
+
+struct Cons {
+  double d, m1, m2, m3, E;
+};
+
+__device__ __forceinline__ Cons load_cons(const double* B, long long PS, const Geom& g, int x,
+                                          int y, int z) {
+  bool fx = false, fy = false, fz = false;
+  const int xx = remap_axis(x, g.ax0, g.ax1, g.wall[0], g.wall[1], fx);
+  const int yy = remap_axis(y, g.ay0, g.ay1, g.wall[2], g.wall[3], fy);
+  const int zz = g.threed ? remap_axis(z, g.az0, g.az1, g.wall[4], g.wall[5], fz) : z;
+  const long long c = g.base + xx + (long long)yy * g.sy + (long long)zz * g.sz;
+  Cons r;
+  r.d = ldg(B + c);
+  r.m1 = ldg(B + PS + c);
+  r.m2 = ldg(B + 2 * PS + c);
+  r.m3 = ldg(B + 3 * PS + c);
+  r.E = ldg(B + 4 * PS + c);
+  if (fx) r.m1 = -r.m1;
+  if (fy) r.m2 = -r.m2;
+  if (fz) r.m3 = -r.m3;
+  return r;
+}
+
+__device__ __forceinline__ void apply_sources(Cons& c, int nsrc, double small_eps) {
+  for (int k = 0; k < nsrc; ++k) c.E = source_energy(c.d, c.m1, c.m2, c.m3, c.E, small_eps);
+}
+
+// Primitives seen by flux(avg) at a cell.
+//  stage 0: cons = src^nsrc(X); u = m/rho (velocity at main.f90:318); p from
+//           state() with the velocity array of the previous step, which equals
+//           m/rho of the same momenta (source adds zero momentum).
+//  stage 1: cons = Y; u = m/rho of Y (velocity at main.f90:355); p from state()
+//           with the stage-0 velocity m0/rho0 (main.f90:353 uses the stale u).
+template <int STAGE>
+__device__ __forceinline__ Prim load_prim(const StageArgs& a, const Geom& g, int x, int y, int z,
+                                          unsigned& flags) {
+  const long long PS = a.ncells_total;
+  Prim q;
+  if (STAGE == 0) {
+    Cons c = load_cons(a.X, PS, g, x, y, z);
+    apply_sources(c, a.nsrc, g.small_eps);
+    q.d = c.d;
+    q.u1 = c.m1 / c.d;
+    q.u2 = c.m2 / c.d;
+    q.u3 = c.m3 / c.d;
+    q.e = recon_eps(q.d, c.E, q.u1, q.u2, q.u3, g.small_eps);
+    q.p = q.e * g.gm1;
+  } else {
+    const Cons c0 = load_cons(a.X, PS, g, x, y, z);
+    const Cons c1 = load_cons(a.Y, PS, g, x, y, z);
+    q.d = c1.d;
+    q.u1 = c1.m1 / c1.d;
+    q.u2 = c1.m2 / c1.d;
+    q.u3 = c1.m3 / c1.d;
+    const double s1 = c0.m1 / c0.d, s2 = c0.m2 / c0.d, s3 = c0.m3 / c0.d;
+    q.e = recon_eps(q.d, c1.E, q.u1, q.u2, q.u3, g.small_eps);
+    q.p = eos_pressure(q.d, c1.E, s1, s2, s3, g.gm1, g.small_eps);
+  }
+  q.c = sqrt(q.p * g.gam / q.d);
+  if (q.d < kLowRho) flags |= kFlagLowRho;
+  if (fabs(q.u1) > g.vlimit || fabs(q.u2) > g.vlimit || fabs(q.u3) > g.vlimit)
+    flags |= kFlagVlimit;
+  return q;
+}
+
+template <bool POW2>
+__device__ __forceinline__ void dir_states(const Prim& m, const Prim& c, const Prim& p, double ud,
+                                           double dt, double ds, double ids, FaceState& mi,
+                                           FaceState& pl) {
+  const double sd = slope3(m.d, c.d, p.d);
+  const double s1 = slope3(m.u1, c.u1, p.u1);
+  const double s2 = slope3(m.u2, c.u2, p.u2);
+  const double s3 = slope3(m.u3, c.u3, p.u3);
+  const double sp = slope3(m.p, c.p, p.p);
+  const double se = slope3(m.e, c.e, p.e);
+  muscl_states<POW2>(c, ud, sd, s1, s2, s3, sp, se, dt, ds, ids, mi, pl);
+}
+
+// shared-memory geometry of the stage kernel
+constexpr int PW = TX + 4;            // prim plane width (x halo 2)
+constexpr int NP = (TY + 4) * PW;     // prim plane cells
+constexpr int NSX = TY * (TX + 2);    // x-state cells
+constexpr int NSY = (TY + 2) * TX;    // y-state cells
+constexpr int NFX = TY * (TX + 1);    // x faces
+constexpr int NFY = (TY + 1) * TX;    // y faces
+constexpr int SMEM_DOUBLES = 7 * NP + 12 * NSX + 12 * NSY;
+static_assert(5 * NFX + 5 * NFY <= 7 * NP, "face fluxes alias the primitive plane");
+
+__device__ __forceinline__ void put_prim(double* SP, int i, const Prim& q) {
+  SP[0 * NP + i] = q.d;
+  SP[1 * NP + i] = q.u1;
+  SP[2 * NP + i] = q.u2;
+  SP[3 * NP + i] = q.u3;
+  SP[4 * NP + i] = q.p;
+  SP[5 * NP + i] = q.e;
+  SP[6 * NP + i] = q.c;
+}
+__device__ __forceinline__ Prim get_prim(const double* SP, int i) {
+  Prim q;
+  q.d = SP[0 * NP + i];
+  q.u1 = SP[1 * NP + i];
+  q.u2 = SP[2 * NP + i];
+  q.u3 = SP[3 * NP + i];
+  q.p = SP[4 * NP + i];
+  q.e = SP[5 * NP + i];
+  q.c = SP[6 * NP + i];
+  return q;
+}
+__device__ __forceinline__ void put_fs(double* S, int n, int i, const FaceState& f) {
+  S[0 * n + i] = f.d;
+  S[1 * n + i] = f.u1;
+  S[2 * n + i] = f.u2;
+  S[3 * n + i] = f.u3;
+  S[4 * n + i] = f.p;
+  S[5 * n + i] = f.e;
+}
+__device__ __forceinline__ FaceState get_fs(const double* S, int n, int i) {
+  FaceState f;
+  f.d = S[0 * n + i];
+  f.u1 = S[1 * n + i];
+  f.u2 = S[2 * n + i];
+  f.u3 = S[3 * n + i];
+  f.p = S[4 * n + i];
+  f.e = S[5 * n + i];
+  return f;
+}
+__device__ __forceinline__ FaceState as_face(const Prim& q) {
+  FaceState f;
+  f.d = q.d; f.u1 = q.u1; f.u2 = q.u2; f.u3 = q.u3; f.p = q.p; f.e = q.e;
+  return f;
+}
+
+__device__ __forceinline__ double warp_max(double v) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  return v;
+}
+
+}  // namespace
+
+// ------------------------------------------------------------------ stage kernel
+template <int STAGE, bool POW2, bool THREED>
+__global__ void __launch_bounds__(TX* TY, 2) k_stage(StageArgs a) {
+  extern __shared__ double sm[];
+  double* SP = sm;                    // [7][TY+4][TX+4] primitives of the plane
+  double* SX = sm + 7 * NP;           // [12][TY][TX+2] x states (minus 0..5, plus 6..11)
+  double* SY = SX + 12 * NSX;         // [12][TY+2][TX] y states
+  double* FX = sm;                    // [5][TY][TX+1] x face fluxes (aliases SP)
+  double* FY = sm + 5 * NFX;          // [5][TY+1][TX] y face fluxes
+  __shared__ Geom sg;
+  __shared__ double red_rate[TX * TY / 32];
+  __shared__ unsigned red_flags[TX * TY / 32];
+
+  const Tile t = a.tiles[blockIdx.x];
+  if (threadIdx.x == 0) sg = a.geom[t.box];
+  __syncthreads();
+  const Geom& g = sg;
+  Ctrl* C = a.ctrl + t.box;
+  if (!C->active) return;
+  const double dt = C->dt;
+
+  const int tid = threadIdx.x;
+  const int tx = tid % TX, ty = tid / TX;
+  const int NAx = g.ax1 - g.ax0, NAy = g.ay1 - g.ay0;
+  const int w = min(TX, NAx - t.x0), h = min(TY, NAy - t.y0);
+  const bool own = (tx < w) && (ty < h);
+  const int bx0 = g.ax0 + t.x0, by0 = g.ay0 + t.y0;  // full-grid tile origin
+  const int gx = bx0 + tx, gy = by0 + ty;
+  const int nhalo = 4 * h + 4 * w;
+  const int nxs = (w + 2) * h, nys = w * (h + 2);
+  const int nxf = (w + 1) * h, nyf = w * (h + 1);
+  const long long PS = a.ncells_total;
+  const double idz = g.idz;
+
+  unsigned flags = 0;
+  double rate = 0.0;
+
+  // z pipeline of the own column (3-D grids)
+  Prim Pk, Pk1;
+  FaceState plusk;
+  double Fzm[5];
+
+  const int z0 = g.az0 + t.z0, z1 = g.az0 + t.z1;
+  if (THREED && own) {
+    const Prim Pm2 = load_prim<STAGE>(a, g, gx, gy, z0 - 2, flags);
+    const Prim Pm1 = load_prim<STAGE>(a, g, gx, gy, z0 - 1, flags);
+    Pk = load_prim<STAGE>(a, g, gx, gy, z0, flags);
+    Pk1 = load_prim<STAGE>(a, g, gx, gy, z0 + 1, flags);
+    FaceState mm, pm, m0;
+    if (z0 - 1 < g.az0) {
+      ghost_states(Pm1, mm, pm);
+    } else {
+      dir_states<POW2>(Pm2, Pm1, Pk, Pm1.u3, dt, g.dz, idz, mm, pm);
+    }
+    dir_states<POW2>(Pm1, Pk, Pk1, Pk.u3, dt, g.dz, idz, m0, plusk);
+    hll_flux<2>(pm, m0, g.gam, Fzm);
+  }
+
+  for (int z = (THREED ? z0 : g.az0 + t.z0); z < (THREED ? z1 : g.az0 + t.z1); ++z) {
+    // ---- A: primitives of plane z (own from the pipeline, halo computed here)
+    Prim P2;
+    FaceState mz1, pz1;
+    double Fzp[5];
+    if (own) {
+      if (THREED) {
+        P2 = load_prim<STAGE>(a, g, gx, gy, z + 2, flags);
+      } else {
+        Pk = load_prim<STAGE>(a, g, gx, gy, z, flags);
+      }
+      put_prim(SP, (ty + 2) * PW + (tx + 2), Pk);
+    }
+    for (int i = tid; i < nhalo; i += TX * TY) {
+      int cx, cy;
+      if (i < 4 * h) {
+        cy = i >> 2;
+        const int j = i & 3;
+        cx = j < 2 ? j - 2 : w + (j - 2);
+      } else {
+        const int k = i - 4 * h;
+        cx = k % w;
+        const int j = k / w;
+        cy = j < 2 ? j - 2 : h + (j - 2);
+      }
+      const Prim q = load_prim<STAGE>(a, g, bx0 + cx, by0 + cy, z, flags);
+      put_prim(SP, (cy + 2) * PW + (cx + 2), q);
+    }
+    if (THREED && own) {
+      if (z + 1 >= g.az1) {
+        ghost_states(Pk1, mz1, pz1);
+      } else {
+        dir_states<POW2>(Pk, Pk1, P2, Pk1.u3, dt, g.dz, idz, mz1, pz1);
+      }
+      hll_flux<2>(plusk, mz1, g.gam, Fzp);
+    }
+    __syncthreads();
+
+    // ---- B: x and y face states of the plane
+    for (int i = tid; i < nxs + nys; i += TX * TY) {
+      FaceState mi, pl;
+      if (i < nxs) {
+        const int cy = i / (w + 2), cx = i % (w + 2) - 1;
+        const int c = (cy + 2) * PW + (cx + 2);
+        const Prim q = get_prim(SP, c);
+        const int fx = bx0 + cx;
+        if (fx < g.ax0 || fx >= g.ax1) {
+          ghost_states(q, mi, pl);
+        } else {
+          dir_states<POW2>(get_prim(SP, c - 1), q, get_prim(SP, c + 1), q.u1, dt, g.dx, g.idx, mi,
+                           pl);
+        }
+        const int o = cy * (TX + 2) + (cx + 1);
+        put_fs(SX, NSX, o, mi);
+        put_fs(SX + 6 * NSX, NSX, o, pl);
+      } else {
+        const int k = i - nxs;
+        const int cy = k / w - 1, cx = k % w;
+        const int c = (cy + 2) * PW + (cx + 2);
+        const Prim q = get_prim(SP, c);
+        const int fy = by0 + cy;
+        if (fy < g.ay0 || fy >= g.ay1) {
+          ghost_states(q, mi, pl);
+        } else {
+          dir_states<POW2>(get_prim(SP, c - PW), q, get_prim(SP, c + PW), q.u2, dt, g.dy, g.idy,
+                           mi, pl);
+        }
+        const int o = (cy + 1) * TX + cx;
+        put_fs(SY, NSY, o, mi);
+        put_fs(SY + 6 * NSY, NSY, o, pl);
+      }
+    }
+    __syncthreads();
+
+    // ---- C: x and y face fluxes (face f lies between cells f-1 and f)
+    for (int i = tid; i < nxf + nyf; i += TX * TY) {
+      double F[5];
+      if (i < nxf) {
+        const int cy = i / (w + 1), f = i % (w + 1);
+        const int base = cy * (TX + 2);
+        const FaceState L = get_fs(SX + 6 * NSX, NSX, base + f);  // plus state of cell f-1
+        const FaceState R = get_fs(SX, NSX, base + f + 1);        // minus state of cell f
+        hll_flux<0>(L, R, g.gam, F);
+        const int o = cy * (TX + 1) + f;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) FX[q * NFX + o] = F[q];
+      } else {
+        const int k = i - nxf;
+        const int f = k / w, cx = k % w;
+        const FaceState L = get_fs(SY + 6 * NSY, NSY, f * TX + cx);
+        const FaceState R = get_fs(SY, NSY, (f + 1) * TX + cx);
+        hll_flux<1>(L, R, g.gam, F);
+        const int o = f * TX + cx;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) FY[q * NFY + o] = F[q];
+      }
+    }
+    __syncthreads();
+
+    // ---- D: conservative update of the own cell (flux.f90:186-230)
+    if (own) {
+      double ft[5];
+#pragma unroll
+      for (int q = 0; q < 5; ++q) {
+        const double dfx = FX[q * NFX + ty * (TX + 1) + tx + 1] - FX[q * NFX + ty * (TX + 1) + tx];
+        const double dfy = FY[q * NFY + (ty + 1) * TX + tx] - FY[q * NFY + ty * TX + tx];
+        double sum = g.ayz * dfx + g.axz * dfy;
+        if (THREED) sum = sum + g.axy * (Fzp[q] - Fzm[q]);
+        ft[q] = POW2 ? -sum * dt * g.ivol : -sum * dt / g.vol;
+      }
+      Cons c0 = load_cons(a.X, PS, g, gx, gy, z);
+      apply_sources(c0, a.nsrc, g.small_eps);
+      double n[5];
+      if (STAGE == 0) {
+        n[0] = c0.d + ft[0];
+        n[1] = c0.m1 + ft[1];
+        n[2] = c0.m2 + ft[2];
+        n[3] = c0.m3 + ft[3];
+        n[4] = c0.E + ft[4];
+      } else {
+        const Cons c1 = load_cons(a.Y, PS, g, gx, gy, z);
+        n[0] = kHalf * (c0.d + c1.d + ft[0]);
+        n[1] = kHalf * (c0.m1 + c1.m1 + ft[1]);
+        n[2] = kHalf * (c0.m2 + c1.m2 + ft[2]);
+        n[3] = kHalf * (c0.m3 + c1.m3 + ft[3]);
+        n[4] = kHalf * (c0.E + c1.E + ft[4]);
+      }
+      floors(n[0], n[1], n[2], n[3], n[4], g.small_rho, g.small_eps);
+      if (!(isfinite(n[0]) && isfinite(n[1]) && isfinite(n[2]) && isfinite(n[3]) &&
+            isfinite(n[4])))
+        flags |= kFlagNonFinite;
+      if (STAGE == 1) {
+        // state/velocity after flux(1) and after source(1) (main.f90:372-380,490-515)
+        const double u1 = n[1] / n[0], u2 = n[2] / n[0], u3 = n[3] / n[0];
+        if (n[0] < kLowRho) flags |= kFlagLowRho;
+        if (fabs(u1) > g.vlimit || fabs(u2) > g.vlimit || fabs(u3) > g.vlimit)
+          flags |= kFlagVlimit;
+        // source(1) energy, then the Courant rate of the next step (courant.f90:173-175)
+        const double E3 = source_energy(n[0], n[1], n[2], n[3], n[4], g.small_eps);
+        const double pA = eos_pressure(n[0], E3, u1, u2, u3, g.gm1, g.small_eps);
+        const double r0 = courant_rate<POW2>(n[0], pA, g.gam, u1, u2, u3, g.dx, g.dy, g.dz,
+                                             g.idx, g.idy, g.idz);
+        rate = fmax(rate, r0);
+        if (!(r0 >= 0.0)) flags |= kFlagNonFinite;
+      }
+      const long long o = g.base + gx + (long long)gy * g.sy + (long long)z * g.sz;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) a.out[q * PS + o] = n[q];
+      if (THREED) {
+#pragma unroll
+        for (int q = 0; q < 5; ++q) Fzm[q] = Fzp[q];
+        plusk = pz1;
+        Pk = Pk1;
+        Pk1 = P2;
+      }
+    }
+    __syncthreads();
+  }
+
+  // block reductions of the Courant rate and the status bits
+  const unsigned wf = __reduce_or_sync(0xffffffffu, flags);
+  const double wr = warp_max(rate);
+  if ((tid & 31) == 0) {
+    red_flags[tid >> 5] = wf;
+    red_rate[tid >> 5] = wr;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    unsigned f = 0;
+    double r = 0.0;
+    for (int k = 0; k < TX * TY / 32; ++k) {
+      f |= red_flags[k];
+      r = fmax(r, red_rate[k]);
+    }
+    if (f) atomicOr(&C->flags, f);
+    if (STAGE == 1) atomicMax(&C->rate_bits, (unsigned long long)__double_as_longlong(r));
+  }
+}
+
+template <int STAGE, bool POW2, bool THREED>
+static cudaError_t launch_stage_t(const StageArgs& a, int ntiles, cudaStream_t s) {
+  const size_t smem = SMEM_DOUBLES * sizeof(double);
+  static bool attr_set = false;
+  if (!attr_set) {
+    cudaError_t e = cudaFuncSetAttribute(k_stage<STAGE, POW2, THREED>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    attr_set = true;
+  }
+  if (ntiles <= 0) return cudaSuccess;
+  k_stage<STAGE, POW2, THREED><<<ntiles, TX * TY, smem, s>>>(a);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_stage(int stage, bool pow2, bool threed, const StageArgs& a, int ntiles,
+                         cudaStream_t s) {
+  if (stage == 0) {
+    if (pow2) return threed ? launch_stage_t<0, true, true>(a, ntiles, s)
+                            : launch_stage_t<0, true, false>(a, ntiles, s);
+    return threed ? launch_stage_t<0, false, true>(a, ntiles, s)
+                  : launch_stage_t<0, false, false>(a, ntiles, s);
+  }
+  if (pow2) return threed ? launch_stage_t<1, true, true>(a, ntiles, s)
+                          : launch_stage_t<1, true, false>(a, ntiles, s);
+  return threed ? launch_stage_t<1, false, true>(a, ntiles, s)
+                : launch_stage_t<1, false, false>(a, ntiles, s);
+}
+
+size_t stage_smem_bytes() { return SMEM_DOUBLES * sizeof(double); }
+
+// ------------------------------------------------------------------ clock kernels
+// dt control of main.f90:266-281 and 342, per box
+__global__ void k_dt(Ctrl* ctrl, int n) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  Ctrl& c = ctrl[b];
+  if (!(c.time < c.endtime) || c.step >= 1000000 || c.step >= c.max_step) {
+    c.active = 0;
+    return;
+  }
+  c.step = c.step + 1;
+  const double rate = __longlong_as_double((long long)c.rate_bits);
+  c.rate = rate;
+  c.rate_bits = 0ull;
+  double dt = c.cfl / rate;            // courant.f90:182
+  dt = dt * 1.0;                       // dt*f1, f1=one
+  if (c.step > 1 && c.dtold > 0.0) dt = fmin(dt, c.dtold * 1.1);
+  c.dtold = dt;
+  if (dt + c.time > c.endtime) dt = c.endtime - c.time;
+  dt = dt * kHalf;                     // source(time,0) runs with dt/2
+  dt = dt * 2.0;                       // flux stages run with the full dt
+  c.dt = dt;
+  c.active = 1;
+}
+
+// main.f90:471,544-545
+__global__ void k_end(Ctrl* ctrl, int n) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  Ctrl& c = ctrl[b];
+  if (!c.active) return;
+  double dt = kHalf * c.dt;
+  dt = dt * 2.0;
+  c.time = c.time + dt;
+}
+
+cudaError_t launch_dt(Ctrl* ctrl, int nbox, cudaStream_t s) {
+  k_dt<<<(nbox + 127) / 128, 128, 0, s>>>(ctrl, nbox);
+  return cudaGetLastError();
+}
+cudaError_t launch_end(Ctrl* ctrl, int nbox, cudaStream_t s) {
+  k_end<<<(nbox + 127) / 128, 128, 0, s>>>(ctrl, nbox);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ phase kernels
+namespace {
+
+constexpr int PB = 256;
+inline int nblk(long long n) { return (int)((n + PB - 1) / PB); }
+
+__device__ __forceinline__ bool is_ghost(const Geom& g, int x, int y, int z) {
+  return x < g.ax0 || x >= g.ax1 || y < g.ay0 || y >= g.ay1 ||
+         (g.threed && (z < g.az0 || z >= g.az1));
+}
+
+// state.f90:29-87, fixed gamma
+__global__ void k_phase_state(Geom g, PhaseArrays a, Ctrl* ctrl) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= g.ng) return;
+  const long long n = g.ng;
+  const double d = a.cons[i];
+  const double u1 = a.u[i], u2 = a.u[n + i], u3 = a.u[2 * n + i];
+  const double ekin = kin_rho_u(d, u1, u2, u3);
+  double eps = fmax(a.cons[4 * n + i] - ekin, g.small_eps);
+  a.adindx[i] = g.gam;
+  if (d < kLowRho) {
+    const double tk = fmin(5e3, a.p[i] / (d * g.rgas) * g.muc);
+    const double p = (d * tk * g.rgas / g.muc);
+    a.p[i] = p;
+    eps = p / (g.gam - 1.0);
+    a.cons[4 * n + i] = eps + ekin;
+    atomicOr(&ctrl->flags, (unsigned)kFlagLowRho);
+  } else {
+    a.p[i] = eps * (g.gam - 1.0);
+  }
+}
+
+// velocity.f90:107-141
+__global__ void k_phase_velocity(Geom g, PhaseArrays a, Ctrl* ctrl) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= g.ng) return;
+  const long long n = g.ng;
+  double* c = a.cons;
+  const double d = c[i];
+  double u[3];
+  for (int k = 0; k < 3; ++k) u[k] = c[(k + 1) * n + i] / d;
+  int flag = 0;
+  for (int k = 0; k < 3; ++k)
+    if (fabs(u[k]) > g.vlimit) flag = 1;
+  if (flag) {
+    double ekin = kin_mom(d, c[n + i], c[2 * n + i], c[3 * n + i]);
+    double speed = 0.0;
+    for (int k = 0; k < 3; ++k) speed = speed + u[k] * u[k];
+    speed = sqrt(speed);
+    for (int k = 0; k < 3; ++k) {
+      u[k] = u[k] * g.vlimit / speed;
+      c[(k + 1) * n + i] = u[k] * d;
+    }
+    double E = c[4 * n + i] - ekin;
+    ekin = kin_mom(d, c[n + i], c[2 * n + i], c[3 * n + i]);
+    c[4 * n + i] = fmax(E, g.small_eps) + ekin;
+    atomicOr(&ctrl->flags, (unsigned)kFlagVlimit);
+  }
+  for (int k = 0; k < 3; ++k) a.u[k * n + i] = u[k];
+}
+
+// courant.f90:172-176 (max over every cell, ghosts included)
+__global__ void k_phase_courant(Geom g, PhaseArrays a, Ctrl* ctrl) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long n = g.ng;
+  double r = 0.0;
+  bool bad = false;
+  if (i < n) {
+    const double sound = sqrt(a.adindx[i] * a.p[i] / a.cons[i]);
+    const double r0 = (sound + fabs(a.u[i])) / g.dx + (sound + fabs(a.u[n + i])) / g.dy +
+                      (sound + fabs(a.u[2 * n + i])) / g.dz;
+    if (!(r0 >= 0.0)) bad = true;
+    r = fmax(r, r0);
+  }
+  __shared__ double wm[PB / 32];
+  r = warp_max(r);
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = r;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int k = 0; k < PB / 32; ++k) m = fmax(m, wm[k]);
+    atomicMax(&ctrl->rate_bits, (unsigned long long)__double_as_longlong(m));
+  }
+  if (bad) atomicOr(&ctrl->flags, (unsigned)kFlagNonFinite);
+}
+
+__global__ void k_phase_courant_finish(Ctrl* ctrl) {
+  Ctrl& c = *ctrl;
+  c.rate = __longlong_as_double((long long)c.rate_bits);
+  c.dt = c.cfl / c.rate;
+}
+
+// source.f90:148-191 (interior cells)
+__global__ void k_phase_source(Geom g, PhaseArrays a, Ctrl* ctrl, double mult) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= g.ng) return;
+  const int x = (int)(i % g.nx), y = (int)((i / g.nx) % g.ny), z = (int)(i / g.sz);
+  if (is_ghost(g, x, y, z)) return;
+  const long long n = g.ng;
+  const double dt = mult * ctrl->dt;
+  double d = a.cons[i], m1 = a.cons[n + i], m2 = a.cons[2 * n + i], m3 = a.cons[3 * n + i],
+         E = a.cons[4 * n + i];
+  double g1 = 0.0, g2 = 0.0, g3 = 0.0;
+  if (a.gforce) {
+    g1 = a.gforce[i];
+    g2 = a.gforce[n + i];
+    g3 = a.gforce[2 * n + i];
+  }
+  source_gravity(d, m1, m2, m3, E, g1, g2, g3, a.u[i], a.u[n + i], a.u[2 * n + i], dt,
+                 g.small_eps);
+  a.cons[n + i] = m1;
+  a.cons[2 * n + i] = m2;
+  a.cons[3 * n + i] = m3;
+  a.cons[4 * n + i] = E;
+}
+
+// set_ghost_cells as gather (values before the sweep) + scatter
+__global__ void k_ghost_gather(int nghost, const int32_t* src, const uint8_t* sgn,
+                               const double* cons, long long n, double* tmp) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nghost) return;
+  const long long s = src[k];
+  const unsigned m = sgn[k];
+  tmp[k] = cons[s];
+  tmp[nghost + k] = (m & 1) ? -cons[n + s] : cons[n + s];
+  tmp[2 * nghost + k] = (m & 2) ? -cons[2 * n + s] : cons[2 * n + s];
+  tmp[3 * nghost + k] = (m & 4) ? -cons[3 * n + s] : cons[3 * n + s];
+  tmp[4 * nghost + k] = cons[4 * n + s];
+}
+__global__ void k_ghost_scatter(int nghost, const int32_t* dst, const double* tmp, double* cons,
+                                long long n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nghost) return;
+  const long long d = dst[k];
+  for (int q = 0; q < 5; ++q) cons[q * n + d] = tmp[q * nghost + k];
+}
+
+// flux.f90:47-116: slopes and interface states of every cell.
+// states layout: [(dir*2+side)*7 + q][cell], side 0 = minus, 1 = plus,
+// q = rho, u1, u2, u3, p, eps, gamma.
+__global__ void k_phase_states(Geom g, PhaseArrays a, Ctrl* ctrl) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= g.ng) return;
+  const long long n = g.ng;
+  const int x = (int)(i % g.nx), y = (int)((i / g.nx) % g.ny), z = (int)(i / g.sz);
+  const bool ghost = is_ghost(g, x, y, z);
+  const double dt = ctrl->dt;
+  const double* c = a.cons;
+  const double* u = a.u;
+  const double ds[3] = {g.dx, g.dy, g.dz};
+  const long long st[3] = {1, g.sy, g.threed ? g.sz : 0};
+  const double d0 = c[i];
+  const double sound = sqrt(a.p[i] * a.adindx[i] / d0);
+  const double eps0 = recon_eps(d0, c[4 * n + i], u[i], u[n + i], u[2 * n + i], g.small_eps);
+  for (int dir = 0; dir < 3; ++dir) {
+    const long long im = ghost ? i : i - st[dir], ip = ghost ? i : i + st[dir];
+    const long long idx3[3] = {im, i, ip};
+    double sl[7];
+    for (int k = 0; k < 3; ++k)
+      sl[1 + k] = slope3(u[k * n + im], u[k * n + i], u[k * n + ip]);
+    double eps[3];
+    for (int k = 0; k < 3; ++k) {
+      const long long j = idx3[k];
+      eps[k] = recon_eps(c[j], c[4 * n + j], u[j], u[n + j], u[2 * n + j], g.small_eps);
+    }
+    sl[4] = slope3(a.p[im], a.p[i], a.p[ip]);
+    sl[0] = slope3(c[im], c[i], c[ip]);
+    sl[5] = slope3(eps[0], eps[1], eps[2]);
+    sl[6] = slope3(a.adindx[im], a.adindx[i], a.adindx[ip]);
+    const double ud = u[dir * n + i];
+    const double lp = fmax(ud + sound, 0.0) * dt / ds[dir];
+    const double lm = fmin(ud - sound, 0.0) * dt / ds[dir];
+    const double q[7] = {d0, u[i], u[n + i], u[2 * n + i], a.p[i], eps0, a.adindx[i]};
+    for (int k = 0; k < 7; ++k) {
+      const double mi = q[k] + kHalf * (-1.0 - lm) * sl[k];
+      const double pl = q[k] + kHalf * (1.0 - lp) * sl[k];
+      a.states[((dir * 2 + 0) * 7 + k) * n + i] = mi + 0.0 * (dt * kHalf / ds[dir]);
+      a.states[((dir * 2 + 1) * 7 + k) * n + i] = pl + 0.0 * (dt * kHalf / ds[dir]);
+    }
+  }
+}
+
+__device__ __forceinline__ void phase_face(const double* S, long long n, int dir, long long lc,
+                                           long long rc, double F[5]) {
+  // plus state of the low cell, minus state of the high cell (flux.f90:504-530)
+  const double* Lp = S + ((dir * 2 + 1) * 7) * n;
+  const double* Rm = S + ((dir * 2 + 0) * 7) * n;
+  const double dl = Lp[lc], vxl = Lp[n + lc], vyl = Lp[2 * n + lc], vzl = Lp[3 * n + lc],
+               pl = Lp[4 * n + lc], el = Lp[5 * n + lc], gl = Lp[6 * n + lc];
+  const double dr = Rm[rc], vxr = Rm[n + rc], vyr = Rm[2 * n + rc], vzr = Rm[3 * n + rc],
+               pr = Rm[4 * n + rc], er = Rm[5 * n + rc], gr = Rm[6 * n + rc];
+  double sl[5], sr[5], fl[5], fr[5];
+  sl[0] = dl; sl[1] = dl * vxl; sl[2] = dl * vyl; sl[3] = dl * vzl;
+  sl[4] = el + kHalf * dl * (vxl * vxl + vyl * vyl + vzl * vzl);
+  sr[0] = dr; sr[1] = dr * vxr; sr[2] = dr * vyr; sr[3] = dr * vzr;
+  sr[4] = er + kHalf * dr * (vxr * vxr + vyr * vyr + vzr * vzr);
+  for (int k = 0; k < 5; ++k) { fl[k] = 0.0; fr[k] = 0.0; }
+  double vl, vr;
+  if (dir == 0) { vr = vxr; vl = vxl; fl[1] = pl; fr[1] = pr; }
+  else if (dir == 1) { vr = vyr; vl = vyl; fl[2] = pl; fr[2] = pr; }
+  else { vr = vzr; vl = vzl; fl[3] = pl; fr[3] = pr; }
+  fl[0] = sl[0] * vl;
+  fl[1] = fl[1] + sl[1] * vl;
+  fl[2] = fl[2] + sl[2] * vl;
+  fl[3] = fl[3] + sl[3] * vl;
+  fl[4] = (sl[4] + pl) * vl;
+  fr[0] = sr[0] * vr;
+  fr[1] = fr[1] + sr[1] * vr;
+  fr[2] = fr[2] + sr[2] * vr;
+  fr[3] = fr[3] + sr[3] * vr;
+  fr[4] = (sr[4] + pr) * vr;
+  const double cr = sqrt(gr * pr / dr);
+  const double cl = sqrt(gl * pl / dl);
+  const double ap = fmax(fmax(0.0, vr + cr), vl + cl);
+  const double am = fmax(fmax(0.0, -(vr - cr)), -(vl - cl));
+  for (int k = 0; k < 5; ++k) F[k] = (ap * fl[k] + am * fr[k] - ap * am * (sr[k] - sl[k])) / (ap + am);
+}
+
+// flux.f90:121-230: face fluxes of interior cells, update of every cell, floors
+__global__ void k_phase_update(Geom g, PhaseArrays a, Ctrl* ctrl, int avg) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= g.ng) return;
+  const long long n = g.ng;
+  const int x = (int)(i % g.nx), y = (int)((i / g.nx) % g.ny), z = (int)(i / g.sz);
+  const double dt = ctrl->dt;
+  double ft[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+  if (!is_ghost(g, x, y, z)) {
+    const long long st[3] = {1, g.sy, g.threed ? g.sz : 0};
+    double fm[3][5], fp[3][5];
+    for (int dir = 0; dir < 3; ++dir) {
+      phase_face(a.states, n, dir, i - st[dir], i, fm[dir]);
+      phase_face(a.states, n, dir, i, i + st[dir], fp[dir]);
+    }
+    for (int k = 0; k < 5; ++k)
+      ft[k] = -(g.ayz * (fp[0][k] - fm[0][k]) + g.axz * (fp[1][k] - fm[1][k]) +
+                g.axy * (fp[2][k] - fm[2][k])) * dt / g.vol;
+  }
+  double v[5];
+  for (int k = 0; k < 5; ++k) {
+    const double c = a.cons[k * n + i];
+    v[k] = avg == 0 ? c + ft[k] : kHalf * (a.cons_old[k * n + i] + c + ft[k]);
+  }
+  floors(v[0], v[1], v[2], v[3], v[4], g.small_rho, g.small_eps);
+  bool bad = false;
+  for (int k = 0; k < 5; ++k) {
+    a.cons[k * n + i] = v[k];
+    if (!isfinite(v[k])) bad = true;
+  }
+  if (bad) atomicOr(&ctrl->flags, (unsigned)kFlagNonFinite);
+}
+
+__global__ void k_copy5(const double* src, double* dst, long long n) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= 5 * n) return;
+  dst[i] = src[i];
+}
+
+// fused state (X planes) -> reference arrays: interior cons = src^(nsrc-1)(X)
+__global__ void k_f2p_interior(Geom g, const double* X, int nsrc, PhaseArrays a) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= g.ng) return;
+  const int x = (int)(i % g.nx), y = (int)((i / g.nx) % g.ny), z = (int)(i / g.sz);
+  if (is_ghost(g, x, y, z)) return;
+  const long long n = g.ng;
+  Cons c{X[i], X[n + i], X[2 * n + i], X[3 * n + i], X[4 * n + i]};
+  apply_sources(c, nsrc - 1, g.small_eps);
+  a.cons[i] = c.d;
+  a.cons[n + i] = c.m1;
+  a.cons[2 * n + i] = c.m2;
+  a.cons[3 * n + i] = c.m3;
+  a.cons[4 * n + i] = c.E;
+}
+__global__ void k_fill_resolved(int nghost, const int32_t* dst, const int32_t* src,
+                                const uint8_t* sgn, double* cons, long long n) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nghost) return;
+  const long long s = src[k], d = dst[k];
+  const unsigned m = sgn[k];
+  cons[d] = cons[s];
+  cons[n + d] = (m & 1) ? -cons[n + s] : cons[n + s];
+  cons[2 * n + d] = (m & 2) ? -cons[2 * n + s] : cons[2 * n + s];
+  cons[3 * n + d] = (m & 4) ? -cons[3 * n + s] : cons[3 * n + s];
+  cons[4 * n + d] = cons[4 * n + s];
+}
+// velocity and pressure arrays of the reference after the last state()/velocity()
+__global__ void k_f2p_prims(Geom g, PhaseArrays a) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= g.ng) return;
+  const long long n = g.ng;
+  const double d = a.cons[i];
+  const double u1 = a.cons[n + i] / d, u2 = a.cons[2 * n + i] / d, u3 = a.cons[3 * n + i] / d;
+  a.u[i] = u1;
+  a.u[n + i] = u2;
+  a.u[2 * n + i] = u3;
+  a.p[i] = eos_pressure(d, a.cons[4 * n + i], u1, u2, u3, g.gm1, g.small_eps);
+  a.adindx[i] = g.gam;
+}
+
+__global__ void k_check_cells(Geom g, PhaseArrays a, Ctrl* ctrl) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= g.ng) return;
+  const long long n = g.ng;
+  const double d = a.cons[i];
+  bool ok = d >= kLowRho;
+  for (int k = 0; k < 3; ++k) ok = ok && (a.u[k * n + i] == a.cons[(k + 1) * n + i] / d);
+  if (!ok) atomicOr(&ctrl->flags, (unsigned)kFlagNotClean);
+}
+__global__ void k_check_ghosts(int nghost, const int32_t* dst, const int32_t* src,
+                               const uint8_t* sgn, const double* cons, long long n, Ctrl* ctrl) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nghost) return;
+  const long long s = src[k], d = dst[k];
+  const unsigned m = sgn[k];
+  bool ok = cons[d] == cons[s] && cons[4 * n + d] == cons[4 * n + s];
+  ok = ok && cons[n + d] == ((m & 1) ? -cons[n + s] : cons[n + s]);
+  ok = ok && cons[2 * n + d] == ((m & 2) ? -cons[2 * n + s] : cons[2 * n + s]);
+  ok = ok && cons[3 * n + d] == ((m & 4) ? -cons[3 * n + s] : cons[3 * n + s]);
+  if (!ok) atomicOr(&ctrl->flags, (unsigned)kFlagNotClean);
+}
+
+__global__ void k_aos_to_soa(const double* aos, double* soa, long long n, int k) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int q = 0; q < k; ++q) soa[q * n + i] = aos[i * k + q];
+}
+__global__ void k_soa_to_aos(const double* soa, double* aos, long long n, int k) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int q = 0; q < k; ++q) aos[i * k + q] = soa[q * n + i];
+}
+
+}  // namespace
+
+cudaError_t phase_state(const Geom& g, PhaseArrays& a, Ctrl* ctrl, cudaStream_t s) {
+  k_phase_state<<<nblk(g.ng), PB, 0, s>>>(g, a, ctrl);
+  return cudaGetLastError();
+}
+cudaError_t phase_velocity(const Geom& g, PhaseArrays& a, Ctrl* ctrl, cudaStream_t s) {
+  k_phase_velocity<<<nblk(g.ng), PB, 0, s>>>(g, a, ctrl);
+  return cudaGetLastError();
+}
+cudaError_t phase_courant(const Geom& g, PhaseArrays& a, Ctrl* ctrl, cudaStream_t s) {
+  k_phase_courant<<<nblk(g.ng), PB, 0, s>>>(g, a, ctrl);
+  return cudaGetLastError();
+}
+cudaError_t phase_courant_finish(Ctrl* ctrl, cudaStream_t s) {
+  k_phase_courant_finish<<<1, 1, 0, s>>>(ctrl);
+  return cudaGetLastError();
+}
+cudaError_t phase_source(const Geom& g, PhaseArrays& a, Ctrl* ctrl, double mult, cudaStream_t s) {
+  k_phase_source<<<nblk(g.ng), PB, 0, s>>>(g, a, ctrl, mult);
+  return cudaGetLastError();
+}
+cudaError_t phase_ghost(int nghost, const int32_t* dst, const int32_t* src, const uint8_t* sgn,
+                        PhaseArrays& a, long long ng, cudaStream_t s) {
+  if (nghost <= 0) return cudaSuccess;
+  k_ghost_gather<<<nblk(nghost), PB, 0, s>>>(nghost, src, sgn, a.cons, ng, a.gtmp);
+  k_ghost_scatter<<<nblk(nghost), PB, 0, s>>>(nghost, dst, a.gtmp, a.cons, ng);
+  return cudaGetLastError();
+}
+cudaError_t phase_flux(const Geom& g, PhaseArrays& a, Ctrl* ctrl, int avg, cudaStream_t s) {
+  k_phase_states<<<nblk(g.ng), PB, 0, s>>>(g, a, ctrl);
+  k_phase_update<<<nblk(g.ng), PB, 0, s>>>(g, a, ctrl, avg);
+  return cudaGetLastError();
+}
+cudaError_t phase_copy_old(const Geom& g, PhaseArrays& a, cudaStream_t s) {
+  k_copy5<<<nblk(5 * g.ng), PB, 0, s>>>(a.cons, a.cons_old, g.ng);
+  return cudaGetLastError();
+}
+cudaError_t fused_to_phase(const Geom& g, const double* X, int nsrc, PhaseArrays& a, int nghost,
+                           const int32_t* dst, const int32_t* src2, const uint8_t* sgn2,
+                           cudaStream_t s) {
+  k_f2p_interior<<<nblk(g.ng), PB, 0, s>>>(g, X, nsrc, a);
+  if (nghost > 0)
+    k_fill_resolved<<<nblk(nghost), PB, 0, s>>>(nghost, dst, src2, sgn2, a.cons, g.ng);
+  k_f2p_prims<<<nblk(g.ng), PB, 0, s>>>(g, a);
+  return cudaGetLastError();
+}
+cudaError_t check_clean(const Geom& g, const PhaseArrays& a, int nghost, const int32_t* dst,
+                        const int32_t* src2, const uint8_t* sgn2, Ctrl* ctrl, cudaStream_t s) {
+  k_check_cells<<<nblk(g.ng), PB, 0, s>>>(g, a, ctrl);
+  if (nghost > 0) k_check_ghosts<<<nblk(nghost), PB, 0, s>>>(nghost, dst, src2, sgn2, a.cons, g.ng, ctrl);
+  return cudaGetLastError();
+}
+cudaError_t aos_to_soa(const double* aos, double* soa, long long n, int k, cudaStream_t s) {
+  k_aos_to_soa<<<nblk(n), PB, 0, s>>>(aos, soa, n, k);
+  return cudaGetLastError();
+}
+cudaError_t soa_to_aos(const double* soa, double* aos, long long n, int k, cudaStream_t s) {
+  k_soa_to_aos<<<nblk(n), PB, 0, s>>>(soa, aos, n, k);
+  return cudaGetLastError();
+}
+
+}  // namespace bx
+
+namespace bx {
+int stage_blocks_per_sm(int stage, bool pow2, bool threed) {
+  int nb = 0;
+  const size_t smem = stage_smem_bytes();
+  const void* fn;
+  if (stage == 0)
+    fn = pow2 ? (threed ? (const void*)k_stage<0, true, true> : (const void*)k_stage<0, true, false>)
+              : (threed ? (const void*)k_stage<0, false, true> : (const void*)k_stage<0, false, false>);
+  else
+    fn = pow2 ? (threed ? (const void*)k_stage<1, true, true> : (const void*)k_stage<1, true, false>)
+              : (threed ? (const void*)k_stage<1, false, true> : (const void*)k_stage<1, false, false>);
+  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, TX * TY, smem) != cudaSuccess) {
+    cudaGetLastError();
+    return 1;
+  }
+  return nb;
+}
+}  // namespace bx

@@ -1,0 +1,182 @@
+"""Host-side mirror of the reference's hydro-step interface, over the C ABI.
+
+`Hydro` holds one grid on the GPU.  Its methods carry the names of the
+reference's subroutines (state, velocity, courant, source, set_ghost_cells,
+flux, avisc) and act on the handle's device copies of the module arrays
+exactly as those subroutines act on grid_commons; `step` is one iteration of
+the main loop (main.f90:212-545) and `run` the loop itself.  Arrays cross the
+boundary in the reference layout: cons (ng,5), u (ng,3), p (ng,).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from ._lib import BoxzyError, check, lib, make_params
+from .params import HydroParams
+
+
+def _arr(a, n, k):
+    if a is None:
+        return None
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if a.size != n * k:
+        raise ValueError(f"expected {n}x{k} doubles, got shape {a.shape}")
+    return a
+
+
+class Hydro:
+    """One BOXZYHYDRO grid advanced by the sm_100a kernels."""
+
+    def __init__(self, params: HydroParams, phase_only: bool = False):
+        params.validate()
+        self.params = params
+        self.ng = params.ngrid
+        self._p = make_params(params, _lib.FLAG_PHASE_ONLY if phase_only else 0)
+        h = C.c_void_p()
+        check(lib().bx_create(C.byref(self._p), C.byref(h)), None)
+        self._h = h
+
+    # ---- lifetime
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().bx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def _c(self, rc):
+        check(rc, self._h)
+
+    # ---- arrays
+    def upload(self, cons, u=None, p=None):
+        c = _arr(cons, self.ng, 5)
+        uu = _arr(u, self.ng, 3)
+        pp = _arr(p, self.ng, 1)
+        ptr = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
+        self._c(lib().bx_upload(self._h, ptr(c), ptr(uu), ptr(pp)))
+
+    def upload_state(self, st):
+        self.upload(st.cons, st.u, st.p)
+
+    def download(self):
+        c = np.empty((self.ng, 5))
+        u = np.empty((self.ng, 3))
+        p = np.empty(self.ng)
+        self._c(lib().bx_download(self._h, c.ctypes.data_as(C.c_void_p),
+                                  u.ctypes.data_as(C.c_void_p), p.ctypes.data_as(C.c_void_p)))
+        return c, u, p
+
+    def set_gforce(self, g3):
+        g = _arr(g3, self.ng, 3)
+        self._c(lib().bx_set_gforce(self._h, None if g is None else g.ctypes.data_as(C.c_void_p)))
+
+    def set_stream(self, stream_ptr):
+        self._c(lib().bx_set_stream(self._h, C.c_void_p(stream_ptr) if stream_ptr else None))
+
+    def device_cons(self):
+        """(device pointer, ngrid) of the reference cons planes (SoA, 5 x ngrid)."""
+        ptr = C.c_void_p()
+        n = C.c_int64()
+        self._c(lib().bx_device_cons(self._h, C.byref(ptr), C.byref(n)))
+        return ptr.value, n.value
+
+    # ---- clock (main.f90 time, dt, dtold, step)
+    def set_clock(self, time=0.0, dtold=0.0, step=0):
+        self._c(lib().bx_set_clock(self._h, float(time), float(dtold), int(step)))
+
+    def clock(self):
+        t, dt, dto = C.c_double(), C.c_double(), C.c_double()
+        st = C.c_int64()
+        self._c(lib().bx_get_clock(self._h, C.byref(t), C.byref(dt), C.byref(dto), C.byref(st)))
+        return dict(time=t.value, dt=dt.value, dtold=dto.value, step=st.value)
+
+    def set_dt(self, dt):
+        self._c(lib().bx_set_dt(self._h, float(dt)))
+
+    # ---- the reference's subroutines
+    def state(self):
+        self._c(lib().bx_state(self._h))
+
+    def velocity(self):
+        self._c(lib().bx_velocity(self._h))
+
+    def courant(self):
+        dt = C.c_double()
+        self._c(lib().bx_courant(self._h, C.byref(dt)))
+        return dt.value
+
+    def source(self, siter):
+        self._c(lib().bx_source(self._h, int(siter)))
+
+    def set_ghost_cells(self):
+        self._c(lib().bx_ghost(self._h))
+
+    def flux(self, avg):
+        self._c(lib().bx_flux(self._h, int(avg)))
+
+    def avisc(self):
+        self._c(lib().bx_avisc(self._h))
+
+    def save_cons_old(self):
+        self._c(lib().bx_save_cons_old(self._h))
+
+    # ---- main loop
+    def step(self, endtime=1e300):
+        ran = C.c_int32()
+        self._c(lib().bx_step(self._h, float(endtime), C.byref(ran)))
+        return bool(ran.value)
+
+    def run(self, endtime=1e300, nsteps=(1 << 62)):
+        n = C.c_int64()
+        self._c(lib().bx_run(self._h, float(endtime), int(nsteps), C.byref(n)))
+        return n.value
+
+    def status(self):
+        bits = C.c_uint32()
+        path = C.c_int32()
+        self._c(lib().bx_status(self._h, C.byref(bits), C.byref(path)))
+        return bits.value, path.value
+
+
+def ghost_plan(params: HydroParams, phase_only=False):
+    """The ghost-fill plan of a grid (host only, no GPU): dict of arrays."""
+    p = make_params(params, _lib.FLAG_PHASE_ONLY if phase_only else 0)
+    n = C.c_int64(0)
+    ok = C.c_int32(0)
+    check(lib().bx_ghost_plan(C.byref(p), C.byref(n), None, None, None, None, None,
+                              C.byref(ok)))
+    k = n.value
+    out = dict(dst=np.empty(k, np.int32), src1=np.empty(k, np.int32), sgn1=np.empty(k, np.uint8),
+               src2=np.empty(k, np.int32), sgn2=np.empty(k, np.uint8))
+    vp = lambda a: a.ctypes.data_as(C.c_void_p)
+    check(lib().bx_ghost_plan(C.byref(p), C.byref(n), vp(out["dst"]), vp(out["src1"]),
+                              vp(out["sgn1"]), vp(out["src2"]), vp(out["sgn2"]), C.byref(ok)))
+    out["fused_ok"] = bool(ok.value)
+    return out
+
+
+def apply_ghost_plan(cons, src, sgn, dst):
+    """Apply a plan to a (ng,5) array on the host (gather then scatter)."""
+    vals = cons[src].copy()
+    for b, k in ((1, 1), (2, 2), (4, 3)):
+        m = (sgn & b) != 0
+        vals[m, k] = -vals[m, k]
+    out = cons.copy()
+    out[dst] = vals
+    return out
+
+
+__all__ = ["Hydro", "BoxzyError", "ghost_plan", "apply_ghost_plan"]

@@ -1,0 +1,153 @@
+/*
+ * boxzy_gpu.h -- C ABI of the B200 (sm_100a) FP64 hydrodynamic step of BOXZYHYDRO.
+ *
+ * The reference has no plugin or FFI API: its hot path is a set of argument-less
+ * Fortran subroutines that share module arrays (grid_commons.f90:11-24) and are
+ * called from the main time loop (main.f90:211-555).  Each entry point below
+ * replaces one of those subroutines (cited beside it) or the whole loop body,
+ * with the module arrays held in device memory by an opaque handle.
+ *
+ * Conventions
+ *  - Every function returns an int status: BX_OK (0) or a BX_ERR_* code; the
+ *    message of the last error is bx_last_error(h).  No C++ exception crosses
+ *    this boundary.
+ *  - Host arrays use the reference layout: cons(5,ngrid), u(3,ngrid) and
+ *    p(ngrid), Fortran column-major, i.e. 5 (resp. 3, 1) doubles per cell, cells
+ *    in igrid order (ix fastest).  A Fortran caller passes its allocatable
+ *    arrays directly.
+ *  - Calls on one handle are single-threaded (outside OpenMP parallel regions or
+ *    under !$OMP MASTER).  Each handle owns one CUDA stream unless one is given.
+ *  - Only the fixed-gamma EOS (H2STAT=-1) and Cartesian fluxing
+ *    (fluxangmom=.false.) are supported; other settings return
+ *    BX_ERR_UNSUPPORTED from bx_create.
+ */
+#ifndef BOXZY_GPU_H
+#define BOXZY_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define BX_OK 0
+#define BX_ERR_ARG 1          /* bad argument or size */
+#define BX_ERR_CUDA 2         /* CUDA runtime error */
+#define BX_ERR_UNSUPPORTED 3  /* configuration outside the GPU path */
+#define BX_ERR_STATE 4        /* non-finite state or zero HLL wave speed */
+#define BX_ERR_NOMEM 5        /* device allocation failed */
+
+/* status bits reported by bx_status */
+#define BX_STATUS_VLIMIT 1u     /* velocity limiter fired (velocity.f90:122-139) */
+#define BX_STATUS_LOWRHO 2u     /* low-density EOS branch taken (state.f90:52-56) */
+#define BX_STATUS_NONFINITE 4u  /* NaN or Inf produced */
+#define BX_STATUS_ZEROWAVE 8u   /* ap+am == 0 at a face (flux.f90:588) */
+
+/* bx_params.flags */
+#define BX_FLAG_PHASE_ONLY 1    /* always run the per-phase kernels, never the fused stages */
+
+typedef struct bx_params {
+  int32_t nx, ny, nz;     /* grid_params nx,ny,nz: cells incl. two ghost layers per side
+                             (z ghosts only when nz>=6), init_grid.f90:18,76-107 */
+  int32_t h2stat;         /* eos_input H2STAT; must be -1 (state.f90:49-59) */
+  double dx, dy, dz;      /* grid_params dx,dy,dz */
+  double cfl;             /* hydro cfl (courant.f90:182) */
+  double small_rho;       /* hydro small_rho (flux.f90:225) */
+  double small_eps;       /* hydro small_eps */
+  double vlimit;          /* hydro vlimit (velocity.f90:122) */
+  double gammafix;        /* eos_input gammafix */
+  double muc;             /* mean molecular weight, eos.f90:144 */
+  double rgas;            /* scale%rgas of get_units, units.f90:17 */
+  int32_t no_outflow[6];  /* grid_params no_outflow_xl,xr,yl,yr,zl,zr (reflective walls) */
+  int32_t fluxangmom;     /* grid_params fluxangmom; must be 0 */
+  int32_t flags;          /* BX_FLAG_* */
+} bx_params;
+
+typedef struct bx_handle bx_handle;
+
+/* Library version string. */
+const char *bx_version(void);
+
+/* Allocate one grid on the current CUDA device and build its ghost tables.
+ * Replaces init_grid (init_grid.f90:7-265) and the allocation of the module
+ * arrays of grid_commons.f90:11-24. */
+int bx_create(const bx_params *params, bx_handle **out);
+
+/* Free all device memory of the handle (cleanup.f90:1-16). */
+int bx_destroy(bx_handle *h);
+
+/* Run all work of the handle on the given cudaStream_t (NULL = own stream). */
+int bx_set_stream(bx_handle *h, void *cuda_stream);
+
+/* Copy the reference's state arrays in: cons(5,ngrid), u(3,ngrid), p(ngrid), as left by
+ * init_conditions (init_conditions.f90:26-77) or read_hydro (read_hydro.f90:122-160).
+ * adindx is set to gammafix everywhere (the value state() gives it).  u or p may be
+ * NULL, meaning zero. */
+int bx_upload(bx_handle *h, const double *cons, const double *u, const double *p);
+
+/* Copy the state arrays out (what write_files.f90:55-63 writes after state()).
+ * Any pointer may be NULL. */
+int bx_download(bx_handle *h, double *cons, double *u, double *p);
+
+/* The main-loop clock of main.f90:102,196-199: time, dtold and step. */
+int bx_set_clock(bx_handle *h, double time, double dtold, int64_t step);
+int bx_get_clock(bx_handle *h, double *time, double *dt, double *dtold, int64_t *step);
+
+/* One iteration of the main loop body (main.f90:212-545 with default flags:
+ * state, courant, dt control, half-dt source, two flux stages of SSP-RK2, half-dt
+ * source).  If time >= endtime the loop would have exited: nothing runs and
+ * *ran = 0 (ran may be NULL). */
+int bx_step(bx_handle *h, double endtime, int32_t *ran);
+
+/* Repeat bx_step until time >= endtime or nsteps steps ran. */
+int bx_run(bx_handle *h, double endtime, int64_t nsteps, int64_t *steps_taken);
+
+/* Per-phase entry points on the handle's module arrays, for bisection against the
+ * reference.  They act exactly like the subroutines they replace. */
+int bx_state(bx_handle *h);                /* state.f90:6-89 (H2STAT=-1 branch) */
+int bx_velocity(bx_handle *h);             /* velocity.f90:93-153 */
+int bx_courant(bx_handle *h, double *dt);  /* courant.f90:157-192; sets and returns dt */
+int bx_source(bx_handle *h, int32_t siter);/* source.f90:5-205 (gravity coupling via gforce) */
+int bx_ghost(bx_handle *h);                /* utils.f90:305-480 set_ghost_cells */
+int bx_flux(bx_handle *h, int32_t avg);    /* flux.f90:6-235 */
+int bx_avisc(bx_handle *h);                /* avisc.f90:197-219: never called by the reference
+                                              and its result qq is never read; a no-op */
+int bx_save_cons_old(bx_handle *h);        /* main.f90:327-333 */
+int bx_set_dt(bx_handle *h, double dt);    /* the module variable dt (grid_commons.f90:12) */
+
+/* Gravitational acceleration gforce(3,ngrid) consumed by source() (source.f90:161-182);
+ * NULL restores the zero force of a run without a gravity solver. */
+int bx_set_gforce(bx_handle *h, const double *gforce);
+
+/* Status bits accumulated since the last call (BX_STATUS_*) and the path the
+ * last step took (0 = per-phase kernels, 1 = fused stage kernels). */
+int bx_status(bx_handle *h, uint32_t *status_bits, int32_t *last_path);
+
+/* Device pointers of the current conserved planes (5 x ngrid doubles, SoA) for
+ * zero-copy users; valid until the next call on the handle. */
+int bx_device_cons(bx_handle *h, double **cons_soa, int64_t *ngrid);
+
+/* Timing hooks: with profiling on, every fused step records CUDA events around
+ * its two stage kernels on the handle's stream; bx_profile_read returns the
+ * accumulated stage times (ms), the number of fused steps timed and the number
+ * of this library's kernels launched since bx_profile was called. */
+int bx_profile(bx_handle *h, int32_t enable);
+int bx_profile_read(bx_handle *h, double *ms_stage0, double *ms_stage1, int64_t *fused_steps,
+                    int64_t *launches);
+
+/* Host-only query (no GPU needed): the ghost-fill plan bx_create builds for a grid.
+ * For each ghost cell in index order: dst = cell, src1/sgn1 = source cell and
+ * momentum sign mask (bit0 m1, bit1 m2, bit2 m3 negated) of one set_ghost_cells
+ * sweep (utils.f90:305-480) with all sources read before the sweep; src2/sgn2 =
+ * the same for two consecutive sweeps.  Call with dst==NULL to get *nghost;
+ * *fused_ok is 1 when the fused stage kernels can run on this grid. */
+int bx_ghost_plan(const bx_params *params, int64_t *nghost, int32_t *dst, int32_t *src1,
+                  uint8_t *sgn1, int32_t *src2, uint8_t *sgn2, int32_t *fused_ok);
+
+/* Message of the last error on the handle (or of the last failed bx_create when h is NULL). */
+const char *bx_last_error(bx_handle *h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* BOXZY_GPU_H */

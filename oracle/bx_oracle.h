@@ -1,0 +1,88 @@
+/*
+ * bx_oracle.h -- CPU restatement of BOXZYHYDRO's fixed-gamma hydrodynamic step.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This library is the checker for the CUDA path
+ * (tests/, __graft_entry__.smoke() and the cpu_baseline leg of bench.py use it);
+ * the product never links or calls it.
+ *
+ * Parity status: the reference (Fortran 95, gfortran) cannot be compiled in
+ * this image (no Fortran front end), so per-step parity of this restatement is
+ * NOT pinned by a reference binary.  End states are pinned against the
+ * reference's own golden files (analysis/sod.ana exact Sod solution and
+ * analysis/sodtest.dat reference output) by tests/test_oracle_golden.py.
+ *
+ * Every routine follows the reference file:line given in bx_oracle.c, in the
+ * same evaluation order, compiled with -ffp-contract=off (no FMA contraction,
+ * no reassociation), which is how gfortran -O3 evaluates the same expressions
+ * on x86-64 without -march (SSE2, no FMA instructions).
+ *
+ * Layout follows the reference exactly: cons(5,ngrid) column-major = AoS with
+ * 5 doubles per cell, u(3,ngrid) AoS, p/adindx/muc_array(ngrid); cell index
+ * igrid = ix + (iy-1)*nx + (iz-1)*nx*ny (1-based in Fortran, 0-based here).
+ */
+#ifndef BX_ORACLE_H
+#define BX_ORACLE_H
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct ox_params {
+  int32_t nx, ny, nz;
+  int32_t h2stat;          /* only -1 (fixed gamma) is supported */
+  double dx, dy, dz;
+  double cfl, small_rho, small_eps, vlimit, gammafix;
+  double muc, rgas;        /* eos.f90:144 and units.f90:17 */
+  int32_t no_outflow[6];   /* xl, xr, yl, yr, zl, zr (parameters.f90:32-37) */
+  int32_t racy_ghosts;     /* 1: parallel ghost loop like the reference (timing only) */
+  int32_t pad;
+} ox_params;
+
+typedef struct ox_sim ox_sim;
+
+ox_sim *ox_create(const ox_params *p);
+void ox_destroy(ox_sim *s);
+int64_t ox_ngrid(const ox_sim *s);
+int64_t ox_nghost(const ox_sim *s);
+void ox_grid_info(const ox_sim *s, int32_t *boundary, int32_t *ineigh6);
+void ox_ghost_list(const ox_sim *s, int64_t *idx);
+
+/* state arrays (reference layout) */
+void ox_set_state(ox_sim *s, const double *cons5, const double *u3, const double *p,
+                  const double *adindx);
+void ox_get_state(const ox_sim *s, double *cons5, double *u3, double *p, double *adindx);
+void ox_set_gforce(ox_sim *s, const double *g3);
+void ox_get_cons_old(const ox_sim *s, double *cons5);
+void ox_set_cons_old(ox_sim *s, const double *cons5);
+
+/* clock: time, dt, dtold and step of main.f90 */
+void ox_set_clock(ox_sim *s, double time, double dt, double dtold, int64_t step);
+void ox_get_clock(const ox_sim *s, double *time, double *dt, double *dtold, int64_t *step,
+                  double *dtrate);
+
+/* phases (argument-less subroutines of the reference, acting on the arrays) */
+void ox_state(ox_sim *s);
+void ox_velocity(ox_sim *s);
+void ox_courant(ox_sim *s);
+void ox_source(ox_sim *s, int siter);
+void ox_set_ghost_cells(ox_sim *s);
+void ox_flux(ox_sim *s, int avg);
+void ox_save_cons_old(ox_sim *s);
+
+/* one iteration of the main loop (main.f90:212-545); returns 0 if it ran,
+ * 1 if the loop would have exited (time>=endtime). */
+int ox_step(ox_sim *s, double endtime);
+/* run until time>=endtime or nsteps steps were taken; returns steps taken */
+int64_t ox_run(ox_sim *s, double endtime, int64_t nsteps);
+
+void ox_set_threads(int n);
+
+/* constants of the reference's units module and EOS */
+double ox_rgas_code_units(void);   /* units.f90:10-17 */
+double ox_muc(double xabun, double yabun, double zabun, double mu_z); /* eos.f90:144 */
+
+#ifdef __cplusplus
+}
+#endif
+#endif
