@@ -1,0 +1,358 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 hydro step: FP64 cell-updates/s on the 256^3 turbulent box.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--n 256]
+
+One step is one full iteration of the reference's main loop (state, courant,
+dt control, half-dt source, two SSP-RK2 flux stages, half-dt source) over a
+256^3-interior box (260^3 cells with ghosts) with a seeded lognormal density,
+uniform pressure and solenoidal Mach-1 velocity, gamma=5/3, CFL 0.4, outflow
+walls (synthetic input, no dataset).  The unit of work is one interior cell
+advanced one step.
+
+ours: K steps timed with CUDA events on the library's stream after W warm-up
+steps, barrier and synchronize on both sides, max over ranks.  Under torchrun
+every rank advances its own replica of the box (the step has no exchange; the
+reference runs on one node's shared memory), so value = ranks x cells x K / t.
+The JSON line also carries the end-to-end figure through the C ABI with host
+arrays (upload of cons/u/p from pinned memory, step, download every step), the
+HBM roofline of the dominant stage kernel, the FP64 roofline, nvidia-smi clocks
+sampled during the timed region and the oracle timed on the host cores.
+
+reference: the reference's algorithm on the CPU (oracle/bx_oracle.c, a
+line-by-line C restatement of the Fortran, OpenMP on all host cores, ghost loop
+parallel like the reference's) on a bounded sample of the same workload; rank 0
+only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "FP64 cell-updates/s"
+UNIT = "cell-updates/s"
+FALLBACK_HBM = 6650.0
+
+
+def env_int(k, d):
+    try:
+        return int(os.environ.get(k, d))
+    except ValueError:
+        return d
+
+
+def measured_hbm():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "200", "-i", str(self.gpu)],
+                stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        out = {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        if self.proc is None:
+            return out
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        sm, mx, reasons = [], [], set()
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        os.unlink(self.path)
+        if sm:
+            out.update(sm_mhz=statistics.median(sm), sm_max_mhz=max(mx), samples=len(sm),
+                       reasons=sorted(reasons))
+        return out
+
+
+def cpu_sample(st, steps=3, threads=None):
+    """The oracle (reference algorithm, OpenMP) on `steps` steps of the state."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    threads = threads or os.cpu_count()
+    O.set_threads(threads)
+    o = O.Oracle(st.params, racy_ghosts=True)
+    o.set_state(st.cons, st.u, st.p, st.adindx)
+    o.step()  # warm-up (first touch of every array)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        o.step()
+    dt = time.perf_counter() - t0
+    o.close()
+    cells = st.params.n_active()
+    return cells * steps / dt, threads, dt
+
+
+def reference_arm(args, rank):
+    if rank != 0:
+        return 0
+    from boxzyhydro_b200 import ic
+    n = args.ref_n
+    st = ic.turbulent_box(n=n, seed=args.seed)
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    threads = os.cpu_count()
+    O.set_threads(threads)
+    o = O.Oracle(st.params, racy_ghosts=True)
+    o.set_state(st.cons, st.u, st.p, st.adindx)
+    for _ in range(args.warmup):
+        o.step()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        o.step()
+    dt = time.perf_counter() - t0
+    cells = st.params.n_active()
+    value = cells * args.steps / dt
+    sample = (f"{n}^3-interior box of the same turbulent workload ({cells} cells), "
+              f"{args.steps} steps after {args.warmup} warm-up, C restatement of the "
+              "reference loop (oracle/bx_oracle.c), OpenMP, parallel ghost loop")
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "impl": "reference", "n_gpus": 0,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"turbulent box {n}^3 interior (sample of the 256^3 workload), "
+                               "gamma=5/3, CFL 0.4, outflow walls", "cells_per_step": cells},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                         "sample": sample},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=256)
+    ap.add_argument("--ref-n", type=int, default=128, dest="ref_n")
+    ap.add_argument("--seed", type=int, default=1234)
+    ap.add_argument("--e2e-steps", type=int, default=10, dest="e2e_steps")
+    ap.add_argument("--cpu-steps", type=int, default=2, dest="cpu_steps")
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+
+    rank = env_int("RANK", 0)
+    world = env_int("WORLD_SIZE", 1)
+    local = env_int("LOCAL_RANK", 0)
+    if args.impl == "reference":
+        return reference_arm(args, rank)
+
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    from boxzyhydro_b200 import ic
+    from boxzyhydro_b200.hydro import Hydro, fp64_peak
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    st = ic.turbulent_box(n=args.n, seed=args.seed)
+    hp = st.params
+    cells = hp.n_active()
+    g = Hydro(hp)
+    stream = torch.cuda.Stream()
+    g.set_stream(stream.cuda_stream)
+    g.upload_state(st)
+    for _ in range(args.warmup):
+        g.step()
+
+    # ---- device-timed steps
+    g.profile(True)
+    sampler = ClockSampler(local)
+    barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        g.step()
+    e1.record(stream)
+    e1.synchronize()
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    barrier()
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    prof = g.profile_read()
+    bits, path = g.status()
+    value = world * cells * args.steps / (ms * 1e-3)
+
+    # ---- roofline of the dominant stage kernel
+    hbm, hbm_src = measured_hbm()
+    fsteps = max(prof["fused_steps"], 1)
+    t0 = prof["ms_stage0"] / fsteps
+    t1 = prof["ms_stage1"] / fsteps
+    dom = 1 if t1 >= t0 else 0
+    tdom = max(t0, t1)
+    alg_bytes = 80.0 * cells  # 5 FP64 conserved fields read once and written once per pass
+    achieved = alg_bytes / (tdom * 1e-3) / 1e9 if tdom > 0 else None
+    traffic = None
+    tr_path = os.path.join(ROOT, "profiles", "stage_traffic.json")
+    if os.path.exists(tr_path):
+        try:
+            tr = json.load(open(tr_path))
+            traffic = tr[f"stage{dom}_bytes_per_cell"] * cells
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": (achieved / hbm) if achieved else None, "traffic": traffic,
+                "kernel": f"k_stage<{dom}> (stage {dom} of SSP-RK2)",
+                "ms_per_launch": tdom, "peak_source": f"{hbm_src} hbm_gbs",
+                "alg_bytes_per_launch": alg_bytes}
+    fp64 = None
+    try:
+        peak64 = fp64_peak()
+        fl_path = os.path.join(ROOT, "profiles", "stage_flops.json")
+        if os.path.exists(fl_path):
+            fl = json.load(open(fl_path))
+            flops = fl[f"stage{dom}_fp64_flops_per_cell"] * cells
+            ach = flops / (tdom * 1e-3) / 1e12
+            fp64 = {"bound": "fp64", "achieved": ach, "peak": peak64, "unit": "TFLOP/s",
+                    "frac": ach / peak64, "peak_source": "measured DFMA probe (bx_fp64_peak)",
+                    "flops_source": "ncu executed FP64 instructions per launch"}
+        else:
+            fp64 = {"bound": "fp64", "peak": peak64, "unit": "TFLOP/s"}
+    except Exception as e:  # noqa: BLE001
+        fp64 = {"error": str(e)}
+
+    # ---- end to end through the C ABI with host arrays
+    e2e = None
+    if not args.no_e2e:
+        ng = hp.ngrid
+        hc = torch.empty((ng, 5), dtype=torch.float64, pin_memory=True).numpy()
+        hu = torch.empty((ng, 3), dtype=torch.float64, pin_memory=True).numpy()
+        hpp = torch.empty((ng,), dtype=torch.float64, pin_memory=True).numpy()
+        c, u, p = g.download()
+        hc[:] = c
+        hu[:] = u
+        hpp[:] = p
+        del c, u, p
+        barrier()
+        torch.cuda.synchronize()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        for _ in range(args.e2e_steps):
+            g.upload(hc, hu, hpp)
+            g.step()
+            g._c(__import__("boxzyhydro_b200")._lib.lib().bx_download(
+                g._h, hc.ctypes.data, hu.ctypes.data, hpp.ctypes.data))
+        a1.record(stream)
+        a1.synchronize()
+        ems = a0.elapsed_time(a1)
+        if world > 1:
+            t = torch.tensor([ems], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            ems = float(t.item())
+        bytes_io = ng * 9 * 8
+        e2e = {"value": world * cells * args.e2e_steps / (ems * 1e-3), "unit": UNIT,
+               "h2d_bytes_per_step": bytes_io, "d2h_bytes_per_step": bytes_io,
+               "steps": args.e2e_steps, "ms_per_step": ems / args.e2e_steps,
+               "api": "bx_upload(cons,u,p) + bx_step + bx_download(cons,u,p), pinned host"}
+
+    # ---- CPU baseline (rank 0, one GPU only)
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        v, thr, secs = cpu_sample(st, steps=args.cpu_steps)
+        cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
+               "sample": f"{args.cpu_steps} steps of the same {args.n}^3 workload after one "
+                         f"warm-up step ({secs:.1f} s), oracle/bx_oracle.c (C restatement of "
+                         "the reference loop), OpenMP on all host threads"}
+
+    g.close()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": f"turbulent box {args.n}^3 interior "
+                                   f"({hp.nx}x{hp.ny}x{hp.nz} with ghosts), lognormal rho "
+                                   "sigma_ln=0.5, solenoidal Mach-1 v, p=1, gamma=5/3, "
+                                   "CFL 0.4, outflow walls",
+                       "cells_per_step": cells, "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (3 x 5 planes x 8 B x "
+                             f"{hp.ngrid} cells = {3 * 40 * hp.ngrid / 1e9:.1f} GB)"},
+            "clocks": clocks,
+            "roofline": roofline,
+            "roofline_fp64": fp64,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "gpu_launches": prof["launches"],
+            "path": "fused stage kernels" if path == 1 else "per-phase kernels",
+            "status_bits": bits,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -78,6 +78,9 @@ def lib():
         "bx_status": (C.c_int, [H, C.POINTER(C.c_uint32), i32p]),
         "bx_device_cons": (C.c_int, [H, C.POINTER(C.c_void_p), i64p]),
         "bx_ghost_plan": (C.c_int, [C.POINTER(BxParams), i64p, vp, vp, vp, vp, vp, i32p]),
+        "bx_profile": (C.c_int, [H, C.c_int32]),
+        "bx_profile_read": (C.c_int, [H, dp, dp, i64p, i64p]),
+        "bx_fp64_peak": (C.c_int, [dp, dp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -144,6 +144,16 @@ class Hydro:
         self._c(lib().bx_run(self._h, float(endtime), int(nsteps), C.byref(n)))
         return n.value
 
+    def profile(self, enable=True):
+        """Start (or stop) CUDA-event timing of the fused stage kernels."""
+        self._c(lib().bx_profile(self._h, 1 if enable else 0))
+
+    def profile_read(self):
+        a, b = C.c_double(), C.c_double()
+        n, k = C.c_int64(), C.c_int64()
+        self._c(lib().bx_profile_read(self._h, C.byref(a), C.byref(b), C.byref(n), C.byref(k)))
+        return dict(ms_stage0=a.value, ms_stage1=b.value, fused_steps=n.value, launches=k.value)
+
     def status(self):
         bits = C.c_uint32()
         path = C.c_int32()
@@ -179,4 +189,11 @@ def apply_ghost_plan(cons, src, sgn, dst):
     return out
 
 
-__all__ = ["Hydro", "BoxzyError", "ghost_plan", "apply_ghost_plan"]
+def fp64_peak():
+    """Measured FP64 FMA throughput of the current device (TFLOP/s)."""
+    t, ms = C.c_double(), C.c_double()
+    check(lib().bx_fp64_peak(C.byref(t), C.byref(ms)))
+    return t.value
+
+
+__all__ = ["Hydro", "BoxzyError", "ghost_plan", "apply_ghost_plan", "fp64_peak"]

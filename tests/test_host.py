@@ -20,7 +20,7 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 def header_functions():
     names = []
-    for hdr in ("boxzy_gpu.h",):
+    for hdr in ("boxzy_gpu.h", "boxzy_diag.h"):
         text = open(os.path.join(ROOT, "include", hdr)).read()
         text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
         names += re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(bx_\w+)\s*\(", text, flags=re.M)
