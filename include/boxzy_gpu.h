@@ -144,6 +144,23 @@ int bx_profile_read(bx_handle *h, double *ms_stage0, double *ms_stage1, int64_t 
 int bx_ghost_plan(const bx_params *params, int64_t *nghost, int32_t *dst, int32_t *src1,
                   uint8_t *sgn1, int32_t *src2, uint8_t *sgn2, int32_t *fused_ok);
 
+/* No counterpart in the reference.  One set_ghost_cells sweep -- the same result as
+ * bx_ghost -- that allocates nothing, for callers that cannot allocate device memory
+ * (a host program that has reserved the device's memory for its own pool, or a
+ * runtime held to a fixed device-memory budget).  The caller passes device memory it
+ * owns: the conserved planes cons_soa (5 x ngrid doubles, SoA, updated in place) and
+ * the sweep plan dst/src/sgn of bx_ghost_plan (src1, sgn1).  The gather scratch is a
+ * static device array of BX_NOALLOC_MAX_GHOSTS x 5 doubles (40 MiB) that every GPU
+ * loading the library holds until exit; larger nghost is rejected with BX_ERR_ARG.
+ * The first call on a device looks up that array's device address (make it before
+ * any stream capture); calls that overlap on the GPU race on the shared array.
+ * Errors are reported by bx_noalloc_last_error. */
+#define BX_NOALLOC_MAX_GHOSTS 1048576
+int bx_ghost_fill_noalloc(double *cons_soa, int64_t ngrid, const int32_t *dst,
+                          const int32_t *src, const uint8_t *sgn, int64_t nghost,
+                          void *cuda_stream);
+const char *bx_noalloc_last_error(void);
+
 /* Message of the last error on the handle (or of the last failed bx_create when h is NULL). */
 const char *bx_last_error(bx_handle *h);
 
