@@ -81,6 +81,8 @@ def lib():
         "bx_profile": (C.c_int, [H, C.c_int32]),
         "bx_profile_read": (C.c_int, [H, dp, dp, i64p, i64p]),
         "bx_fp64_peak": (C.c_int, [dp, dp]),
+        "bx_check_shared_division": (C.c_int, [C.c_ulonglong, C.c_ulonglong, C.c_int,
+                                               C.POINTER(C.c_ulonglong), dp, dp]),
         "bx_ghost_fill_noalloc": (C.c_int, [vp, C.c_int64, vp, vp, vp, C.c_int64, vp]),
         "bx_noalloc_last_error": (C.c_char_p, []),
     }

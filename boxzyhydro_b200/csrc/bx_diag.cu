@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include "../../include/boxzy_diag.h"
+#include "bx_math.cuh"
 
 namespace {
 constexpr int kChains = 8;
@@ -22,6 +23,62 @@ __global__ void __launch_bounds__(256) k_dfma(double* out, double seed) {
   if (s == 1234.5678) out[0] = s;  // keeps the chains live
 }
 }  // namespace
+
+namespace {
+// splitmix64 stream -> doubles with random mantissa and exponent in [-e, e]
+__device__ __forceinline__ unsigned long long mix(unsigned long long z) {
+  z += 0x9e3779b97f4a7c15ull;
+  z = (z ^ (z >> 30)) * 0xbf58476d1ce4e5b9ull;
+  z = (z ^ (z >> 27)) * 0x94d049bb133111ebull;
+  return z ^ (z >> 31);
+}
+__device__ __forceinline__ double rnd(unsigned long long z, int erange, bool sign) {
+  const unsigned long long mant = z & 0xfffffffffffffull;
+  const int ex = (int)((z >> 52) % (2 * erange + 1)) - erange;
+  unsigned long long bits = mant | ((unsigned long long)(ex + 1023) << 52);
+  if (sign && ((z >> 63) & 1)) bits |= 1ull << 63;
+  return __longlong_as_double((long long)bits);
+}
+__global__ void k_divcheck(unsigned long long n, unsigned long long seed, int erange,
+                           unsigned long long* bad, double* example) {
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  for (unsigned long long i = blockIdx.x * (unsigned long long)blockDim.x + threadIdx.x; i < n;
+       i += stride) {
+    const unsigned long long z1 = mix(seed ^ (2 * i)), z2 = mix(seed ^ (2 * i + 1));
+    const double d = rnd(z1, erange, false);
+    double a = rnd(z2, erange, true);
+    if ((i & 7) == 0) a = d * (double)(long long)(z2 % 1000003ull);  // exact multiples
+    if ((i & 15) == 1) a = __longlong_as_double(__double_as_longlong(d) + (long long)(z2 % 5) - 2);
+    const bx::SharedDiv div(d);
+    const double q = div(a), ref = a / d;
+    if (__double_as_longlong(q) != __double_as_longlong(ref) && !(q == 0.0 && ref == 0.0)) {
+      if (atomicAdd(bad, 1ull) == 0) { example[0] = a; example[1] = d; }
+    }
+  }
+}
+}  // namespace
+
+extern "C" int bx_check_shared_division(unsigned long long n, unsigned long long seed,
+                                         int exp_range, unsigned long long* mismatches,
+                                         double* example_a, double* example_d) {
+  unsigned long long* bad = nullptr;
+  double* ex = nullptr;
+  if (cudaMalloc(&bad, sizeof(unsigned long long)) != cudaSuccess) return 5;
+  if (cudaMalloc(&ex, 2 * sizeof(double)) != cudaSuccess) { cudaFree(bad); return 5; }
+  cudaMemset(bad, 0, sizeof(unsigned long long));
+  cudaMemset(ex, 0, 2 * sizeof(double));
+  k_divcheck<<<1184, 256>>>(n, seed, exp_range, bad, ex);
+  unsigned long long h = 0;
+  double hx[2] = {0, 0};
+  cudaMemcpy(&h, bad, sizeof(h), cudaMemcpyDeviceToHost);
+  cudaMemcpy(hx, ex, sizeof(hx), cudaMemcpyDeviceToHost);
+  cudaFree(bad);
+  cudaFree(ex);
+  if (mismatches) *mismatches = h;
+  if (example_a) *example_a = hx[0];
+  if (example_d) *example_d = hx[1];
+  return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
 
 extern "C" int bx_fp64_peak(double* tflops, double* ms_out) {
   int dev = 0, sms = 0;

@@ -78,7 +78,7 @@ __device__ __forceinline__ void apply_sources(Cons& c, int nsrc, double small_ep
 //           with the stage-0 velocity m0/rho0 (main.f90:353 uses the stale u).
 template <int STAGE>
 __device__ __forceinline__ Prim load_prim(const StageArgs& a, const Geom& g, int x, int y, int z,
-                                          unsigned& flags) {
+                                          unsigned& flags, bool need_c = true) {
   const long long PS = a.ncells_total;
   Prim q;
   if (STAGE == 0) {
@@ -101,7 +101,8 @@ __device__ __forceinline__ Prim load_prim(const StageArgs& a, const Geom& g, int
     q.e = recon_eps(q.d, c1.E, q.u1, q.u2, q.u3, g.small_eps);
     q.p = eos_pressure(q.d, c1.E, s1, s2, s3, g.gm1, g.small_eps);
   }
-  q.c = sqrt(q.p * g.gam / q.d);
+  // the sound speed enters only the lambdas of cells whose face states are built
+  q.c = need_c ? sqrt(q.p * g.gam / q.d) : 0.0;
   if (q.d < kLowRho) flags |= kFlagLowRho;
   if (fabs(q.u1) > g.vlimit || fabs(q.u2) > g.vlimit || fabs(q.u3) > g.vlimit)
     flags |= kFlagVlimit;
@@ -183,30 +184,23 @@ __device__ __forceinline__ double warp_max(double v) {
 }  // namespace
 
 // ------------------------------------------------------------------ stage kernel
-template <int STAGE, bool POW2, bool THREED>
-__global__ void __launch_bounds__(TX* TY, 2) k_stage(StageArgs a) {
-  extern __shared__ double sm[];
+// One tile of one stage.  FULL: the tile is a whole 32x8 block of interior
+// columns, so its extents are compile-time constants.
+template <int STAGE, bool POW2, bool THREED, bool FULL>
+__device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, const Geom& g,
+                                           Ctrl* C, double* sm, double* red_rate,
+                                           unsigned* red_flags) {
   double* SP = sm;                    // [7][TY+4][TX+4] primitives of the plane
   double* SX = sm + 7 * NP;           // [12][TY][TX+2] x states (minus 0..5, plus 6..11)
   double* SY = SX + 12 * NSX;         // [12][TY+2][TX] y states
   double* FX = sm;                    // [5][TY][TX+1] x face fluxes (aliases SP)
   double* FY = sm + 5 * NFX;          // [5][TY+1][TX] y face fluxes
-  __shared__ Geom sg;
-  __shared__ double red_rate[TX * TY / 32];
-  __shared__ unsigned red_flags[TX * TY / 32];
-
-  const Tile t = a.tiles[blockIdx.x];
-  if (threadIdx.x == 0) sg = a.geom[t.box];
-  __syncthreads();
-  const Geom& g = sg;
-  Ctrl* C = a.ctrl + t.box;
-  if (!C->active) return;
   const double dt = C->dt;
 
   const int tid = threadIdx.x;
   const int tx = tid % TX, ty = tid / TX;
   const int NAx = g.ax1 - g.ax0, NAy = g.ay1 - g.ay0;
-  const int w = min(TX, NAx - t.x0), h = min(TY, NAy - t.y0);
+  const int w = FULL ? TX : min(TX, NAx - t.x0), h = FULL ? TY : min(TY, NAy - t.y0);
   const bool own = (tx < w) && (ty < h);
   const int bx0 = g.ax0 + t.x0, by0 = g.ay0 + t.y0;  // full-grid tile origin
   const int gx = bx0 + tx, gy = by0 + ty;
@@ -265,7 +259,11 @@ __global__ void __launch_bounds__(TX* TY, 2) k_stage(StageArgs a) {
         const int j = k / w;
         cy = j < 2 ? j - 2 : h + (j - 2);
       }
-      const Prim q = load_prim<STAGE>(a, g, bx0 + cx, by0 + cy, z, flags);
+      // cells two away from the tile only feed slopes; ghost cells need no lambda
+      const int fx = bx0 + cx, fy = by0 + cy;
+      const bool near = cx >= -1 && cx <= w && cy >= -1 && cy <= h;
+      const bool inner = fx >= g.ax0 && fx < g.ax1 && fy >= g.ay0 && fy < g.ay1;
+      const Prim q = load_prim<STAGE>(a, g, fx, fy, z, flags, near && inner);
       put_prim(SP, (cy + 2) * PW + (cx + 2), q);
     }
     if (THREED && own) {
@@ -417,6 +415,24 @@ __global__ void __launch_bounds__(TX* TY, 2) k_stage(StageArgs a) {
     if (f) atomicOr(&C->flags, f);
     if (STAGE == 1) atomicMax(&C->rate_bits, (unsigned long long)__double_as_longlong(r));
   }
+}
+
+template <int STAGE, bool POW2, bool THREED>
+__global__ void __launch_bounds__(TX* TY, 2) k_stage(StageArgs a) {
+  extern __shared__ double sm[];
+  __shared__ Geom sg;
+  __shared__ double red_rate[TX * TY / 32];
+  __shared__ unsigned red_flags[TX * TY / 32];
+  const Tile t = a.tiles[blockIdx.x];
+  if (threadIdx.x == 0) sg = a.geom[t.box];
+  __syncthreads();
+  Ctrl* C = a.ctrl + t.box;
+  if (!C->active) return;
+  const bool full = (t.x0 + TX <= sg.ax1 - sg.ax0) && (t.y0 + TY <= sg.ay1 - sg.ay0);
+  if (full)
+    stage_tile<STAGE, POW2, THREED, true>(a, t, sg, C, sm, red_rate, red_flags);
+  else
+    stage_tile<STAGE, POW2, THREED, false>(a, t, sg, C, sm, red_rate, red_flags);
 }
 
 template <int STAGE, bool POW2, bool THREED>

@@ -138,6 +138,33 @@ BX_HD void ghost_states(const Prim& q, FaceState& mi, FaceState& pl) {
   pl = mi;
 }
 
+// a/d for several numerators sharing one denominator d > 0.  With r the
+// correctly rounded reciprocal of d, q0 = RN(a*r) is within one ulp of a/d and
+// the residual a - d*q0 is exact under a fused multiply-add, so
+// RN(q0 + (a - d*q0)*r) is the correctly rounded quotient (Markstein's
+// theorem, as used for IEEE division on FMA hardware).  The theorem needs the
+// quotient and the residual away from the overflow and subnormal ranges:
+// with d and |a| in [2^-450, 2^450] the quotient lies in [2^-900, 2^900] and
+// the residual (about |a|*2^-53) stays normal.  Outside that window (and for
+// a = 0) the IEEE division is taken instead.
+struct SharedDiv {
+  double d, r;
+  bool ok;
+  __device__ __forceinline__ explicit SharedDiv(double den) : d(den) {
+    ok = den >= 0x1p-450 && den <= 0x1p+450;
+    r = ok ? __drcp_rn(den) : 0.0;
+  }
+  __device__ __forceinline__ double operator()(double a) const {
+    const double aa = fabs(a);
+    if (ok && aa >= 0x1p-450 && aa <= 0x1p+450) {
+      const double q0 = a * r;
+      const double e = fma(-d, q0, a);
+      return fma(e, r, q0);
+    }
+    return a / d;
+  }
+};
+
 // HLL flux through one face normal to axis DIR (0,1,2) from the plus state of
 // the cell on the low side (L) and the minus state of the cell on the high side
 // (R): get_fluxes + flux_hll, flux.f90:504-590.  gl=gr=gamma.
@@ -176,8 +203,13 @@ BX_HD void hll_flux(const FaceState& L, const FaceState& R, double gam, double F
   const double am = fmax(fmax(0.0, -(vr - cr)), -(vl - cl));
   const double apam = ap * am;
   const double den = ap + am;
+#ifdef __CUDA_ARCH__
+  const SharedDiv div(den);
 #pragma unroll
+  for (int i = 0; i < 5; ++i) F[i] = div(ap * fl[i] + am * fr[i] - apam * (sr[i] - sl[i]));
+#else
   for (int i = 0; i < 5; ++i) F[i] = (ap * fl[i] + am * fr[i] - apam * (sr[i] - sl[i])) / den;
+#endif
 }
 
 // floors after the conservative update (flux.f90:223-230)

@@ -16,6 +16,15 @@ extern "C" {
  * NULL) receives nothing (clocks are sampled by the caller).  Returns 0 on success. */
 int bx_fp64_peak(double *tflops, double *ms);
 
+/* Self-check of the shared-denominator division used by the HLL flux: n random
+ * (numerator, denominator) pairs with exponents in [-exp_range, exp_range] (plus
+ * exact multiples and near-ties) are divided both ways on the device; returns the
+ * number of results that differ from IEEE division in any bit (zeros of either
+ * sign compare equal) and one example. */
+int bx_check_shared_division(unsigned long long n, unsigned long long seed, int exp_range,
+                             unsigned long long *mismatches, double *example_a,
+                             double *example_d);
+
 #ifdef __cplusplus
 }
 #endif

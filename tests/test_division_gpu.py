@@ -1,0 +1,25 @@
+"""The shared-denominator division of the HLL flux equals IEEE division bit for bit.
+
+Each HLL face divides five flux numerators by the same wave-speed sum; the
+kernels compute one correctly rounded reciprocal and correct each quotient with
+an FMA residual.  This checks the device implementation against the device's
+IEEE double division on random operands (random mantissas and exponents inside
+and far outside the window where the short form is used, exact multiples and
+near-ties)."""
+import ctypes as C
+
+import pytest
+
+from boxzyhydro_b200 import _lib
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("exp_range,seed", [(60, 1), (200, 2), (449, 3), (1000, 4)])
+def test_shared_division_is_ieee(exp_range, seed):
+    bad = C.c_ulonglong()
+    a, d = C.c_double(), C.c_double()
+    rc = _lib.lib().bx_check_shared_division(50_000_000, seed, exp_range, C.byref(bad),
+                                             C.byref(a), C.byref(d))
+    assert rc == 0
+    assert bad.value == 0, f"{bad.value} mismatches, e.g. {a.value!r} / {d.value!r}"
