@@ -85,6 +85,16 @@ def lib():
                                                C.POINTER(C.c_ulonglong), dp, dp]),
         "bx_ghost_fill_noalloc": (C.c_int, [vp, C.c_int64, vp, vp, vp, C.c_int64, vp]),
         "bx_noalloc_last_error": (C.c_char_p, []),
+        "bx_batch_create": (C.c_int, [C.c_int32, C.POINTER(BxParams), C.POINTER(H)]),
+        "bx_batch_destroy": (C.c_int, [H]),
+        "bx_batch_set_stream": (C.c_int, [H, vp]),
+        "bx_batch_upload": (C.c_int, [H, C.c_int32, vp]),
+        "bx_batch_set_clock": (C.c_int, [H, C.c_int32, C.c_double, C.c_double, C.c_int64]),
+        "bx_batch_get_clock": (C.c_int, [H, C.c_int32, dp, dp, dp, i64p]),
+        "bx_batch_run": (C.c_int, [H, C.c_int64, C.c_double, C.c_int32]),
+        "bx_batch_download": (C.c_int, [H, C.c_int32, vp, vp, vp]),
+        "bx_batch_info": (C.c_int, [H, dp, i64p, i32p, i64p]),
+        "bx_batch_last_error": (C.c_char_p, [H]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

@@ -27,38 +27,7 @@ size_t stage_smem_bytes();
 int stage_blocks_per_sm(int stage, bool pow2, bool threed);
 }  // namespace bx
 
-struct bx_handle {
-  bx_params P{};
-  Geom g{};
-  GhostTable T;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  double* buf[3] = {nullptr, nullptr, nullptr};
-  int cur = 0;
-  int nsrc = 1;
-  PhaseArrays pa{};
-  int nghost = 0;
-  int32_t *d_dst = nullptr, *d_src1 = nullptr, *d_src2 = nullptr;
-  uint8_t *d_sgn1 = nullptr, *d_sgn2 = nullptr;
-  Geom* d_geom = nullptr;
-  Tile* d_tiles = nullptr;
-  int ntiles = 0;
-  Ctrl* d_ctrl = nullptr;
-  Ctrl* h_ctrl = nullptr;  // pinned mirror
-  Ctrl clock{};            // host copy of the clock after the last completed call
-  int mode = 0;            // 0 = reference arrays current, 1 = fused planes current
-  bool eligible = false;
-  bool gforce_set = false;
-  uint32_t status = 0;
-  int last_path = 0;
-  // profiling: CUDA events around the stage launches, accumulated per step
-  bool prof = false;
-  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
-  double ms_stage[2] = {0.0, 0.0};
-  long long n_stage = 0;
-  long long launches = 0;  // kernels of this library launched on the handle's stream
-  std::string err;
-};
+#include "bx_handle.h"
 
 static std::string g_create_err;
 
@@ -637,6 +606,27 @@ int bx_profile_read(bx_handle* h, double* ms_stage0, double* ms_stage1, int64_t*
   if (launches) *launches = h->launches;
   return BX_OK;
 }
+
+}  // extern "C"
+
+int bx_handle_adopt_fused(bx_handle* h, const double* planes, long long ps, int nsrc,
+                          const Ctrl& clock) {
+  const long long n = h->g.ng;
+  for (int q = 0; q < 5; ++q)
+    CK(cudaMemcpyAsync(h->buf[h->cur] + q * n, planes + q * ps, n * sizeof(double),
+                       cudaMemcpyDeviceToDevice, h->stream));
+  h->nsrc = nsrc;
+  h->mode = 1;
+  h->clock = clock;
+  h->clock.flags = 0;
+  h->clock.active = 0;
+  h->clock.tripped = 0;
+  h->clock.nsrc = 0;
+  if (int r = push_clock(h)) return r;
+  return BX_OK;
+}
+
+extern "C" {
 
 int bx_ghost_plan(const bx_params* params, int64_t* nghost, int32_t* dst, int32_t* src1,
                   uint8_t* sgn1, int32_t* src2, uint8_t* sgn2, int32_t* fused_ok) {

@@ -1,0 +1,47 @@
+// bx_handle.h -- the handle behind the opaque bx_handle of the C ABI (private).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "bx_internal.h"
+
+struct bx_handle {
+  bx_params P{};
+  bx::Geom g{};
+  bx::GhostTable T;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  double* buf[3] = {nullptr, nullptr, nullptr};
+  int cur = 0;
+  int nsrc = 1;
+  bx::PhaseArrays pa{};
+  int nghost = 0;
+  int32_t *d_dst = nullptr, *d_src1 = nullptr, *d_src2 = nullptr;
+  uint8_t *d_sgn1 = nullptr, *d_sgn2 = nullptr;
+  bx::Geom* d_geom = nullptr;
+  bx::Tile* d_tiles = nullptr;
+  int ntiles = 0;
+  bx::Ctrl* d_ctrl = nullptr;
+  bx::Ctrl* h_ctrl = nullptr;  // pinned mirror
+  bx::Ctrl clock{};            // host copy of the clock after the last completed call
+  int mode = 0;            // 0 = reference arrays current, 1 = fused planes current
+  bool eligible = false;
+  bool gforce_set = false;
+  uint32_t status = 0;
+  int last_path = 0;
+  // profiling: CUDA events around the stage launches, accumulated per step
+  bool prof = false;
+  cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};
+  double ms_stage[2] = {0.0, 0.0};
+  long long n_stage = 0;
+  long long launches = 0;  // kernels of this library launched on the handle's stream
+  std::string err;
+};
+
+// Take over a fused state held elsewhere on the device: the five conserved
+// planes of one grid (plane stride `ps`), `nsrc` sources short of the
+// reference state, with the given clock.  The batched path uses it to continue
+// a box on a handle of its own.
+int bx_handle_adopt_fused(bx_handle* h, const double* planes, long long ps, int nsrc,
+                          const bx::Ctrl& clock);

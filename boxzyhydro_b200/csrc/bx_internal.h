@@ -37,7 +37,15 @@ struct Ctrl {
   unsigned int flags;
   int active;         // 1 while the step in flight is to be taken
   double cfl;
-  double pad[2];
+  // batched path: sources the planes are short of (0 = use StageArgs::nsrc),
+  // clock saved at step start, and whether the box left the fused path
+  int nsrc;
+  int tripped;        // 1: a guard fired; the box's planes hold the tripped step's input
+  long long trip_step;  // batch step index (within the run) of the trip
+  double time0, dtold0;
+  long long step0;
+  unsigned long long rate_bits0;
+  long long run_step;   // steps launched in the current run (for trip_step)
 };
 
 // Geometry and constants of one box (one reference grid).
@@ -91,7 +99,7 @@ struct StageArgs {
   const Geom* geom;  // per box geometry (device)
   const Tile* tiles;
   long long ncells_total;  // plane stride of the pooled buffers
-  int nsrc;
+  int nsrc;                // > 0: sources the input is short of; 0: per box (Ctrl::nsrc)
 };
 
 cudaError_t launch_stage(int stage, bool pow2, bool threed, const StageArgs& a, int ntiles,
@@ -124,7 +132,15 @@ cudaError_t phase_copy_old(const Geom& g, PhaseArrays& a, cudaStream_t s);
 // fused <-> phase representation changes
 cudaError_t fused_to_phase(const Geom& g, const double* X, int nsrc, PhaseArrays& a, int nghost,
                            const int32_t* dst, const int32_t* src2, const uint8_t* sgn2,
-                           cudaStream_t s);
+                           cudaStream_t s, long long xps = 0);
+
+// batched path: per-box checks on planes with stride ps (X points at the box)
+cudaError_t box_check_clean(const Geom& g, const double* X, long long ps, int nghost,
+                            const int32_t* dst, const int32_t* src2, const uint8_t* sgn2,
+                            Ctrl* ctrl, cudaStream_t s);
+cudaError_t box_rate(const Geom& g, const double* X, long long ps, Ctrl* ctrl, cudaStream_t s);
+cudaError_t launch_dt_batch(Ctrl* ctrl, int nbox, cudaStream_t s);
+cudaError_t launch_end_batch(Ctrl* ctrl, int nbox, cudaStream_t s);
 
 
 // does the uploaded reference state equal what the fused form reproduces

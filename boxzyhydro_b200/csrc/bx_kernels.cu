@@ -78,12 +78,12 @@ __device__ __forceinline__ void apply_sources(Cons& c, int nsrc, double small_ep
 //           with the stage-0 velocity m0/rho0 (main.f90:353 uses the stale u).
 template <int STAGE>
 __device__ __forceinline__ Prim load_prim(const StageArgs& a, const Geom& g, int x, int y, int z,
-                                          unsigned& flags, bool need_c = true) {
+                                          unsigned& flags, int nsrc, bool need_c = true) {
   const long long PS = a.ncells_total;
   Prim q;
   if (STAGE == 0) {
     Cons c = load_cons(a.X, PS, g, x, y, z);
-    apply_sources(c, a.nsrc, g.small_eps);
+    apply_sources(c, nsrc, g.small_eps);
     q.d = c.d;
     q.u1 = c.m1 / c.d;
     q.u2 = c.m2 / c.d;
@@ -196,6 +196,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
   double* FX = sm;                    // [5][TY][TX+1] x face fluxes (aliases SP)
   double* FY = sm + 5 * NFX;          // [5][TY+1][TX] y face fluxes
   const double dt = C->dt;
+  const int nsrc = a.nsrc > 0 ? a.nsrc : C->nsrc;
 
   const int tid = threadIdx.x;
   const int tx = tid % TX, ty = tid / TX;
@@ -220,10 +221,10 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
 
   const int z0 = g.az0 + t.z0, z1 = g.az0 + t.z1;
   if (THREED && own) {
-    const Prim Pm2 = load_prim<STAGE>(a, g, gx, gy, z0 - 2, flags);
-    const Prim Pm1 = load_prim<STAGE>(a, g, gx, gy, z0 - 1, flags);
-    Pk = load_prim<STAGE>(a, g, gx, gy, z0, flags);
-    Pk1 = load_prim<STAGE>(a, g, gx, gy, z0 + 1, flags);
+    const Prim Pm2 = load_prim<STAGE>(a, g, gx, gy, z0 - 2, flags, nsrc);
+    const Prim Pm1 = load_prim<STAGE>(a, g, gx, gy, z0 - 1, flags, nsrc);
+    Pk = load_prim<STAGE>(a, g, gx, gy, z0, flags, nsrc);
+    Pk1 = load_prim<STAGE>(a, g, gx, gy, z0 + 1, flags, nsrc);
     FaceState mm, pm, m0;
     if (z0 - 1 < g.az0) {
       ghost_states(Pm1, mm, pm);
@@ -241,9 +242,9 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
     double Fzp[5];
     if (own) {
       if (THREED) {
-        P2 = load_prim<STAGE>(a, g, gx, gy, z + 2, flags);
+        P2 = load_prim<STAGE>(a, g, gx, gy, z + 2, flags, nsrc);
       } else {
-        Pk = load_prim<STAGE>(a, g, gx, gy, z, flags);
+        Pk = load_prim<STAGE>(a, g, gx, gy, z, flags, nsrc);
       }
       put_prim(SP, (ty + 2) * PW + (tx + 2), Pk);
     }
@@ -263,7 +264,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
       const int fx = bx0 + cx, fy = by0 + cy;
       const bool near = cx >= -1 && cx <= w && cy >= -1 && cy <= h;
       const bool inner = fx >= g.ax0 && fx < g.ax1 && fy >= g.ay0 && fy < g.ay1;
-      const Prim q = load_prim<STAGE>(a, g, fx, fy, z, flags, near && inner);
+      const Prim q = load_prim<STAGE>(a, g, fx, fy, z, flags, nsrc, near && inner);
       put_prim(SP, (cy + 2) * PW + (cx + 2), q);
     }
     if (THREED && own) {
@@ -349,7 +350,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         ft[q] = POW2 ? -sum * dt * g.ivol : -sum * dt / g.vol;
       }
       Cons c0 = load_cons(a.X, PS, g, gx, gy, z);
-      apply_sources(c0, a.nsrc, g.small_eps);
+      apply_sources(c0, nsrc, g.small_eps);
       double n[5];
       if (STAGE == 0) {
         n[0] = c0.d + ft[0];
@@ -500,6 +501,64 @@ __global__ void k_end(Ctrl* ctrl, int n) {
   double dt = kHalf * c.dt;
   dt = dt * 2.0;
   c.time = c.time + dt;
+}
+
+// batched boxes: as k_dt/k_end, plus the saved clock and the trip of a box
+// whose step raised a guard (its planes then keep the step's input)
+__global__ void k_dt_batch(Ctrl* ctrl, int n) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  Ctrl& c = ctrl[b];
+  c.run_step += 1;
+  if (c.tripped || !(c.time < c.endtime) || c.step >= 1000000 || c.step >= c.max_step) {
+    c.active = 0;
+    return;
+  }
+  c.time0 = c.time;
+  c.dtold0 = c.dtold;
+  c.step0 = c.step;
+  c.rate_bits0 = c.rate_bits;
+  c.step = c.step + 1;
+  const double rate = __longlong_as_double((long long)c.rate_bits);
+  c.rate = rate;
+  c.rate_bits = 0ull;
+  double dt = c.cfl / rate;
+  dt = dt * 1.0;
+  if (c.step > 1 && c.dtold > 0.0) dt = fmin(dt, c.dtold * 1.1);
+  c.dtold = dt;
+  if (dt + c.time > c.endtime) dt = c.endtime - c.time;
+  dt = dt * kHalf;
+  dt = dt * 2.0;
+  c.dt = dt;
+  c.active = 1;
+}
+__global__ void k_end_batch(Ctrl* ctrl, int n) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b >= n) return;
+  Ctrl& c = ctrl[b];
+  if (!c.active) return;
+  if (c.flags & (kFlagVlimit | kFlagLowRho | kFlagNonFinite)) {
+    c.tripped = 1;
+    c.trip_step = c.run_step - 1;
+    c.time = c.time0;
+    c.dtold = c.dtold0;
+    c.step = c.step0;
+    c.rate_bits = c.rate_bits0;
+    c.active = 0;
+    return;
+  }
+  double dt = kHalf * c.dt;
+  dt = dt * 2.0;
+  c.time = c.time + dt;
+  c.nsrc = 2;
+}
+cudaError_t launch_dt_batch(Ctrl* ctrl, int nbox, cudaStream_t s) {
+  k_dt_batch<<<(nbox + 127) / 128, 128, 0, s>>>(ctrl, nbox);
+  return cudaGetLastError();
+}
+cudaError_t launch_end_batch(Ctrl* ctrl, int nbox, cudaStream_t s) {
+  k_end_batch<<<(nbox + 127) / 128, 128, 0, s>>>(ctrl, nbox);
+  return cudaGetLastError();
 }
 
 cudaError_t launch_dt(Ctrl* ctrl, int nbox, cudaStream_t s) {
@@ -770,13 +829,13 @@ __global__ void k_copy5(const double* src, double* dst, long long n) {
 }
 
 // fused state (X planes) -> reference arrays: interior cons = src^(nsrc-1)(X)
-__global__ void k_f2p_interior(Geom g, const double* X, int nsrc, PhaseArrays a) {
+__global__ void k_f2p_interior(Geom g, const double* X, long long xps, int nsrc, PhaseArrays a) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= g.ng) return;
   const int x = (int)(i % g.nx), y = (int)((i / g.nx) % g.ny), z = (int)(i / g.sz);
   if (is_ghost(g, x, y, z)) return;
   const long long n = g.ng;
-  Cons c{X[i], X[n + i], X[2 * n + i], X[3 * n + i], X[4 * n + i]};
+  Cons c{X[i], X[xps + i], X[2 * xps + i], X[3 * xps + i], X[4 * xps + i]};
   apply_sources(c, nsrc - 1, g.small_eps);
   a.cons[i] = c.d;
   a.cons[n + i] = c.m1;
@@ -883,13 +942,76 @@ cudaError_t phase_copy_old(const Geom& g, PhaseArrays& a, cudaStream_t s) {
 }
 cudaError_t fused_to_phase(const Geom& g, const double* X, int nsrc, PhaseArrays& a, int nghost,
                            const int32_t* dst, const int32_t* src2, const uint8_t* sgn2,
-                           cudaStream_t s) {
-  k_f2p_interior<<<nblk(g.ng), PB, 0, s>>>(g, X, nsrc, a);
+                           cudaStream_t s, long long xps) {
+  k_f2p_interior<<<nblk(g.ng), PB, 0, s>>>(g, X, xps > 0 ? xps : g.ng, nsrc, a);
   if (nghost > 0)
     k_fill_resolved<<<nblk(nghost), PB, 0, s>>>(nghost, dst, src2, sgn2, a.cons, g.ng);
   k_f2p_prims<<<nblk(g.ng), PB, 0, s>>>(g, a);
   return cudaGetLastError();
 }
+// does a box's plane set hold a state the fused stages start from
+// (interior rho >= 1e-4 and finite, ghosts = two-sweep fill of the interior)?
+__global__ void k_box_check_cells(Geom g, const double* X, long long ps, Ctrl* ctrl) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= g.ng) return;
+  const int x = (int)(i % g.nx), y = (int)((i / g.nx) % g.ny), z = (int)(i / g.sz);
+  if (is_ghost(g, x, y, z)) return;
+  bool ok = X[i] >= kLowRho;
+  for (int q = 0; q < 5; ++q) ok = ok && isfinite(X[q * ps + i]);
+  if (!ok) atomicOr(&ctrl->flags, (unsigned)kFlagNotClean);
+}
+__global__ void k_box_check_ghosts(int nghost, const int32_t* dst, const int32_t* src,
+                                   const uint8_t* sgn, const double* X, long long ps,
+                                   Ctrl* ctrl) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nghost) return;
+  const long long s = src[k], d = dst[k];
+  const unsigned m = sgn[k];
+  bool ok = X[d] == X[s] && X[4 * ps + d] == X[4 * ps + s];
+  ok = ok && X[ps + d] == ((m & 1) ? -X[ps + s] : X[ps + s]);
+  ok = ok && X[2 * ps + d] == ((m & 2) ? -X[2 * ps + s] : X[2 * ps + s]);
+  ok = ok && X[3 * ps + d] == ((m & 4) ? -X[3 * ps + s] : X[3 * ps + s]);
+  if (!ok) atomicOr(&ctrl->flags, (unsigned)kFlagNotClean);
+}
+// Courant rate (courant.f90:172-176) of a box whose planes hold the reference
+// cons with u == m/rho: the max over interior cells (ghosts repeat them)
+__global__ void k_box_rate(Geom g, const double* X, long long ps, Ctrl* ctrl) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double r = 0.0;
+  if (i < g.ng) {
+    const int x = (int)(i % g.nx), y = (int)((i / g.nx) % g.ny), z = (int)(i / g.sz);
+    if (!is_ghost(g, x, y, z)) {
+      const double d = X[i];
+      const double u1 = X[ps + i] / d, u2 = X[2 * ps + i] / d, u3 = X[3 * ps + i] / d;
+      const double p = eos_pressure(d, X[4 * ps + i], u1, u2, u3, g.gm1, g.small_eps);
+      r = g.pow2 ? courant_rate<true>(d, p, g.gam, u1, u2, u3, g.dx, g.dy, g.dz, g.idx, g.idy, g.idz)
+                 : courant_rate<false>(d, p, g.gam, u1, u2, u3, g.dx, g.dy, g.dz, g.idx, g.idy, g.idz);
+    }
+  }
+  __shared__ double wm[PB / 32];
+  r = warp_max(r);
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = r;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int k = 0; k < PB / 32; ++k) m = fmax(m, wm[k]);
+    atomicMax(&ctrl->rate_bits, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+cudaError_t box_check_clean(const Geom& g, const double* X, long long ps, int nghost,
+                            const int32_t* dst, const int32_t* src2, const uint8_t* sgn2,
+                            Ctrl* ctrl, cudaStream_t s) {
+  k_box_check_cells<<<nblk(g.ng), PB, 0, s>>>(g, X, ps, ctrl);
+  if (nghost > 0)
+    k_box_check_ghosts<<<nblk(nghost), PB, 0, s>>>(nghost, dst, src2, sgn2, X, ps, ctrl);
+  return cudaGetLastError();
+}
+cudaError_t box_rate(const Geom& g, const double* X, long long ps, Ctrl* ctrl, cudaStream_t s) {
+  k_box_rate<<<nblk(g.ng), PB, 0, s>>>(g, X, ps, ctrl);
+  return cudaGetLastError();
+}
+
 cudaError_t check_clean(const Geom& g, const PhaseArrays& a, int nghost, const int32_t* dst,
                         const int32_t* src2, const uint8_t* sgn2, Ctrl* ctrl, cudaStream_t s) {
   k_check_cells<<<nblk(g.ng), PB, 0, s>>>(g, a, ctrl);

@@ -144,6 +144,33 @@ int bx_profile_read(bx_handle *h, double *ms_stage0, double *ms_stage1, int64_t 
 int bx_ghost_plan(const bx_params *params, int64_t *nghost, int32_t *dst, int32_t *src1,
                   uint8_t *sgn1, int32_t *src2, uint8_t *sgn2, int32_t *fused_ok);
 
+/* ---- Batched ensembles.  No counterpart in the reference, which advances one grid
+ * per process.  Many independent grids ("boxes", each with its own size, gamma, cfl,
+ * dt and clock) advance together: one tile list spans all boxes, a step is four
+ * launches for the whole ensemble, and a run of n steps is replayed as one CUDA
+ * graph.  Each box evolves bit for bit as it would under bx_step on its own.  Boxes
+ * must be fused-eligible (bx_ghost_plan fused_ok) and all 3-D (nz>=6) or all 2-D;
+ * an uploaded state must be one the fused stages start from (interior rho >= 1e-4,
+ * u == m/rho, ghosts equal to the two-sweep fill), else BX_ERR_STATE.  A box whose
+ * step fires the velocity limiter or the low-density EOS branch continues on a
+ * single-grid handle of its own after the run. */
+typedef struct bx_batch bx_batch;
+int bx_batch_create(int32_t nbox, const bx_params *params, bx_batch **out);
+int bx_batch_destroy(bx_batch *b);
+int bx_batch_set_stream(bx_batch *b, void *cuda_stream);
+int bx_batch_upload(bx_batch *b, int32_t box, const double *cons);
+int bx_batch_set_clock(bx_batch *b, int32_t box, double time, double dtold, int64_t step);
+int bx_batch_get_clock(bx_batch *b, int32_t box, double *time, double *dt, double *dtold,
+                       int64_t *step);
+/* nsteps iterations of every box's main loop (boxes at endtime stop). */
+int bx_batch_run(bx_batch *b, int64_t nsteps, double endtime, int32_t use_graph);
+int bx_batch_download(bx_batch *b, int32_t box, double *cons, double *u, double *p);
+/* device time of the last run (ms), kernels it launched, boxes running on their own
+ * handles, cells in the pool */
+int bx_batch_info(bx_batch *b, double *last_run_ms, int64_t *launches, int32_t *n_solo,
+                  int64_t *cells);
+const char *bx_batch_last_error(bx_batch *b);
+
 /* No counterpart in the reference.  One set_ghost_cells sweep -- the same result as
  * bx_ghost -- that allocates nothing, for callers that cannot allocate device memory
  * (a host program that has reserved the device's memory for its own pool, or a
