@@ -24,7 +24,7 @@ using namespace bx;
 
 namespace bx {
 size_t stage_smem_bytes();
-int stage_blocks_per_sm(int stage, bool pow2, bool threed);
+int stage_blocks_per_sm(int stage, int pm, bool threed);
 }  // namespace bx
 
 #include "bx_handle.h"
@@ -103,6 +103,11 @@ int bx_create(const bx_params* params, bx_handle** out) {
     return set_err(nullptr, BX_ERR_ARG, "grid exceeds 2^31 cells");
   if (!(P.dx > 0 && P.dy > 0 && P.dz > 0 && P.gammafix > 1.0 && P.cfl > 0))
     return set_err(nullptr, BX_ERR_ARG, "dx,dy,dz,cfl must be >0 and gammafix>1");
+  // divisions by the cell sizes and volume use their correctly rounded
+  // reciprocals, exact while these stay far from the overflow/subnormal range
+  if (!(P.dx >= 1e-40 && P.dx <= 1e40 && P.dy >= 1e-40 && P.dy <= 1e40 && P.dz >= 1e-40 &&
+        P.dz <= 1e40))
+    return set_err(nullptr, BX_ERR_ARG, "dx,dy,dz must lie in [1e-40, 1e40]");
   bx_handle* h = new bx_handle();
   h->P = P;
   fill_geom(P, h->g);

@@ -29,7 +29,7 @@
 using namespace bx;
 
 namespace bx {
-int stage_blocks_per_sm(int stage, bool pow2, bool threed);
+int stage_blocks_per_sm(int stage, int pm, bool threed);
 }
 
 namespace {
@@ -59,6 +59,7 @@ struct bx_batch {
   Tile* d_tiles = nullptr;
   int ntiles = 0;
   bool pow2 = true, threed = true;
+  int pm = 1;  // 1: all boxes have power-of-two spacings; 0: otherwise (cdiv, exact for any)
   PhaseArrays scratch{};  // reference arrays of the largest box (downloads)
   double* staging = nullptr;
   cudaStream_t stream = nullptr;
@@ -122,7 +123,8 @@ int bx_batch_create(int32_t nbox, const bx_params* params, bx_batch** out) {
   for (int i = 0; i < nbox; ++i) {
     const bx_params& P = b->P[i];
     if (P.h2stat != -1 || P.fluxangmom || P.nx < 5 || P.ny < 5 || P.nz < 1 ||
-        !(P.dx > 0 && P.dy > 0 && P.dz > 0 && P.gammafix > 1.0 && P.cfl > 0)) {
+        !(P.dx >= 1e-40 && P.dx <= 1e40 && P.dy >= 1e-40 && P.dy <= 1e40 && P.dz >= 1e-40 &&
+          P.dz <= 1e40 && P.gammafix > 1.0 && P.cfl > 0)) {
       bx_batch_destroy(b);
       return berr(nullptr, BX_ERR_UNSUPPORTED, "box " + std::to_string(i) +
                                                    ": unsupported or invalid parameters");
@@ -169,6 +171,11 @@ int bx_batch_create(int32_t nbox, const bx_params* params, bx_batch** out) {
     }
   }
   b->threed = b->G[0].threed != 0;
+  {
+    int np2 = 0;
+    for (int i = 0; i < nbox; ++i) np2 += b->G[i].pow2 ? 1 : 0;
+    b->pm = np2 == nbox ? 1 : 0;
+  }
   b->N = off;
   auto fail = [&](int code) {
     g_batch_err = b->err;
@@ -226,8 +233,8 @@ int bx_batch_create(int32_t nbox, const bx_params* params, bx_batch** out) {
   BCKC(cudaMalloc(&b->staging, 5 * m * sizeof(double)));
   BCKC(cudaEventCreate(&b->ev0));
   BCKC(cudaEventCreate(&b->ev1));
-  stage_blocks_per_sm(0, b->pow2, b->threed);  // sets the shared-memory attribute
-  stage_blocks_per_sm(1, b->pow2, b->threed);
+  stage_blocks_per_sm(0, b->pm, b->threed);  // sets the shared-memory attribute
+  stage_blocks_per_sm(1, b->pm, b->threed);
 #undef BCKC
   *out = b;
   return BX_OK;
@@ -353,10 +360,10 @@ static int enqueue_steps(bx_batch* b, int nsteps) {
     a.X = b->buf[X];
     a.Y = nullptr;
     a.out = b->buf[Y];
-    BCK(launch_stage(0, b->pow2, b->threed, a, b->ntiles, b->stream));
+    BCK(launch_stage(0, b->pm, b->threed, a, b->ntiles, b->stream));
     a.Y = b->buf[Y];
     a.out = b->buf[Z];
-    BCK(launch_stage(1, b->pow2, b->threed, a, b->ntiles, b->stream));
+    BCK(launch_stage(1, b->pm, b->threed, a, b->ntiles, b->stream));
     BCK(launch_end_batch(b->d_ctrl, b->nbox, b->stream));
     c = Z;
   }

@@ -102,7 +102,8 @@ struct StageArgs {
   int nsrc;                // > 0: sources the input is short of; 0: per box (Ctrl::nsrc)
 };
 
-cudaError_t launch_stage(int stage, bool pow2, bool threed, const StageArgs& a, int ntiles,
+// pm: 1 = every box has power-of-two spacings, 0 = otherwise
+cudaError_t launch_stage(int stage, int pm, bool threed, const StageArgs& a, int ntiles,
                          cudaStream_t s);
 cudaError_t launch_dt(Ctrl* ctrl, int nbox, cudaStream_t s);
 cudaError_t launch_end(Ctrl* ctrl, int nbox, cudaStream_t s);

@@ -347,7 +347,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         const double dfy = FY[q * NFY + (ty + 1) * TX + tx] - FY[q * NFY + ty * TX + tx];
         double sum = g.ayz * dfx + g.axz * dfy;
         if (THREED) sum = sum + g.axy * (Fzp[q] - Fzm[q]);
-        ft[q] = POW2 ? -sum * dt * g.ivol : -sum * dt / g.vol;
+        ft[q] = POW2 ? -sum * dt * g.ivol : cdiv(-sum * dt, g.vol, g.ivol);
       }
       Cons c0 = load_cons(a.X, PS, g, gx, gy, z);
       apply_sources(c0, nsrc, g.small_eps);
@@ -418,7 +418,10 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
   }
 }
 
-template <int STAGE, bool POW2, bool THREED>
+// PM: 1 = every box of the launch has power-of-two spacings (divisions by the
+// cell sizes are multiplications by exact reciprocals), 0 = otherwise (cdiv,
+// exact for any spacing)
+template <int STAGE, int PM, bool THREED>
 __global__ void __launch_bounds__(TX* TY, 2) k_stage(StageArgs a) {
   extern __shared__ double sm[];
   __shared__ Geom sg;
@@ -430,39 +433,48 @@ __global__ void __launch_bounds__(TX* TY, 2) k_stage(StageArgs a) {
   Ctrl* C = a.ctrl + t.box;
   if (!C->active) return;
   const bool full = (t.x0 + TX <= sg.ax1 - sg.ax0) && (t.y0 + TY <= sg.ay1 - sg.ay0);
-  if (full)
-    stage_tile<STAGE, POW2, THREED, true>(a, t, sg, C, sm, red_rate, red_flags);
-  else
-    stage_tile<STAGE, POW2, THREED, false>(a, t, sg, C, sm, red_rate, red_flags);
+  if (PM == 1) {
+    if (full)
+      stage_tile<STAGE, true, THREED, true>(a, t, sg, C, sm, red_rate, red_flags);
+    else
+      stage_tile<STAGE, true, THREED, false>(a, t, sg, C, sm, red_rate, red_flags);
+  } else {
+    if (full)
+      stage_tile<STAGE, false, THREED, true>(a, t, sg, C, sm, red_rate, red_flags);
+    else
+      stage_tile<STAGE, false, THREED, false>(a, t, sg, C, sm, red_rate, red_flags);
+  }
 }
 
-template <int STAGE, bool POW2, bool THREED>
+template <int STAGE, int PM, bool THREED>
 static cudaError_t launch_stage_t(const StageArgs& a, int ntiles, cudaStream_t s) {
   const size_t smem = SMEM_DOUBLES * sizeof(double);
   static bool attr_set = false;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(k_stage<STAGE, POW2, THREED>,
+    cudaError_t e = cudaFuncSetAttribute(k_stage<STAGE, PM, THREED>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
   if (ntiles <= 0) return cudaSuccess;
-  k_stage<STAGE, POW2, THREED><<<ntiles, TX * TY, smem, s>>>(a);
+  k_stage<STAGE, PM, THREED><<<ntiles, TX * TY, smem, s>>>(a);
   return cudaGetLastError();
 }
 
-cudaError_t launch_stage(int stage, bool pow2, bool threed, const StageArgs& a, int ntiles,
+template <int STAGE>
+static cudaError_t launch_stage_s(int pm, bool threed, const StageArgs& a, int ntiles,
+                                  cudaStream_t s) {
+  if (pm == 1) return threed ? launch_stage_t<STAGE, 1, true>(a, ntiles, s)
+                             : launch_stage_t<STAGE, 1, false>(a, ntiles, s);
+  return threed ? launch_stage_t<STAGE, 0, true>(a, ntiles, s)
+                : launch_stage_t<STAGE, 0, false>(a, ntiles, s);
+}
+
+// pm: 1 every box has power-of-two spacings, 0 otherwise
+cudaError_t launch_stage(int stage, int pm, bool threed, const StageArgs& a, int ntiles,
                          cudaStream_t s) {
-  if (stage == 0) {
-    if (pow2) return threed ? launch_stage_t<0, true, true>(a, ntiles, s)
-                            : launch_stage_t<0, true, false>(a, ntiles, s);
-    return threed ? launch_stage_t<0, false, true>(a, ntiles, s)
-                  : launch_stage_t<0, false, false>(a, ntiles, s);
-  }
-  if (pow2) return threed ? launch_stage_t<1, true, true>(a, ntiles, s)
-                          : launch_stage_t<1, true, false>(a, ntiles, s);
-  return threed ? launch_stage_t<1, false, true>(a, ntiles, s)
-                : launch_stage_t<1, false, false>(a, ntiles, s);
+  return stage == 0 ? launch_stage_s<0>(pm, threed, a, ntiles, s)
+                    : launch_stage_s<1>(pm, threed, a, ntiles, s);
 }
 
 size_t stage_smem_bytes() { return SMEM_DOUBLES * sizeof(double); }
@@ -1030,16 +1042,16 @@ cudaError_t soa_to_aos(const double* soa, double* aos, long long n, int k, cudaS
 }  // namespace bx
 
 namespace bx {
-int stage_blocks_per_sm(int stage, bool pow2, bool threed) {
+int stage_blocks_per_sm(int stage, int pm, bool threed) {
   int nb = 0;
   const size_t smem = stage_smem_bytes();
   const void* fn;
   if (stage == 0)
-    fn = pow2 ? (threed ? (const void*)k_stage<0, true, true> : (const void*)k_stage<0, true, false>)
-              : (threed ? (const void*)k_stage<0, false, true> : (const void*)k_stage<0, false, false>);
+    fn = pm == 1 ? (threed ? (const void*)k_stage<0, 1, true> : (const void*)k_stage<0, 1, false>)
+                 : (threed ? (const void*)k_stage<0, 0, true> : (const void*)k_stage<0, 0, false>);
   else
-    fn = pow2 ? (threed ? (const void*)k_stage<1, true, true> : (const void*)k_stage<1, true, false>)
-              : (threed ? (const void*)k_stage<1, false, true> : (const void*)k_stage<1, false, false>);
+    fn = pm == 1 ? (threed ? (const void*)k_stage<1, 1, true> : (const void*)k_stage<1, 1, false>)
+                 : (threed ? (const void*)k_stage<1, 0, true> : (const void*)k_stage<1, 0, false>);
   cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, TX * TY, smem) != cudaSuccess) {
     cudaGetLastError();

@@ -85,9 +85,27 @@ BX_HD double recon_eps(double d, double E, double u1, double u2, double u3, doub
   return fmax(E - kHalf * d * (u1 * u1 + u2 * u2 + u3 * u3), small_eps);
 }
 
-// Courant rate of one cell (courant.f90:173-174); inv_* are 1/dx etc. when the
-// spacing is a power of two (x/2^k and x*2^-k round identically), else the
-// division is done.
+// x/d for a grid constant d (a cell size or the cell volume) given its
+// correctly rounded reciprocal r, computed on the host.  With q0 = RN(x*r) the
+// residual x - d*q0 is exact under a fused multiply-add and RN(q0 + (x-d*q0)*r)
+// is the IEEE quotient (Markstein's theorem) while |x| and d lie in
+// [2^-450, 2^450] (bx_create keeps d there); zero gives x*r, a signed zero like
+// x/d; other x take the IEEE division.
+BX_HD double cdiv(double x, double d, double r) {
+#ifdef __CUDA_ARCH__
+  const double ax = fabs(x);
+  if (ax >= 0x1p-450 && ax <= 0x1p+450) {
+    const double q0 = x * r;
+    return fma(fma(-d, q0, x), r, q0);
+  }
+  if (ax == 0.0) return x * r;
+#endif
+  return x / d;
+}
+
+// Courant rate of one cell (courant.f90:173-174); idx etc. are 1/dx etc.: when
+// the spacing is a power of two x/2^k and x*2^-k round identically, otherwise
+// cdiv gives the IEEE quotient.
 template <bool POW2>
 BX_HD double courant_rate(double d, double p, double gam, double u1, double u2, double u3,
                           double dx, double dy, double dz, double idx, double idy,
@@ -95,7 +113,8 @@ BX_HD double courant_rate(double d, double p, double gam, double u1, double u2, 
   const double sound = sqrt(gam * p / d);
   if (POW2)
     return (sound + fabs(u1)) * idx + (sound + fabs(u2)) * idy + (sound + fabs(u3)) * idz;
-  return (sound + fabs(u1)) / dx + (sound + fabs(u2)) / dy + (sound + fabs(u3)) / dz;
+  return cdiv(sound + fabs(u1), dx, idx) + cdiv(sound + fabs(u2), dy, idy) +
+         cdiv(sound + fabs(u3), dz, idz);
 }
 
 // calculate_states for one cell and one direction (flux.f90:327-351):
@@ -112,8 +131,8 @@ BX_HD void muscl_states(const Prim& q, double ud, double sd, double su1, double 
     lp = lp * ids;
     lm = lm * ids;
   } else {
-    lp = lp / ds;
-    lm = lm / ds;
+    lp = cdiv(lp, ds, ids);
+    lm = cdiv(lm, ds, ids);
   }
   const double hm = kHalf * (-1.0 - lm);
   const double hp = kHalf * (1.0 - lp);
@@ -161,6 +180,7 @@ struct SharedDiv {
       const double e = fma(-d, q0, a);
       return fma(e, r, q0);
     }
+    if (ok && aa == 0.0) return a * r;  // signed zero, as a/d
     return a / d;
   }
 };

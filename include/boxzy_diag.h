@@ -16,7 +16,8 @@ extern "C" {
  * NULL) receives nothing (clocks are sampled by the caller).  Returns 0 on success. */
 int bx_fp64_peak(double *tflops, double *ms);
 
-/* Self-check of the shared-denominator division used by the HLL flux: n random
+/* Self-check of the divisions by a shared denominator (HLL flux) and by a grid
+ * constant with a precomputed reciprocal (cell sizes, cell volume): n random
  * (numerator, denominator) pairs with exponents in [-exp_range, exp_range] (plus
  * exact multiples and near-ties) are divided both ways on the device; returns the
  * number of results that differ from IEEE division in any bit (zeros of either

@@ -1,8 +1,10 @@
-"""The shared-denominator division of the HLL flux equals IEEE division bit for bit.
+"""The reciprocal-based divisions of the stage kernels equal IEEE division bit for bit.
 
-Each HLL face divides five flux numerators by the same wave-speed sum; the
-kernels compute one correctly rounded reciprocal and correct each quotient with
-an FMA residual.  This checks the device implementation against the device's
+Each HLL face divides five flux numerators by the same wave-speed sum, and the
+lambdas, the update and the Courant rate divide by the cell sizes and volume;
+the kernels compute one correctly rounded reciprocal (on the device for the
+wave-speed sum, on the host for the grid constants) and correct each quotient
+with an FMA residual.  This checks the device implementation against the device's
 IEEE double division on random operands (random mantissas and exponents inside
 and far outside the window where the short form is used, exact multiples and
 near-ties)."""
