@@ -95,6 +95,14 @@ def lib():
         "bx_batch_download": (C.c_int, [H, C.c_int32, vp, vp, vp]),
         "bx_batch_info": (C.c_int, [H, dp, i64p, i32p, i64p]),
         "bx_batch_last_error": (C.c_char_p, [H]),
+        "bx_adj_create": (C.c_int, [C.POINTER(BxParams), C.c_int64, C.c_int32, C.POINTER(H)]),
+        "bx_adj_destroy": (C.c_int, [H]),
+        "bx_adj_set_stream": (C.c_int, [H, vp]),
+        "bx_adj_forward": (C.c_int, [H, vp, vp, C.c_int32]),
+        "bx_adj_backward": (C.c_int, [H, vp, vp]),
+        "bx_adj_stats": (C.c_int, [H, dp, dp, i64p, i64p]),
+        "bx_adj_dts": (C.c_int, [H, dp]),
+        "bx_adj_last_error": (C.c_char_p, [H]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)

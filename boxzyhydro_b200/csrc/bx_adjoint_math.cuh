@@ -1,0 +1,125 @@
+// bx_adjoint_math.cuh -- vector-Jacobian products of the per-face and per-cell
+// arithmetic of the fused hydro step (bx_math.cuh), with every max/min/branch
+// frozen at the choice the forward values make.  Derivatives need not round
+// like the forward; they are written for clarity.
+#pragma once
+#include "bx_math.cuh"
+
+namespace bx {
+
+struct FS6 {  // a face state or its adjoint: rho, u1, u2, u3, p, eps
+  double d, u1, u2, u3, p, e;
+};
+
+__device__ __forceinline__ FS6 fs_zero() { return FS6{0, 0, 0, 0, 0, 0}; }
+
+// --- HLL flux (flux.f90:504-590): adjoints of the two face states from gF.
+template <int DIR>
+__device__ __forceinline__ void hll_vjp(const FaceState& L, const FaceState& R, double gam,
+                                        const double gF[5], FS6& gL, FS6& gR) {
+  const double dl = L.d, pl = L.p, el = L.e;
+  const double dr = R.d, pr = R.p, er = R.e;
+  const double ul[3] = {L.u1, L.u2, L.u3}, ur[3] = {R.u1, R.u2, R.u3};
+  const double vl = ul[DIR], vr = ur[DIR];
+  const double Kl = ul[0] * ul[0] + ul[1] * ul[1] + ul[2] * ul[2];
+  const double Kr = ur[0] * ur[0] + ur[1] * ur[1] + ur[2] * ur[2];
+  double sl[5], sr[5], fl[5], fr[5];
+  sl[0] = dl; sr[0] = dr;
+  for (int j = 0; j < 3; ++j) { sl[1 + j] = dl * ul[j]; sr[1 + j] = dr * ur[j]; }
+  sl[4] = el + kHalf * dl * Kl;
+  sr[4] = er + kHalf * dr * Kr;
+  fl[0] = sl[0] * vl; fr[0] = sr[0] * vr;
+  for (int j = 0; j < 3; ++j) {
+    fl[1 + j] = (j == DIR ? pl : 0.0) + sl[1 + j] * vl;
+    fr[1 + j] = (j == DIR ? pr : 0.0) + sr[1 + j] * vr;
+  }
+  fl[4] = (sl[4] + pl) * vl;
+  fr[4] = (sr[4] + pr) * vr;
+  const double cr = sqrt(gam * pr / dr), cl = sqrt(gam * pl / dl);
+  // ap = max(0, vr+cr, vl+cl), am = max(0, -(vr-cr), -(vl-cl)), evaluated as the forward
+  const double a1 = vr + cr, a2 = vl + cl;
+  const double b1 = -(vr - cr), b2 = -(vl - cl);
+  const double t1 = fmax(0.0, a1);
+  const double ap = fmax(t1, a2);
+  const int sap = (a2 > t1) ? 2 : (a1 > 0.0 ? 1 : 0);
+  const double t2 = fmax(0.0, b1);
+  const double am = fmax(t2, b2);
+  const int sam = (b2 > t2) ? 2 : (b1 > 0.0 ? 1 : 0);
+  const double D = ap + am;
+  double F[5], gN[5], gD = 0.0, gap = 0.0, gam_ = 0.0;
+  for (int k = 0; k < 5; ++k) {
+    F[k] = (ap * fl[k] + am * fr[k] - ap * am * (sr[k] - sl[k])) / D;
+    gN[k] = gF[k] / D;
+    gD -= gN[k] * F[k];
+  }
+  gap = gD;
+  gam_ = gD;
+  double gfl[5], gfr[5], gsl[5], gsr[5];
+  for (int k = 0; k < 5; ++k) {
+    const double ds = sr[k] - sl[k];
+    gap += gN[k] * (fl[k] - am * ds);
+    gam_ += gN[k] * (fr[k] - ap * ds);
+    gfl[k] = gN[k] * ap;
+    gfr[k] = gN[k] * am;
+    gsr[k] = -gN[k] * ap * am;
+    gsl[k] = gN[k] * ap * am;
+  }
+  double gvl = 0, gvr = 0, gcl = 0, gcr = 0;
+  if (sap == 1) { gvr += gap; gcr += gap; }
+  else if (sap == 2) { gvl += gap; gcl += gap; }
+  if (sam == 1) { gcr += gam_; gvr -= gam_; }
+  else if (sam == 2) { gcl += gam_; gvl -= gam_; }
+  double gpl = 0, gpr = 0, gdl = 0, gdr = 0, gel = 0, ger = 0;
+  double gul[3] = {0, 0, 0}, gur[3] = {0, 0, 0};
+  // sound speeds
+  if (cl > 0.0) { gpl += gcl * cl / (2.0 * pl); gdl -= gcl * cl / (2.0 * dl); }
+  if (cr > 0.0) { gpr += gcr * cr / (2.0 * pr); gdr -= gcr * cr / (2.0 * dr); }
+  // fluxes
+  gdl += gfl[0] * vl; gsl[0] += 0.0; gvl += gfl[0] * sl[0];
+  gdr += gfr[0] * vr; gvr += gfr[0] * sr[0];
+  for (int j = 0; j < 3; ++j) {
+    if (j == DIR) { gpl += gfl[1 + j]; gpr += gfr[1 + j]; }
+    gsl[1 + j] += gfl[1 + j] * vl; gvl += gfl[1 + j] * sl[1 + j];
+    gsr[1 + j] += gfr[1 + j] * vr; gvr += gfr[1 + j] * sr[1 + j];
+  }
+  gsl[4] += gfl[4] * vl; gpl += gfl[4] * vl; gvl += gfl[4] * (sl[4] + pl);
+  gsr[4] += gfr[4] * vr; gpr += gfr[4] * vr; gvr += gfr[4] * (sr[4] + pr);
+  // fl[0] = sl[0]*vl with sl[0] = dl was taken as dl*vl above (gfl0 -> gdl)
+  // conserved face variables
+  gdl += gsl[0]; gdr += gsr[0];
+  for (int j = 0; j < 3; ++j) {
+    gdl += gsl[1 + j] * ul[j]; gul[j] += gsl[1 + j] * dl;
+    gdr += gsr[1 + j] * ur[j]; gur[j] += gsr[1 + j] * dr;
+  }
+  gel += gsl[4]; gdl += gsl[4] * kHalf * Kl;
+  ger += gsr[4]; gdr += gsr[4] * kHalf * Kr;
+  for (int j = 0; j < 3; ++j) {
+    gul[j] += gsl[4] * dl * ul[j];
+    gur[j] += gsr[4] * dr * ur[j];
+  }
+  gul[DIR] += gvl;
+  gur[DIR] += gvr;
+  gL = FS6{gdl, gul[0], gul[1], gul[2], gpl, gel};
+  gR = FS6{gdr, gur[0], gur[1], gur[2], gpr, ger};
+}
+
+// --- generalised minmod slope: index of the selected argument (1: theta*(c1-c0),
+// 2: half*(c2-c0), 3: theta*(c2-c1)) or 0 when the slope is zero.
+__device__ __forceinline__ int slope_sel(double c0, double c1, double c2) {
+  const double d1 = c1 - c0, d2 = c2 - c0, d3 = c2 - c1;
+  const bool pos = (d1 > 0.0) && (d3 > 0.0), neg = (d1 < 0.0) && (d3 < 0.0);
+  if (!(pos || neg)) return 0;
+  const double x1 = fabs(kTheta * d1), x2 = fabs(kHalf * d2), x3 = fabs(kTheta * d3);
+  const double m23 = fmin(x2, x3);
+  if (x1 <= m23) return 1;
+  return x2 <= x3 ? 2 : 3;
+}
+// d slope / d (c0, c1, c2) for a selection
+__device__ __forceinline__ void slope_coef(int sel, double& k0, double& k1, double& k2) {
+  k0 = k1 = k2 = 0.0;
+  if (sel == 1) { k0 = -kTheta; k1 = kTheta; }
+  else if (sel == 2) { k0 = -kHalf; k2 = kHalf; }
+  else if (sel == 3) { k1 = -kTheta; k2 = kTheta; }
+}
+
+}  // namespace bx

@@ -171,6 +171,27 @@ int bx_batch_info(bx_batch *b, double *last_run_ms, int64_t *launches, int32_t *
                   int64_t *cells);
 const char *bx_batch_last_error(bx_batch *b);
 
+/* ---- Discrete adjoint.  No counterpart in the reference.  Reverse-mode derivative
+ * of an nsteps-step run of the fused stage kernels (the step of bx_step on grids whose
+ * ghost plan resolves), with the dt sequence of the forward run held fixed and every
+ * limiter/max/min branch taken as in the forward.  Device arrays are SoA planes
+ * (5 x ngrid doubles, rho, m1, m2, m3, E) of the reference cons; ghost entries of
+ * the inputs are ignored and those of gradients are zero.  Snapshots follow a
+ * binomial schedule in `snapshots` plane sets. */
+typedef struct bx_adj bx_adj;
+int bx_adj_create(const bx_params *params, int64_t nsteps, int32_t snapshots, bx_adj **out);
+int bx_adj_destroy(bx_adj *a);
+int bx_adj_set_stream(bx_adj *a, void *cuda_stream);
+/* frozen=0: dt by the CFL rule (main.f90:266-281) and recorded; frozen=1: the recorded
+ * dt sequence (for finite differences).  BX_ERR_STATE if a guard fired. */
+int bx_adj_forward(bx_adj *a, const double *cons0, double *consT, int32_t frozen);
+/* lam0 = (d consT / d cons0)^T lamT for the last unfrozen forward run */
+int bx_adj_backward(bx_adj *a, const double *lamT, double *lam0);
+int bx_adj_stats(bx_adj *a, double *ms_forward, double *ms_backward, int64_t *recomputed_steps,
+                 int64_t *device_bytes);
+int bx_adj_dts(bx_adj *a, double *dts);
+const char *bx_adj_last_error(bx_adj *a);
+
 /* No counterpart in the reference.  One set_ghost_cells sweep -- the same result as
  * bx_ghost -- that allocates nothing, for callers that cannot allocate device memory
  * (a host program that has reserved the device's memory for its own pool, or a

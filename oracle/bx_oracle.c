@@ -707,6 +707,38 @@ int ox_step(ox_sim *s, double endtime) {
   return 0;
 }
 
+/* main.f90:212-545 with the full step dt given instead of the CFL rule
+ * (finite differences of a run with its dt sequence held fixed) */
+void ox_step_dt(ox_sim *s, double dt_full) {
+  s->step = s->step + 1;
+  ox_state(s);
+  ox_courant(s);
+  s->dt = dt_full;
+  s->dtold = s->dt;
+  s->dt = s->dt * HALF;
+  ox_source(s, 0);
+  ox_set_ghost_cells(s);
+  ox_state(s);
+  ox_velocity(s);
+  ox_save_cons_old(s);
+  s->dt = s->dt * TWO;
+  ox_flux(s, 0);
+  ox_set_ghost_cells(s);
+  ox_state(s);
+  ox_velocity(s);
+  ox_flux(s, 1);
+  ox_set_ghost_cells(s);
+  ox_state(s);
+  ox_velocity(s);
+  s->dt = HALF * s->dt;
+  ox_source(s, 1);
+  ox_set_ghost_cells(s);
+  ox_state(s);
+  ox_velocity(s);
+  s->dt = s->dt * TWO;
+  s->time = s->time + s->dt;
+}
+
 int64_t ox_run(ox_sim *s, double endtime, int64_t nsteps) {
   int64_t n = 0;
   while (n < nsteps) {

@@ -73,6 +73,8 @@ void ox_save_cons_old(ox_sim *s);
 /* one iteration of the main loop (main.f90:212-545); returns 0 if it ran,
  * 1 if the loop would have exited (time>=endtime). */
 int ox_step(ox_sim *s, double endtime);
+/* one iteration with the full step dt given (dt sequence held fixed) */
+void ox_step_dt(ox_sim *s, double dt_full);
 /* run until time>=endtime or nsteps steps were taken; returns steps taken */
 int64_t ox_run(ox_sim *s, double endtime, int64_t nsteps);
 

@@ -68,6 +68,7 @@ def lib():
         L.ox_flux.argtypes = [P, C.c_int]
         L.ox_step.argtypes = [P, C.c_double]
         L.ox_step.restype = C.c_int
+        L.ox_step_dt.argtypes = [P, C.c_double]
         L.ox_run.argtypes = [P, C.c_double, C.c_int64]
         L.ox_run.restype = C.c_int64
         L.ox_set_threads.argtypes = [C.c_int]
@@ -193,6 +194,9 @@ class Oracle:
 
     def step(self, endtime=1e300):
         return lib().ox_step(self._h, float(endtime)) == 0
+
+    def step_dt(self, dt_full):
+        lib().ox_step_dt(self._h, float(dt_full))
 
     def run(self, endtime=1e300, nsteps=1 << 62):
         return int(lib().ox_run(self._h, float(endtime), int(nsteps)))

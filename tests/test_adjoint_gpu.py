@@ -1,0 +1,158 @@
+"""Discrete adjoint of a run (bx_adj_*): dot-product test against the tangent-linear
+model (oracle/tangent.py), finite differences of the GPU forward and of the CPU
+oracle, checkpoint schedules, and the torch.autograd.Function."""
+import numpy as np
+import pytest
+
+import oracle as O
+import tangent as TLM
+from boxzyhydro_b200 import grid as G
+from boxzyhydro_b200.adjoint import AdjointEngine, AdjointRun
+from tests.helpers import small_random_box
+
+pytestmark = pytest.mark.gpu
+
+
+def _torch():
+    import torch
+    return torch
+
+
+def interior_mask(hp):
+    return G.boundary_flags(hp.nx, hp.ny, hp.nz) == 0
+
+
+def setup(walls=(0,) * 6, dims=(14, 12, 11), nsteps=4, snaps=2, seed=0, amp=0.25):
+    st = small_random_box(nx=dims[0], ny=dims[1], nz=dims[2], walls=walls, seed=seed, amp=amp,
+                          cfl=0.4)
+    # ghosts as the donor rule fills them, so the oracle starts from the same state
+    from boxzyhydro_b200.hydro import apply_ghost_plan, ghost_plan
+    pl = ghost_plan(st.params)
+    st.cons[:] = apply_ghost_plan(st.cons, pl["src2"], pl["sgn2"], pl["dst"])
+    st.u[:] = st.cons[:, 1:4] / st.cons[:, :1]
+    eng = AdjointEngine(st.params, nsteps, snaps)
+    return st, eng
+
+
+def fwd(eng, cons, frozen):
+    torch = _torch()
+    c0 = torch.tensor(np.ascontiguousarray(cons.T), device="cuda")
+    out = torch.empty_like(c0)
+    torch.cuda.synchronize()
+    eng.forward_ptr(c0.data_ptr(), out.data_ptr(), frozen=frozen)
+    return out.cpu().numpy().T.copy()
+
+
+def bwd(eng, lamT):
+    torch = _torch()
+    l = torch.tensor(np.ascontiguousarray(lamT.T), device="cuda")
+    out = torch.empty_like(l)
+    torch.cuda.synchronize()
+    eng.backward_ptr(l.data_ptr(), out.data_ptr())
+    return out.cpu().numpy().T.copy()
+
+
+def rand_dir(hp, rng, scale):
+    m = interior_mask(hp)
+    v = rng.standard_normal((hp.ngrid, 5)) * scale
+    v[~m] = 0.0
+    return v
+
+
+@pytest.mark.parametrize("walls,dims", [((0,) * 6, (14, 12, 11)),
+                                        ((1, 1, 1, 1, 1, 1), (40, 9, 4)),
+                                        ((0, 1, 1, 0, 0, 1), (13, 12, 10))])
+def test_dot_product(walls, dims):
+    st, eng = setup(walls, dims)
+    hp = st.params
+    consT = fwd(eng, st.cons, frozen=False)
+    dts = eng.dts()
+    rng = np.random.default_rng(7)
+    scale = np.array([1.0, 0.3, 0.3, 0.3, 2.0])
+    v = rand_dir(hp, rng, scale)
+    cT, dT = TLM.run(hp, st.cons, v, dts)
+    m = interior_mask(hp)
+    assert np.allclose(cT[m], consT[m], rtol=1e-13, atol=0), "TLM forward differs from GPU"
+    lamT = rand_dir(hp, rng, np.ones(5))
+    lam0 = bwd(eng, lamT)
+    assert np.all(lam0[~m] == 0.0)
+    d1 = float(np.sum(lamT[m] * dT[m]))
+    d2 = float(np.sum(lam0[m] * v[m]))
+    assert abs(d1 - d2) <= 1e-12 * abs(d1), (d1, d2)
+    eng.close()
+
+
+def test_finite_differences_gpu_and_oracle():
+    st, eng = setup()
+    hp = st.params
+    fwd(eng, st.cons, frozen=False)
+    dts = eng.dts()
+    rng = np.random.default_rng(11)
+    m = interior_mask(hp)
+    lamT = np.zeros((hp.ngrid, 5))
+    lamT[m, 0] = rng.standard_normal(m.sum())
+    lam0 = bwd(eng, lamT)
+    for k in range(3):
+        v = rand_dir(hp, rng, np.array([1.0, 0.3, 0.3, 0.3, 2.0]))
+        adj = float(np.sum(lam0[m] * v[m]))
+        h = 1e-7
+        # GPU forward with the frozen dt sequence
+        fp = fwd(eng, st.cons + h * v, frozen=True)
+        fm = fwd(eng, st.cons - h * v, frozen=True)
+        fd = float(np.sum(lamT[m] * (fp[m] - fm[m]))) / (2 * h)
+        assert abs(fd - adj) <= 1e-6 * abs(adj), (fd, adj)
+        # the oracle (CPU restatement of the reference loop) with the same dts
+        vals = []
+        for sgn in (1.0, -1.0):
+            c = st.cons + sgn * h * v
+            from boxzyhydro_b200.hydro import apply_ghost_plan, ghost_plan
+            pl = ghost_plan(hp)
+            c = apply_ghost_plan(c, pl["src2"], pl["sgn2"], pl["dst"])
+            o = O.Oracle(hp)
+            o.set_state(c, c[:, 1:4] / c[:, :1], np.ones(hp.ngrid), np.full(hp.ngrid, hp.gammafix))
+            for dt in dts:
+                o.step_dt(dt)
+            vals.append(o.get_state()[0])
+            o.close()
+        fdo = float(np.sum(lamT[m] * (vals[0][m] - vals[1][m]))) / (2 * h)
+        assert abs(fdo - adj) <= 1e-6 * abs(adj), (fdo, adj)
+    eng.close()
+
+
+def test_checkpoint_schedules_agree():
+    st, eng1 = setup(nsteps=6, snaps=1)
+    hp = st.params
+    fwd(eng1, st.cons, frozen=False)
+    rng = np.random.default_rng(3)
+    lamT = rand_dir(hp, rng, np.ones(5))
+    ref = bwd(eng1, lamT)
+    s1 = eng1.stats()
+    eng1.close()
+    for snaps in (2, 3, 6):
+        eng = AdjointEngine(hp, 6, snaps)
+        fwd(eng, st.cons, frozen=False)
+        got = bwd(eng, lamT)
+        assert np.array_equal(got, ref), snaps
+        st_ = eng.stats()
+        assert st_["recomputed_steps"] <= s1["recomputed_steps"]
+        eng.close()
+
+
+def test_torch_autograd_function():
+    torch = _torch()
+    st, eng = setup()
+    hp = st.params
+    m = torch.tensor(interior_mask(hp), device="cuda")
+    c0 = torch.tensor(np.ascontiguousarray(st.cons.T), device="cuda", requires_grad=True)
+    cT = AdjointRun.apply(c0, eng)
+    target = cT.detach()[0] * 1.01
+    loss = 0.5 * torch.sum(((cT[0] - target) * m) ** 2)
+    loss.backward()
+    lamT = torch.zeros_like(cT)
+    lamT[0] = (cT.detach()[0] - target) * m
+    ref = torch.empty_like(lamT)
+    eng.backward_ptr(lamT.contiguous().data_ptr(), ref.data_ptr())
+    torch.cuda.synchronize()
+    assert torch.equal(c0.grad, ref)
+    assert float(torch.abs(c0.grad).sum()) > 0
+    eng.close()
