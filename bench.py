@@ -281,6 +281,99 @@ def batched_arm(args, rank, world, local):
     return 0
 
 
+def adjoint_arm(args, rank, world, local):
+    """C4/C5: discrete adjoint of an n^3 run of `steps` steps.  Loss
+    0.5*||rho(T) - rho_target||^2 over interior cells, rho_target from the run of
+    the unperturbed state; gradient w.r.t. the initial rho, m, E.  Reports the
+    adjoint/forward device-time ratio, device memory, recomputed steps and the
+    agreement with central finite differences (dt sequence held fixed) along
+    seeded random directions."""
+    import numpy as np
+    import torch
+
+    from boxzyhydro_b200 import grid as G
+    from boxzyhydro_b200 import ic
+    from boxzyhydro_b200.adjoint import AdjointEngine
+
+    torch.cuda.set_device(local)
+    n = args.n
+    if args.adj_ic == "blob":
+        st = ic.sod_blob_box(n=n, seed=args.seed)
+        st0 = ic.sod_blob_box(n=n, seed=args.seed, blob=False)
+        ic_name = "x-split Sod state + seeded 5% Gaussian density blob, outflow walls"
+    else:
+        st = ic.turbulent_box(n=n, seed=args.seed)
+        st0 = None
+        ic_name = "lognormal/solenoidal turbulent state, outflow walls"
+    hp = st.params
+    dev = torch.device("cuda", local)
+    m = torch.tensor(G.boundary_flags(hp.nx, hp.ny, hp.nz) == 0, device=dev)
+    eng = AdjointEngine(hp, args.steps, args.snapshots)
+    stream = torch.cuda.Stream()
+    eng.set_stream(stream.cuda_stream)
+
+    def run(c, frozen):
+        out = torch.empty_like(c)
+        torch.cuda.synchronize()
+        eng.forward_ptr(c.data_ptr(), out.data_ptr(), frozen=frozen)
+        return out
+
+    c0 = torch.tensor(np.ascontiguousarray(st.cons.T), device=dev)
+    del st
+    if st0 is not None:
+        target = run(torch.tensor(np.ascontiguousarray(st0.cons.T), device=dev), False)[0].clone()
+        del st0
+    else:
+        target = None
+    cT = run(c0, False)
+    if target is None:
+        target = cT[0] * 1.01
+    lamT = torch.zeros_like(cT)
+    lamT[0] = (cT[0] - target) * m
+    loss = 0.5 * float(torch.sum(lamT[0] ** 2))
+    stats_fwd = eng.stats()
+    grad = torch.empty_like(cT)
+    torch.cuda.synchronize()
+    eng.backward_ptr(lamT.data_ptr(), grad.data_ptr())
+    torch.cuda.synchronize()
+    stt = eng.stats()
+    ratio = stt["ms_backward"] / stats_fwd["ms_forward"]
+    # finite differences with the frozen dt sequence
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(args.seed + 99)
+    scale = torch.tensor([1.0, 0.3, 0.3, 0.3, 2.0], device=dev, dtype=torch.float64)[:, None]
+    rel = []
+    for k in range(args.fd_dirs):
+        v = torch.randn(cT.shape, generator=gen, device=dev, dtype=torch.float64) * scale * m
+        h = 1e-7
+        lp = run(c0 + h * v, True)[0]
+        lm = run(c0 - h * v, True)[0]
+        fd = float(torch.sum(((lp - target) ** 2 - (lm - target) ** 2) * m)) * 0.5 / (2 * h)
+        adj = float(torch.sum(grad * v))
+        rel.append(abs(fd - adj) / max(abs(adj), 1e-300))
+    line = {
+        "metric": "adjoint/forward time ratio", "value": ratio, "unit": "x",
+        "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": 0,
+        "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"discrete adjoint, {n}^3 interior, gamma=5/3, {ic_name}, "
+                               f"{args.steps} steps, loss 0.5||rho(T)-rho_target||^2",
+                   "snapshots": args.snapshots},
+        "ms_forward": stats_fwd["ms_forward"], "ms_backward": stt["ms_backward"],
+        "forward_cell_updates_per_s": hp.n_active() * args.steps / (stats_fwd["ms_forward"] * 1e-3),
+        "recomputed_steps": stt["recomputed_steps"],
+        "recompute_fraction": stt["recomputed_steps"] / args.steps,
+        "device_bytes": stt["device_bytes"],
+        "peak_device_bytes_torch": torch.cuda.max_memory_allocated(dev),
+        "loss": loss,
+        "fd_check": {"directions": args.fd_dirs, "h": 1e-7, "max_rel_diff": max(rel) if rel else None,
+                     "median_rel_diff": float(np.median(rel)) if rel else None},
+    }
+    eng.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -294,7 +387,10 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2, dest="cpu_steps")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="turb", choices=["turb", "batched"])
+    ap.add_argument("--workload", default="turb", choices=["turb", "batched", "adjoint"])
+    ap.add_argument("--snapshots", type=int, default=15)
+    ap.add_argument("--fd-dirs", type=int, default=16, dest="fd_dirs")
+    ap.add_argument("--adj-ic", default="blob", choices=["blob", "turb"], dest="adj_ic")
     ap.add_argument("--nbox", type=int, default=4096)
     ap.add_argument("--check-boxes", type=int, default=16, dest="check_boxes")
     ap.add_argument("--loop-sample", type=int, default=8, dest="loop_sample")
@@ -308,6 +404,8 @@ def main():
         return reference_arm(args, rank)
     if args.workload == "batched":
         return batched_arm(args, rank, world, local)
+    if args.workload == "adjoint":
+        return adjoint_arm(args, rank, world, local)
 
     import numpy as np
     import torch

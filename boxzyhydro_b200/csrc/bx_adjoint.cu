@@ -10,18 +10,19 @@
 // fixed; every max/min/limiter branch is taken where the forward values put it;
 // the floors of flux.f90:223-230 must not fire in the forward (checked).
 //
-// The reverse of one stage runs five kernels over full-grid scratch planes:
-//  R1 primitives of every cell;  R2 per face: recompute the two face states
-//  and the HLL flux, and turn the flux adjoint into the adjoints of the plus
-//  state of the low cell and the minus state of the high cell (each written by
-//  exactly one face: no atomics);  R3 per cell: adjoint of the MUSCL states
-//  into direct primitive adjoints and slope adjoints;  R4 per cell: gather the
-//  slope adjoints of the (up to three) slopes that read this cell's
-//  primitives, then primitives -> conserved variables;  R5 per interior cell:
-//  add the adjoints that landed on face ghosts back onto their donor cells.
+// The reverse of one stage runs, with two scratch plane sets of 7 (primitives
+// P and their adjoints PA) beside the state planes:
+//  k_r1_prims  primitives of every cell;
+//  k_rdir<d>   for each direction, line segments in shared memory: face states
+//              and the HLL derivative of every face once, the MUSCL and slope
+//              derivatives, summed into PA (no atomics: each cell of a line
+//              belongs to one segment, the directions run one after another);
+//  k_rcell     per interior cell: primitives -> conserved variables for the cell
+//              and the face ghosts it donates to, then the step combination
+//              (and, for stage 0, the sources of the step input).
 //
-// Snapshots follow a binomial (revolve-style) schedule in a fixed pool of
-// plane sets, so a run of any length is reversed in bounded memory.
+// Snapshots follow a checkpoint schedule over a fixed pool of plane sets (see
+// build_schedule), so a run of any length is reversed in bounded memory.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -86,11 +87,11 @@ __device__ __forceinline__ void decode(const Geom& g, long long i, int& x, int& 
 
 // ---- primitives of a stage (as load_prim of the stage kernels)
 // P planes: 0 rho, 1-3 u, 4 p, 5 eps, 6 c
+// grid: x threads by (y, z) blocks
 __global__ void k_r1_prims(Geom g, int stage, const double* A, const double* B, double* P) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= g.ng) return;
-  int x, y, z;
-  decode(g, i, x, y, z);
+  const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
+  if (x >= g.nx) return;
+  const long long i = x + (long long)y * g.sy + (long long)z * g.sz;
   const long long n = g.ng;
   const C5 a = aload(A, n, g, x, y, z);
   const double u1 = a.m1 / a.d, u2 = a.m2 / a.d, u3 = a.m3 / a.d;
@@ -112,263 +113,400 @@ __global__ void k_r1_prims(Geom g, int stage, const double* A, const double* B, 
   P[6 * n + i] = sqrt(p * g.gam / a.d);
 }
 
-__device__ __forceinline__ Prim pget(const double* P, long long n, long long i) {
-  return Prim{P[i], P[n + i], P[2 * n + i], P[3 * n + i], P[4 * n + i], P[5 * n + i],
-              P[6 * n + i]};
-}
-__device__ __forceinline__ double pq(const Prim& q, int k) {
-  return k == 0 ? q.d : k == 1 ? q.u1 : k == 2 ? q.u2 : k == 3 ? q.u3 : k == 4 ? q.p : q.e;
-}
-__device__ __forceinline__ double fq(const FS6& q, int k) {
-  return k == 0 ? q.d : k == 1 ? q.u1 : k == 2 ? q.u2 : k == 3 ? q.u3 : k == 4 ? q.p : q.e;
-}
-__device__ __forceinline__ double ud_of(const Prim& q, int dir) {
-  return dir == 0 ? q.u1 : dir == 1 ? q.u2 : q.u3;
-}
-
-// face states of cell i in direction dir (ghost cells: the cell values)
-__device__ __forceinline__ void states_of(const Geom& g, const double* P, long long i, long long st,
-                                          bool interior, int dir, double dt, FaceState& mi,
-                                          FaceState& pl) {
+// ---- conserved-variable VJP at cell (x,y,z) of a stage: gq holds the adjoints
+// of the primitives rho, u1, u2, u3, p, eps, c (whose values are in the P planes
+// at index pi; a ghost's primitives are its donor's through the donor rule);
+// returns the adjoints of A's (gA) and, for stage 1, B's (gB) conserved values
+// at that location.  Branches (the eps floors) are taken as the forward took
+// them: eps > small_eps exactly when the floor did not fire.
+__device__ __forceinline__ void cons_vjp(const Geom& g, int stage, const double* P, long long pi,
+                                         const double* A, const double* B, int x, int y, int z,
+                                         const double gq[7], double gA[5], double gB[5]) {
   const long long n = g.ng;
-  const Prim c = pget(P, n, i);
-  if (!interior) {
-    ghost_states(c, mi, pl);
-    return;
-  }
-  const Prim m = pget(P, n, i - st), p = pget(P, n, i + st);
-  const double ds = dir == 0 ? g.dx : dir == 1 ? g.dy : g.dz;
-  const double ids = dir == 0 ? g.idx : dir == 1 ? g.idy : g.idz;
-  const double sd = slope3(m.d, c.d, p.d), s1 = slope3(m.u1, c.u1, p.u1);
-  const double s2 = slope3(m.u2, c.u2, p.u2), s3 = slope3(m.u3, c.u3, p.u3);
-  const double sp = slope3(m.p, c.p, p.p), se = slope3(m.e, c.e, p.e);
-  if (g.pow2)
-    muscl_states<true>(c, ud_of(c, dir), sd, s1, s2, s3, sp, se, dt, ds, ids, mi, pl);
-  else
-    muscl_states<false>(c, ud_of(c, dir), sd, s1, s2, s3, sp, se, dt, ds, ids, mi, pl);
-}
-
-// G planes: [(dir*2 + side)*6 + q], side 0 = minus-state adjoint, 1 = plus-state adjoint
-// R2: faces of direction DIR; thread per high-side cell (index along DIR in [a0, a1])
-template <int DIR>
-__global__ void k_r2_faces(Geom g, const double* P, const double* lamL, double dt, double* G) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= g.ng) return;
-  int x, y, z;
-  decode(g, i, x, y, z);
-  const int c[3] = {x, y, z};
-  const int lo[3] = {g.ax0, g.ay0, g.az0}, hi[3] = {g.ax1, g.ay1, g.az1};
-  for (int k = 0; k < 3; ++k) {
-    if (k == DIR) {
-      if (c[k] < lo[k] || c[k] > hi[k]) return;
-    } else if (k < 2 || g.threed) {
-      if (c[k] < lo[k] || c[k] >= hi[k]) return;
-    }
-  }
-  const long long n = g.ng;
-  const long long st = DIR == 0 ? 1 : DIR == 1 ? g.sy : g.sz;
-  const long long L = i - st, R = i;
-  int lx = x, ly = y, lz = z;
-  if (DIR == 0) lx -= 1; else if (DIR == 1) ly -= 1; else lz -= 1;
-  const bool Lin = ainterior(g, lx, ly, lz), Rin = ainterior(g, x, y, z);
-  FaceState Lm, Lp, Rm, Rp;
-  states_of(g, P, L, st, Lin, DIR, dt, Lm, Lp);
-  states_of(g, P, R, st, Rin, DIR, dt, Rm, Rp);
-  const double area = DIR == 0 ? g.ayz : DIR == 1 ? g.axz : g.axy;
-  const double coef = -(dt / g.vol) * area;
-  double gF[5];
-  for (int q = 0; q < 5; ++q) {
-    const double lL = Lin ? lamL[q * n + L] : 0.0;
-    const double lR = Rin ? lamL[q * n + R] : 0.0;
-    gF[q] = coef * (lL - lR);
-  }
-  FS6 gL, gR;
-  hll_vjp<DIR>(Lp, Rm, g.gam, gF, gL, gR);
-  double* Gp = G + ((DIR * 2 + 1) * 6) * n;
-  double* Gm = G + ((DIR * 2 + 0) * 6) * n;
-  for (int q = 0; q < 6; ++q) {
-    Gp[q * n + L] = fq(gL, q);
-    Gm[q * n + R] = fq(gR, q);
-  }
-}
-
-// R3: MUSCL adjoint per cell.  LQ planes: 7 direct primitive adjoints (q0..5, c);
-// LS planes: [dir*6 + q] slope adjoints; SEL: [dir*6 + q] slope selections.
-__global__ void k_r3_muscl(Geom g, const double* P, const double* G, double dt, double* LQ,
-                           double* LS, uint8_t* SEL) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= g.ng) return;
-  int x, y, z;
-  decode(g, i, x, y, z);
-  const long long n = g.ng;
-  const bool in = ainterior(g, x, y, z);
-  double lq[7] = {0, 0, 0, 0, 0, 0, 0};
-  const int ndir = g.threed ? 3 : 2;
-  const Prim c = pget(P, n, i);
-  for (int dir = 0; dir < ndir; ++dir) {
-    double gm[6], gp[6];
-    for (int q = 0; q < 6; ++q) {
-      gm[q] = G[((dir * 2 + 0) * 6 + q) * n + i];
-      gp[q] = G[((dir * 2 + 1) * 6 + q) * n + i];
-    }
-    if (!in) {
-      for (int q = 0; q < 6; ++q) lq[q] += gm[q] + gp[q];
-      continue;
-    }
-    const long long st = dir == 0 ? 1 : dir == 1 ? g.sy : g.sz;
-    const Prim m = pget(P, n, i - st), p = pget(P, n, i + st);
-    double s[6];
-    for (int q = 0; q < 6; ++q) {
-      const double c0 = pq(m, q), c1 = pq(c, q), c2 = pq(p, q);
-      s[q] = slope3(c0, c1, c2);
-      SEL[(dir * 6 + q) * n + i] = (uint8_t)slope_sel(c0, c1, c2);
-    }
-    const double ud = ud_of(c, dir);
-    const double ds = dir == 0 ? g.dx : dir == 1 ? g.dy : g.dz;
-    const double rr = dt / ds;
-    const double lp = fmax(ud + c.c, 0.0) * rr, lm = fmin(ud - c.c, 0.0) * rr;
-    const double hm = kHalf * (-1.0 - lm), hp = kHalf * (1.0 - lp);
-    double ghm = 0, ghp = 0;
-    for (int q = 0; q < 6; ++q) {
-      lq[q] += gm[q] + gp[q];
-      LS[(dir * 6 + q) * n + i] = hm * gm[q] + hp * gp[q];
-      ghm += s[q] * gm[q];
-      ghp += s[q] * gp[q];
-    }
-    const double glm = -kHalf * ghm, glp = -kHalf * ghp;
-    if (ud + c.c > 0.0) { lq[1 + dir] += glp * rr; lq[6] += glp * rr; }
-    if (ud - c.c < 0.0) { lq[1 + dir] += glm * rr; lq[6] -= glm * rr; }
-  }
-  if (!in)
-    for (int k = 0; k < 18; ++k) { LS[k * n + i] = 0.0; SEL[k * n + i] = 0; }
-  else if (!g.threed)
-    for (int k = 12; k < 18; ++k) { LS[k * n + i] = 0.0; SEL[k * n + i] = 0; }
-  for (int q = 0; q < 7; ++q) LQ[q * n + i] = lq[q];
-}
-
-// R4: total primitive adjoint of cell k, then primitives -> conserved.
-// GK planes: 0-4 adjoint of A's conserved values at k, 5-9 of B's (stage 1).
-__global__ void k_r4_cells(Geom g, int stage, const double* A, const double* B, const double* P,
-                           const double* LQ, const double* LS, const uint8_t* SEL, double* GK) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= g.ng) return;
-  int x, y, z;
-  decode(g, i, x, y, z);
-  const long long n = g.ng;
-  double gq[7];
-  for (int q = 0; q < 7; ++q) gq[q] = LQ[q * n + i];
-  const int ndir = g.threed ? 3 : 2;
-  const int c[3] = {x, y, z};
-  const int lim[3] = {g.nx, g.ny, g.nz};
-  for (int dir = 0; dir < ndir; ++dir) {
-    const long long st = dir == 0 ? 1 : dir == 1 ? g.sy : g.sz;
-    // slopes of cells j = i - st (i is its plus neighbour), i, i + st (i is its minus neighbour)
-    for (int o = -1; o <= 1; ++o) {
-      const int cj = c[dir] + o;
-      if (cj < 0 || cj >= lim[dir]) continue;
-      const long long j = i + o * st;
-      int jx = x, jy = y, jz = z;
-      if (dir == 0) jx = cj; else if (dir == 1) jy = cj; else jz = cj;
-      if (!ainterior(g, jx, jy, jz)) continue;
-      for (int q = 0; q < 6; ++q) {
-        const int sel = SEL[(dir * 6 + q) * n + j];
-        if (!sel) continue;
-        double k0, k1, k2;
-        slope_coef(sel, k0, k1, k2);
-        const double kk = o == 1 ? k0 : (o == 0 ? k1 : k2);
-        gq[q] += kk * LS[(dir * 6 + q) * n + j];
-      }
-    }
-  }
-  // primitives -> conserved values (load through the donor rule, like R1)
-  const C5 a = aload(A, n, g, x, y, z);
-  const double rho = a.d;
-  const double u[3] = {a.m1 / rho, a.m2 / rho, a.m3 / rho};
-  const double K = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
-  const double e = recon_eps(rho, a.E, u[0], u[1], u[2], g.small_eps);
-  double p;
-  double gA[5] = {0, 0, 0, 0, 0}, gB[5] = {0, 0, 0, 0, 0};
+  const double rho = P[pi], u[3] = {P[n + pi], P[2 * n + pi], P[3 * n + pi]};
+  const double p = P[4 * n + pi], e = P[5 * n + pi], cs = P[6 * n + pi];
+  const double ir = 1.0 / rho;
+  for (int q = 0; q < 5; ++q) gA[q] = gB[q] = 0.0;
   double grho = gq[0], gu[3] = {gq[1], gq[2], gq[3]}, gp = gq[4], ge = gq[5];
-  C5 b{};
-  double us[3] = {0, 0, 0};
-  if (stage == 0) {
-    p = e * g.gm1;
-  } else {
-    b = aload(B, n, g, x, y, z);
-    us[0] = b.m1 / b.d; us[1] = b.m2 / b.d; us[2] = b.m3 / b.d;
-    p = eos_pressure(rho, a.E, us[0], us[1], us[2], g.gm1, g.small_eps);
-  }
-  const double cs = sqrt(p * g.gam / rho);
   if (cs > 0.0) {
-    gp += gq[6] * cs / (2.0 * p);
-    grho -= gq[6] * cs / (2.0 * rho);
+    // c = sqrt(gam p / rho)
+    const double h = kHalf * gq[6] * cs;
+    gp += h / p;
+    grho -= h * ir;
   }
   if (stage == 0) {
     ge += gp * g.gm1;
   } else {
+    // p = max(E - rho K(u*)/2, eps)(gam-1) with u* = m/rho of B (main.f90:351-355)
+    const C5 a = aload(A, n, g, x, y, z);
+    const C5 b = aload(B, n, g, x, y, z);
+    const double us[3] = {b.m1 / b.d, b.m2 / b.d, b.m3 / b.d};
     const double Ks = us[0] * us[0] + us[1] * us[1] + us[2] * us[2];
     if (a.E - rho * kHalf * Ks > g.small_eps) {
-      gA[4] += gp * g.gm1;
-      grho += gp * g.gm1 * (-kHalf * Ks);
-      double gus[3];
-      for (int j = 0; j < 3; ++j) gus[j] = gp * g.gm1 * (-rho * us[j]);
+      const double gpg = gp * g.gm1, ib = 1.0 / b.d;
+      gA[4] += gpg;
+      grho = fma(gpg, -kHalf * Ks, grho);
       for (int j = 0; j < 3; ++j) {
-        gB[1 + j] += gus[j] / b.d;
-        gB[0] -= gus[j] * us[j] / b.d;
+        const double gus = gpg * (-rho * us[j]) * ib;
+        gB[1 + j] += gus;
+        gB[0] = fma(-gus, us[j], gB[0]);
       }
     }
   }
-  if (a.E - kHalf * rho * K > g.small_eps) {
+  if (e > g.small_eps) {
+    const double K = u[0] * u[0] + u[1] * u[1] + u[2] * u[2];
     gA[4] += ge;
-    grho += ge * (-kHalf * K);
-    for (int j = 0; j < 3; ++j) gu[j] += ge * (-rho * u[j]);
+    grho = fma(ge, -kHalf * K, grho);
+    for (int j = 0; j < 3; ++j) gu[j] = fma(ge, -rho * u[j], gu[j]);
   }
   for (int j = 0; j < 3; ++j) {
-    gA[1 + j] += gu[j] / rho;
-    grho -= gu[j] * u[j] / rho;
+    const double t = gu[j] * ir;
+    gA[1 + j] += t;
+    grho = fma(-t, u[j], grho);
   }
   gA[0] += grho;
-  for (int q = 0; q < 5; ++q) {
-    GK[q * n + i] = gA[q];
-    GK[(5 + q) * n + i] = gB[q];
+}
+
+// ---- reverse of the faces of one direction, line by line.
+// A line is a row of cells along DIR at interior coordinates in the other
+// directions, from the ghost below the interior (lo-1) to the ghost above (hi);
+// those are exactly the cells the DIR faces of the stage touch.  A block takes NL
+// lines and a segment of W cells [s0, s0+W) of each, with a halo of 3, and in
+// shared memory:
+//  P1 loads the primitives of [s0-3, s0+W+3);
+//  P2 forms the face states (MUSCL, the forward's own arithmetic), slopes and
+//     slope selections of [s0-2, s0+W+2);
+//  P3 differentiates the HLL flux of each face with high cell in [s0-1, s0+W+1]
+//     (flux adjoint coef*(lam_low - lam_high) from the interior cells' adjoints);
+//  P4 takes each cell of [s0-1, s0+W] back through its MUSCL states: direct
+//     primitive adjoints and the adjoints of its six slopes;
+//  P5 gathers, for the cells of the segment, their direct adjoints and the
+//     slope adjoints of the (up to three) slopes that read them, and adds the
+//     sum to PA (7 planes: rho, u1, u2, u3, p, eps, c).
+// Each face's states and HLL derivative are computed once.
+// Segment shape: a line of Lc cells is cut into nseg equal segments of W <= wmax
+// cells, and a block takes NL = floor(target/(W+4)) lines, so the state, face
+// and MUSCL phases (W+4, W+3, W+2 cells per line) each take one pass of the
+// block.  Blocks of about 128 threads: four per SM (registers), so the
+// barrier-separated phases of different blocks overlap.
+struct RShape {
+  int NL, W, NQ, NS, NF, ND, nseg, threads;
+  size_t r1, r2, r3, smem;  // region sizes in doubles; smem in bytes
+};
+
+static RShape rshape(int Lc, int wmax, int target) {
+  RShape r{};
+  r.nseg = (Lc + wmax - 1) / wmax;
+  r.W = (Lc + r.nseg - 1) / r.nseg;
+  r.NQ = r.W + 6; r.NS = r.W + 4; r.NF = r.W + 3; r.ND = r.W + 2;
+  r.NL = std::max(1, target / r.NS);
+  r.threads = std::min(1024, ((r.NL * r.NS + 31) / 32) * 32);
+  r.r1 = (size_t)std::max(7 * r.NQ + 5 * r.NS, 13 * r.ND) * r.NL;
+  r.r2 = (size_t)21 * r.NS * r.NL;
+  r.r3 = (size_t)12 * r.NF * r.NL;
+  r.smem = (r.r1 + r.r2 + r.r3) * sizeof(double) + (size_t)r.NS * r.NL * sizeof(int);
+  return r;
+}
+
+template <int DIR>
+__device__ __forceinline__ int rsx(int l, int j, int M, int NL) {
+  return DIR == 0 ? l * M + j : j * NL + l;
+}
+
+template <int DIR, bool POW2>
+__global__ void __launch_bounds__(128, 4)
+k_rdir(Geom g, const double* P, const double* lamL, double lscale, double dt, double* PA,
+       RShape sh) {
+  const int NL = sh.NL, W = sh.W, NQ = sh.NQ, NS = sh.NS, NF = sh.NF, ND = sh.ND;
+  extern __shared__ double sm[];
+  double* r1 = sm;
+  double* r2 = sm + sh.r1;
+  double* r3 = r2 + sh.r2;
+  int* sel_s = reinterpret_cast<int*>(r3 + sh.r3);
+  double* lm_s = r1 + 7 * NL * NQ;  // lives in r1 beside the primitives until P4
+  const long long n = g.ng;
+  const int zlo = g.threed ? g.az0 : 0, zhi = g.threed ? g.az1 : g.nz;
+  const int nxi = g.ax1 - g.ax0, nyi = g.ay1 - g.ay0, nzi = zhi - zlo;
+  const int lo = DIR == 0 ? g.ax0 : DIR == 1 ? g.ay0 : g.az0;
+  const int hi = DIR == 0 ? g.ax1 : DIR == 1 ? g.ay1 : g.az1;
+  const long long st = DIR == 0 ? 1 : DIR == 1 ? g.sy : g.sz;
+  const long long nlines = DIR == 0 ? (long long)nyi * nzi : DIR == 1 ? (long long)nxi * nzi
+                                                                       : (long long)nxi * nyi;
+  const int s0 = lo - 1 + (int)blockIdx.y * W;
+  const double ds = DIR == 0 ? g.dx : DIR == 1 ? g.dy : g.dz;
+  const double ids = DIR == 0 ? g.idx : DIR == 1 ? g.idy : g.idz;
+  const double area = DIR == 0 ? g.ayz : DIR == 1 ? g.axz : g.axy;
+  const double coef = -(dt / g.vol) * area;
+  const double rr = dt / ds;
+  auto line_base = [&](int l, bool& ok) -> long long {
+    const long long L = (long long)blockIdx.x * NL + l;
+    ok = L < nlines;
+    if (!ok) return 0;
+    if (DIR == 0) return (g.ay0 + L % nyi) * g.sy + (zlo + L / nyi) * g.sz;
+    if (DIR == 1) return (g.ax0 + L % nxi) + (zlo + L / nxi) * g.sz;
+    return (g.ax0 + L % nxi) + (g.ay0 + L / nxi) * g.sy;
+  };
+  auto valid = [&](int c) { return c >= lo - 1 && c <= hi; };
+  auto inner = [&](int c) { return c >= lo && c < hi; };
+
+  // P1: primitives
+  for (int t = threadIdx.x; t < NL * NQ; t += blockDim.x) {
+    const int l = DIR == 0 ? t / NQ : t % NL, j = DIR == 0 ? t % NQ : t / NL;
+    const int c = s0 - 3 + j;
+    bool ok;
+    const long long b = line_base(l, ok);
+    const int k = rsx<DIR>(l, j, NQ, NL);
+    const long long i = b + c * st;
+    if (ok && valid(c)) {
+      for (int q = 0; q < 7; ++q) r1[q * NL * NQ + k] = P[q * n + i];
+    } else {
+      for (int q = 0; q < 7; ++q) r1[q * NL * NQ + k] = 1.0;
+    }
+    // scaled adjoints of the interior cells of [s0-2, s0+W+2) (zero elsewhere)
+    if (j >= 1 && j <= NS) {
+      const int kl = rsx<DIR>(l, j - 1, NS, NL);
+      const bool in = ok && inner(c);
+      for (int q = 0; q < 5; ++q) lm_s[q * NL * NS + kl] = in ? lscale * lamL[q * n + i] : 0.0;
+    }
+  }
+  __syncthreads();
+  // P2: face states, slopes, selections
+  for (int t = threadIdx.x; t < NL * NS; t += blockDim.x) {
+    const int l = DIR == 0 ? t / NS : t % NL, j = DIR == 0 ? t % NS : t / NL;
+    const int c = s0 - 2 + j;
+    const int k = rsx<DIR>(l, j, NS, NL);
+    auto qv = [&](int jj) {
+      const int kk = rsx<DIR>(l, jj, NQ, NL);
+      return Prim{r1[kk], r1[NL * NQ + kk], r1[2 * NL * NQ + kk], r1[3 * NL * NQ + kk],
+                  r1[4 * NL * NQ + kk], r1[5 * NL * NQ + kk], r1[6 * NL * NQ + kk]};
+    };
+    const Prim qc = qv(j + 1);
+    FaceState mi, pl;
+    double sl[6] = {0, 0, 0, 0, 0, 0};
+    int sel = 0;
+    double hm = 0.0, hp = 0.0, flg = 0.0;
+    if (inner(c)) {
+      const Prim qm = qv(j), qp = qv(j + 2);
+      const double a0[6] = {qm.d, qm.u1, qm.u2, qm.u3, qm.p, qm.e};
+      const double a1[6] = {qc.d, qc.u1, qc.u2, qc.u3, qc.p, qc.e};
+      const double a2[6] = {qp.d, qp.u1, qp.u2, qp.u3, qp.p, qp.e};
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        sl[q] = slope3(a0[q], a1[q], a2[q]);
+        sel |= slope_sel(a0[q], a1[q], a2[q]) << (2 * q);
+      }
+      const double ud = DIR == 0 ? qc.u1 : DIR == 1 ? qc.u2 : qc.u3;
+      muscl_states<POW2>(qc, ud, sl[0], sl[1], sl[2], sl[3], sl[4], sl[5], dt, ds, ids, mi, pl);
+      double lp = fmax(ud + qc.c, 0.0) * dt, lm = fmin(ud - qc.c, 0.0) * dt;
+      if (POW2) { lp *= ids; lm *= ids; }
+      else { lp = cdiv(lp, ds, ids); lm = cdiv(lm, ds, ids); }
+      hm = kHalf * (-1.0 - lm);
+      hp = kHalf * (1.0 - lp);
+      flg = (ud + qc.c > 0.0 ? 1.0 : 0.0) + (ud - qc.c < 0.0 ? 2.0 : 0.0);
+    } else {
+      ghost_states(qc, mi, pl);
+    }
+    const int M = NL * NS;
+    const double mv[6] = {mi.d, mi.u1, mi.u2, mi.u3, mi.p, mi.e};
+    const double pv[6] = {pl.d, pl.u1, pl.u2, pl.u3, pl.p, pl.e};
+#pragma unroll
+    for (int q = 0; q < 6; ++q) {
+      r2[q * M + k] = mv[q];
+      r2[(6 + q) * M + k] = pv[q];
+      r2[(12 + q) * M + k] = sl[q];
+    }
+    r2[18 * M + k] = hm;
+    r2[19 * M + k] = hp;
+    r2[20 * M + k] = flg;
+    sel_s[k] = sel;
+  }
+  __syncthreads();
+  // P3: HLL derivative per face (high cell c = s0-1+j)
+  for (int t = threadIdx.x; t < NL * NF; t += blockDim.x) {
+    const int l = DIR == 0 ? t / NF : t % NL, j = DIR == 0 ? t % NF : t / NL;
+    const int c = s0 - 1 + j;
+    bool ok;
+    const long long b = line_base(l, ok);
+    const int k = rsx<DIR>(l, j, NF, NL);
+    const int M3 = NL * NF;
+    if (!(ok && c >= lo && c <= hi)) {
+      for (int q = 0; q < 12; ++q) r3[q * M3 + k] = 0.0;
+      continue;
+    }
+    const int M = NL * NS;
+    const int kl = rsx<DIR>(l, j, NS, NL), kr = rsx<DIR>(l, j + 1, NS, NL);
+    const FaceState L{r2[6 * M + kl], r2[7 * M + kl], r2[8 * M + kl], r2[9 * M + kl],
+                      r2[10 * M + kl], r2[11 * M + kl]};
+    const FaceState R{r2[kr], r2[M + kr], r2[2 * M + kr], r2[3 * M + kr], r2[4 * M + kr],
+                      r2[5 * M + kr]};
+    double gF[5];
+#pragma unroll
+    for (int q = 0; q < 5; ++q) gF[q] = coef * (lm_s[q * NL * NS + kl] - lm_s[q * NL * NS + kr]);
+    FS6 gL, gR;
+    hll_vjp<DIR>(L, R, g.gam, gF, gL, gR);
+    const double a[12] = {gL.d, gL.u1, gL.u2, gL.u3, gL.p, gL.e,
+                          gR.d, gR.u1, gR.u2, gR.u3, gR.p, gR.e};
+#pragma unroll
+    for (int q = 0; q < 12; ++q) r3[q * M3 + k] = a[q];
+  }
+  __syncthreads();
+  // P4: MUSCL adjoint per cell c = s0-1+j (into r1: DQ planes 0-6, LS planes 7-12)
+  for (int t = threadIdx.x; t < NL * ND; t += blockDim.x) {
+    const int l = DIR == 0 ? t / ND : t % NL, j = DIR == 0 ? t % ND : t / NL;
+    const int c = s0 - 1 + j;
+    const int k = rsx<DIR>(l, j, ND, NL);
+    const int M1 = NL * ND, M = NL * NS, M3 = NL * NF;
+    double lq[7] = {0, 0, 0, 0, 0, 0, 0}, ls[6] = {0, 0, 0, 0, 0, 0};
+    if (valid(c)) {
+      const int kf0 = rsx<DIR>(l, j, NF, NL), kf1 = rsx<DIR>(l, j + 1, NF, NL);
+      double gm[6], gp[6];
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        gm[q] = r3[(6 + q) * M3 + kf0];  // minus state of c: high side of face (c-1, c)
+        gp[q] = r3[q * M3 + kf1];        // plus state of c: low side of face (c, c+1)
+        lq[q] = gm[q] + gp[q];
+      }
+      if (inner(c)) {
+        const int ks = rsx<DIR>(l, j + 1, NS, NL);
+        const double hm = r2[18 * M + ks], hp = r2[19 * M + ks];
+        const int flg = (int)r2[20 * M + ks];
+        double ghm = 0.0, ghp = 0.0;
+#pragma unroll
+        for (int q = 0; q < 6; ++q) {
+          const double sq = r2[(12 + q) * M + ks];
+          ls[q] = hm * gm[q] + hp * gp[q];
+          ghm += sq * gm[q];
+          ghp += sq * gp[q];
+        }
+        const double glm = -kHalf * ghm, glp = -kHalf * ghp;
+        if (flg & 1) { lq[1 + DIR] += glp * rr; lq[6] += glp * rr; }
+        if (flg & 2) { lq[1 + DIR] += glm * rr; lq[6] -= glm * rr; }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < 7; ++q) r1[q * M1 + k] = lq[q];
+#pragma unroll
+    for (int q = 0; q < 6; ++q) r1[(7 + q) * M1 + k] = ls[q];
+  }
+  __syncthreads();
+  // P5: gather and accumulate
+  for (int t = threadIdx.x; t < NL * W; t += blockDim.x) {
+    const int l = DIR == 0 ? t / W : t % NL, j = DIR == 0 ? t % W : t / NL;
+    const int c = s0 + j;
+    bool ok;
+    const long long b = line_base(l, ok);
+    if (!(ok && valid(c))) continue;
+    const int M1 = NL * ND;
+    const int kc = rsx<DIR>(l, j + 1, ND, NL);
+    double acc[7];
+#pragma unroll
+    for (int q = 0; q < 7; ++q) acc[q] = r1[q * M1 + kc];
+#pragma unroll
+    for (int o = -1; o <= 1; ++o) {
+      if (!inner(c + o)) continue;
+      const int sel = sel_s[rsx<DIR>(l, j + 2 + o, NS, NL)];
+      const int kn = rsx<DIR>(l, j + 1 + o, ND, NL);
+#pragma unroll
+      for (int q = 0; q < 6; ++q) {
+        double k0, k1, k2;
+        slope_coef((sel >> (2 * q)) & 3, k0, k1, k2);
+        const double kk = o == 1 ? k0 : (o == 0 ? k1 : k2);
+        acc[q] += kk * r1[(7 + q) * M1 + kn];
+      }
+    }
+    const long long i = b + c * st;
+#pragma unroll
+    for (int q = 0; q < 7; ++q) PA[q * n + i] += acc[q];
   }
 }
 
-// R5: interior cell i collects its own adjoint and those of the face ghosts that
-// read it (with the momentum signs of the donor rule); accumulates into outA/outB.
-__global__ void k_r5_fold(Geom g, int stage, const double* GK, double* outA, double* outB) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i >= g.ng) return;
-  int x, y, z;
-  decode(g, i, x, y, z);
-  if (!ainterior(g, x, y, z)) return;
+// ---- per interior cell: conserved adjoints of its own primitives and of the
+// face ghosts it donates to (momentum signs of the donor rule), then the step
+// combination C2 = (C0' + C1 + L1(C1, C0'))/2, C1 = C0' + L0(C0'):
+//  stage 1 (lin = adjoint of C2): o1 <- adjoint of C1 = lin/2 + a_A,
+//           o2 <- adjoint of C0' so far = (lin/2 + a_B) + o1;
+//  stage 0 (lin = adjoint of C0' so far): o1 <- (lin + a_A) + a_B, then through
+//           the nsrc sources of X (source.f90:176-182); ghost entries of o1 zero.
+// conserved adjoints of the face ghosts next to interior cell (x,y,z) whose donor
+// it is, added to a (kept out of line: only boundary cells take it)
+template <int STAGE>
+__device__ __noinline__ void ghost_fold(const Geom& g, const double* SA, const double* SB,
+                                        const double* P, const double* PA, int x, int y, int z,
+                                        long long i, double a[10]) {
   const long long n = g.ng;
-  double a[10];
-  for (int q = 0; q < 10; ++q) a[q] = GK[q * n + i];
   const int ndir = g.threed ? 3 : 2;
   const int lo[3] = {g.ax0, g.ay0, g.az0}, hi[3] = {g.ax1, g.ay1, g.az1};
   const int c[3] = {x, y, z};
+  double gq[7], gA[5], gB[5];
   for (int dir = 0; dir < ndir; ++dir) {
-    const int wl = g.wall[2 * dir], wr = g.wall[2 * dir + 1];
     const long long st = dir == 0 ? 1 : dir == 1 ? g.sy : g.sz;
-    const int ghosts[4] = {lo[dir] - 2, lo[dir] - 1, hi[dir], hi[dir] + 1};
-    for (int k = 0; k < 4; ++k) {
-      bool flip = false;
-      const int dnr = amap(ghosts[k], lo[dir], hi[dir], wl, wr, flip);
-      if (dnr != c[dir]) continue;
-      const long long gi = i + (long long)(ghosts[k] - c[dir]) * st;
-      for (int q = 0; q < 10; ++q) {
-        const double v = GK[q * n + gi];
-        const bool neg = flip && ((q % 5) == 1 + dir);
-        a[q] += neg ? -v : v;
+    for (int side = 0; side < 2; ++side) {
+      // the face ghost next to this cell (lo-1 or hi), whose donor is this cell
+      if (c[dir] != (side == 0 ? lo[dir] : hi[dir] - 1)) continue;
+      const int gc = side == 0 ? lo[dir] - 1 : hi[dir];
+      const long long gi = i + (long long)(gc - c[dir]) * st;
+      const bool flip = g.wall[2 * dir + side] != 0;
+      for (int q = 0; q < 7; ++q) gq[q] = PA[q * n + gi];
+      int gx = x, gy = y, gz = z;
+      if (dir == 0) gx = gc; else if (dir == 1) gy = gc; else gz = gc;
+      cons_vjp(g, STAGE, P, gi, SA, SB, gx, gy, gz, gq, gA, gB);
+      for (int q = 0; q < 5; ++q) {
+        const bool neg = flip && q == 1 + dir;
+        a[q] += neg ? -gA[q] : gA[q];
+        a[5 + q] += neg ? -gB[q] : gB[q];
       }
     }
   }
-  for (int q = 0; q < 5; ++q) outA[q * n + i] += a[q];
-  if (stage == 1)
-    for (int q = 0; q < 5; ++q) outB[q * n + i] += a[5 + q];
-  else
-    for (int q = 0; q < 5; ++q) outA[q * n + i] += a[5 + q];
+}
+
+// grid over interior cells: x threads by (y, z) blocks.  Writes interior entries
+// only (the ghost entries of the adjoint planes stay zero).
+template <int STAGE>
+__global__ void k_rcell(Geom g, const double* SA, const double* SB, const double* P,
+                        const double* PA, const double* lin, double* o1, double* o2,
+                        const double* X, int nsrc) {
+  const int x = g.ax0 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int y = g.ay0 + blockIdx.y;
+  const int z = (g.threed ? g.az0 : 0) + blockIdx.z;
+  if (x >= g.ax1) return;
+  const long long i = x + (long long)y * g.sy + (long long)z * g.sz;
+  const long long n = g.ng;
+  double gq[7], a[10], gA[5], gB[5];
+  for (int q = 0; q < 7; ++q) gq[q] = PA[q * n + i];
+  cons_vjp(g, STAGE, P, i, SA, SB, x, y, z, gq, gA, gB);
+  for (int q = 0; q < 5; ++q) { a[q] = gA[q]; a[5 + q] = gB[q]; }
+  const bool edge = x == g.ax0 || x == g.ax1 - 1 || y == g.ay0 || y == g.ay1 - 1 ||
+                    (g.threed && (z == g.az0 || z == g.az1 - 1));
+  if (edge) ghost_fold<STAGE>(g, SA, SB, P, PA, x, y, z, i, a);
+  if constexpr (STAGE == 1) {
+    for (int q = 0; q < 5; ++q) {
+      const double h = kHalf * lin[q * n + i];
+      const double c1 = h + a[q];
+      o1[q * n + i] = c1;
+      o2[q * n + i] = (h + a[5 + q]) + c1;
+    }
+  } else {
+    double l[5];
+    for (int q = 0; q < 5; ++q) l[q] = (lin[q * n + i] + a[q]) + a[5 + q];
+    if (nsrc > 0) {
+      const double d = X[i], m[3] = {X[n + i], X[2 * n + i], X[3 * n + i]};
+      double Es[3];
+      Es[0] = X[4 * n + i];
+      for (int k = 0; k < nsrc; ++k)
+        Es[k + 1] = source_energy(d, m[0], m[1], m[2], Es[k], g.small_eps);
+      const double K = kin_mom(d, m[0], m[1], m[2]);
+      for (int k = nsrc - 1; k >= 0; --k) {
+        // E' = max(E - K, eps) + K
+        if (!(Es[k] - K > g.small_eps)) {
+          const double gE = l[4];
+          l[4] = 0.0;
+          for (int j = 0; j < 3; ++j) l[1 + j] += gE * m[j] / d;
+          l[0] += gE * (-K / d);
+        }
+      }
+    }
+    for (int q = 0; q < 5; ++q) o1[q * n + i] = l[q];
+  }
 }
 
 // C0' = src^nsrc(X) on interior cells (source.f90:176-182)
@@ -415,14 +553,6 @@ __global__ void k_adj_src_vjp(Geom g, const double* X, int nsrc, double* lam) {
   for (int q = 0; q < 5; ++q) lam[q * n + i] = l[q];
 }
 
-__global__ void k_axpy(long long n, double a, const double* x, double* y) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i < n) y[i] += a * x[i];
-}
-__global__ void k_scale_copy(long long n, double a, const double* x, double* y) {
-  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-  if (i < n) y[i] = a * x[i];
-}
 __global__ void k_set_clock(Ctrl* c, double dt, int active) {
   c->dt = dt;
   c->active = active;
@@ -432,6 +562,64 @@ __global__ void k_record_dt(const Ctrl* c, double* dts, long long k) { dts[k] = 
 }  // namespace
 
 // ------------------------------------------------------------------ host engine
+// Checkpoint schedule.  Reversing l steps from a held state with s free
+// snapshot slots costs C(l, s) recomputed steps; splitting at m (advance m steps,
+// store, reverse the last l-m with s-1 slots, then the first m with s):
+//   C(l, s) = min_m  m + C(l-m, s-1) + C(m, s),   C(l, 0) = l(l-1)/2,  C(1, s) = 0.
+// The snapshots of the first chain of splits are stored by the forward run
+// itself, so their advances cost nothing:
+//   F(l, s) = min_m  F(l-m, s-1) + C(m, s),   F(l, 0) = C(l, 0).
+// Solved by dynamic programming when l^2 s is small enough; otherwise the split
+// follows the binomial rule (largest right part reversible with r repetitions).
+struct Schedule {
+  long long L = 0;
+  int S = 0;
+  bool dp = false;
+  std::vector<long long> C, F;
+  std::vector<int> mc, mf;
+  size_t at(long long l, int s) const { return (size_t)l * (S + 1) + s; }
+};
+
+static void build_schedule(Schedule& sc, long long L, int S) {
+  sc.L = L;
+  sc.S = S;
+  sc.dp = (double)L * (double)L * (double)S <= 4e8;
+  if (!sc.dp) return;
+  const size_t N = (size_t)(L + 1) * (S + 1);
+  sc.C.assign(N, 0);
+  sc.F.assign(N, 0);
+  sc.mc.assign(N, 1);
+  sc.mf.assign(N, 1);
+  for (int s = 0; s <= S; ++s) {
+    for (long long l = 2; l <= L; ++l) {
+      const size_t k = sc.at(l, s);
+      if (s == 0) {
+        sc.C[k] = sc.F[k] = l * (l - 1) / 2;
+        continue;
+      }
+      if (s >= l - 1) {
+        sc.C[k] = l - 1;
+        sc.F[k] = 0;
+        sc.mc[k] = sc.mf[k] = 1;
+        continue;
+      }
+      long long bc = -1, bf = -1;
+      int mc = 1, mf = 1;
+      for (long long m = 1; m < l; ++m) {
+        const long long right_c = sc.C[sc.at(l - m, s - 1)], left = sc.C[sc.at(m, s)];
+        const long long vc = m + right_c + left;
+        const long long vf = sc.F[sc.at(l - m, s - 1)] + left;
+        if (bc < 0 || vc < bc) { bc = vc; mc = (int)m; }
+        if (bf < 0 || vf <= bf) { bf = vf; mf = (int)m; }
+      }
+      sc.C[k] = bc;
+      sc.F[k] = bf;
+      sc.mc[k] = mc;
+      sc.mf[k] = mf;
+    }
+  }
+}
+
 struct bx_adj {
   bx_handle* h = nullptr;  // geometry, tiles, control block, stream
   long long ng = 0;
@@ -442,12 +630,18 @@ struct bx_adj {
   std::vector<double> dts;    // frozen dt sequence
   double* d_dts = nullptr;
   std::vector<int> step_nsrc;
+  // checkpoint schedule: splits of the recursion, and the chain of snapshots
+  // the unfrozen forward stores on its way (pool slot 1 + j holds chain[j])
+  Schedule sched;
+  std::vector<long long> chain;
+  std::vector<int> chain_slot_of;  // per step index: pool slot holding it, or -1
+  bool chain_valid = false;
+  int chain_left = 0;
   // work planes
   double *W0 = nullptr, *W1 = nullptr, *W2 = nullptr;  // C0', C1, scratch state
   double* XT = nullptr;  // state after the last step of the forward run (C2_T)
-  double *lamA = nullptr, *lamB = nullptr, *lamT = nullptr, *lamC1 = nullptr;
-  double *P = nullptr, *G = nullptr, *LQ = nullptr, *LS = nullptr, *GK = nullptr;
-  uint8_t* SEL = nullptr;
+  double *lamA = nullptr, *lamB = nullptr, *lamC1 = nullptr;
+  double *P = nullptr, *PA = nullptr;  // primitives and their adjoints (7 planes each)
   double ms_fwd = 0.0, ms_bwd = 0.0;
   long long fwd_steps_in_bwd = 0;
   size_t bytes = 0;
@@ -502,22 +696,62 @@ static int fwd_step(bx_adj* A, const double* X, int nsrc, double dt, double* Y,
   return BX_OK;
 }
 
-// reverse of one stage: lamL = adjoint of the flux-operator output (interior cells);
-// accumulates into outA (and outB for stage 1)
+template <int DIR, bool POW2>
+static cudaError_t launch_rdir(const Geom& g, const double* P, const double* lamL, double lscale,
+                               double dt, double* PA, cudaStream_t s) {
+  const long long nzi = g.threed ? g.az1 - g.az0 : g.nz;
+  const long long nxi = g.ax1 - g.ax0, nyi = g.ay1 - g.ay0;
+  const long long nlines = DIR == 0 ? nyi * nzi : DIR == 1 ? nxi * nzi : nxi * nyi;
+  const int lo = DIR == 0 ? g.ax0 : DIR == 1 ? g.ay0 : g.az0;
+  const int hi = DIR == 0 ? g.ax1 : DIR == 1 ? g.ay1 : g.az1;
+  // x lines run along contiguous memory: long segments; y/z lines: 8 lines of
+  // adjacent x per block (coalesced), short segments
+  const RShape sh = DIR == 0 ? rshape(hi - lo + 2, 60, 128) : rshape(hi - lo + 2, 28, 128);
+  static size_t attr = 0;  // per instantiation; the attribute is per function
+  if (sh.smem > attr) {
+    cudaError_t e = cudaFuncSetAttribute(k_rdir<DIR, POW2>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sh.smem);
+    if (e != cudaSuccess) return e;
+    attr = sh.smem;
+  }
+  dim3 grid((unsigned)((nlines + sh.NL - 1) / sh.NL), (unsigned)sh.nseg);
+  k_rdir<DIR, POW2><<<grid, sh.threads, sh.smem, s>>>(g, P, lamL, lscale, dt, PA, sh);
+  return cudaGetLastError();
+}
+
+template <int DIR>
+static cudaError_t launch_rdir(const Geom& g, const double* P, const double* lamL, double lscale,
+                               double dt, double* PA, cudaStream_t s) {
+  return g.pow2 ? launch_rdir<DIR, true>(g, P, lamL, lscale, dt, PA, s)
+                : launch_rdir<DIR, false>(g, P, lamL, lscale, dt, PA, s);
+}
+
+// reverse of one stage: lamL*lscale = adjoint of the flux-operator output on
+// interior cells; k_rcell combines the result with the step's other terms
 static int rev_stage(bx_adj* A, int stage, const double* SA, const double* SB, const double* lamL,
-                     double dt, double* outA, double* outB) {
+                     double lscale, double dt, const double* lin, double* o1, double* o2,
+                     const double* X, int nsrc) {
   bx_handle* h = A->h;
   const Geom& g = h->g;
   cudaStream_t s = h->stream;
   const long long n = g.ng;
-  k_r1_prims<<<ablk(n), AB, 0, s>>>(g, stage, SA, SB, A->P);
-  ACK(cudaMemsetAsync(A->G, 0, 36 * n * sizeof(double), s));
-  k_r2_faces<0><<<ablk(n), AB, 0, s>>>(g, A->P, lamL, dt, A->G);
-  k_r2_faces<1><<<ablk(n), AB, 0, s>>>(g, A->P, lamL, dt, A->G);
-  if (g.threed) k_r2_faces<2><<<ablk(n), AB, 0, s>>>(g, A->P, lamL, dt, A->G);
-  k_r3_muscl<<<ablk(n), AB, 0, s>>>(g, A->P, A->G, dt, A->LQ, A->LS, A->SEL);
-  k_r4_cells<<<ablk(n), AB, 0, s>>>(g, stage, SA, SB, A->P, A->LQ, A->LS, A->SEL, A->GK);
-  k_r5_fold<<<ablk(n), AB, 0, s>>>(g, stage, A->GK, outA, outB);
+  // primitives of every cell: one block row per (y, z)
+  const int tp = std::min(512, ((g.nx + 31) / 32) * 32);
+  const dim3 pgrid((unsigned)((g.nx + tp - 1) / tp), (unsigned)g.ny, (unsigned)g.nz);
+  k_r1_prims<<<pgrid, tp, 0, s>>>(g, stage, SA, SB, A->P);
+  // interior cells
+  const int nxi = g.ax1 - g.ax0, tc = std::min(256, ((nxi + 31) / 32) * 32);
+  const dim3 cgrid((unsigned)((nxi + tc - 1) / tc), (unsigned)(g.ay1 - g.ay0),
+                   (unsigned)(g.threed ? g.az1 - g.az0 : g.nz));
+  ACK(cudaMemsetAsync(A->PA, 0, 7 * n * sizeof(double), s));
+  ACK(launch_rdir<0>(g, A->P, lamL, lscale, dt, A->PA, s));
+  ACK(launch_rdir<1>(g, A->P, lamL, lscale, dt, A->PA, s));
+  if (g.threed) ACK(launch_rdir<2>(g, A->P, lamL, lscale, dt, A->PA, s));
+  if (stage == 1)
+    k_rcell<1><<<cgrid, tc, 0, s>>>(g, SA, SB, A->P, A->PA, lin, o1, o2, X, nsrc);
+  else
+    k_rcell<0><<<cgrid, tc, 0, s>>>(g, SA, SB, A->P, A->PA, lin, o1, o2, X, nsrc);
   ACK(cudaGetLastError());
   return BX_OK;
 }
@@ -527,22 +761,15 @@ static int rev_step(bx_adj* A, const double* X, int nsrc, double dt, double* lam
   bx_handle* h = A->h;
   const Geom& g = h->g;
   cudaStream_t s = h->stream;
-  const long long n5 = 5 * g.ng;
   // recompute C0' and C1
   k_adj_src<<<ablk(g.ng), AB, 0, s>>>(g, X, nsrc, A->W0);
   if (int r = fwd_step(A, X, nsrc, dt, nullptr, true)) return r;  // W1 <- C1
-  // C2 = (C0' + C1 + L1)/2: half of lam to C0', C1 and the flux operator
-  k_scale_copy<<<ablk(n5), AB, 0, s>>>(n5, kHalf, lam, A->lamT);   // lamT: lam/2 (L1 input)
-  k_scale_copy<<<ablk(n5), AB, 0, s>>>(n5, kHalf, lam, A->lamC1);  // adjoint of C1
-  k_scale_copy<<<ablk(n5), AB, 0, s>>>(n5, kHalf, lam, A->lamA);   // adjoint of C0'
-  if (int r = rev_stage(A, 1, A->W1, A->W0, A->lamT, dt, A->lamC1, A->lamA)) return r;
-  // C1 = C0' + L0(C0')
-  k_axpy<<<ablk(n5), AB, 0, s>>>(n5, 1.0, A->lamC1, A->lamA);
-  if (int r = rev_stage(A, 0, A->W0, A->W0, A->lamC1, dt, A->lamA, A->lamA)) return r;
-  // through the sources: adjoint of X
-  ACK(cudaMemcpyAsync(lam, A->lamA, n5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
-  k_adj_src_vjp<<<ablk(g.ng), AB, 0, s>>>(g, X, nsrc, lam);
-  ACK(cudaGetLastError());
+  // stage 1 reads lam/2; writes lamC1 (adjoint of C1) and lamA (of C0')
+  if (int r = rev_stage(A, 1, A->W1, A->W0, lam, kHalf, dt, lam, A->lamC1, A->lamA, X, nsrc))
+    return r;
+  // stage 0 reads lamC1; lam <- adjoint of X through the sources
+  if (int r = rev_stage(A, 0, A->W0, A->W0, A->lamC1, 1.0, dt, A->lamA, lam, nullptr, X, nsrc))
+    return r;
   return BX_OK;
 }
 
@@ -567,6 +794,17 @@ static long long binom(long long n, long long k) {
   return r;
 }
 
+static long long binom(long long n, long long k);
+
+static long long split_of(const Schedule& sc, bool chain, long long l, int s) {
+  if (sc.dp && l <= sc.L && s <= sc.S) return chain ? sc.mf[sc.at(l, s)] : sc.mc[sc.at(l, s)];
+  long long r = 1;
+  while (binom(s + r, s) < l) ++r;
+  long long l2 = std::min(binom(s - 1 + r, s - 1), l - 1);
+  if (l2 < 1) l2 = 1;
+  return l - l2;
+}
+
 // state of step `to` from the state of step `from` (held in src) into dst,
 // ping-ponging between dst and W2 so the last step lands in dst
 static int advance(bx_adj* A, const double* src, long long from, long long to, double* dst) {
@@ -586,12 +824,14 @@ static int advance(bx_adj* A, const double* src, long long from, long long to, d
   return BX_OK;
 }
 
-// reverse steps [a, b) with the state of step a in Xa (owned by the caller)
-static int reverse_range(bx_adj* A, const double* Xa, long long a, long long b, double* lam) {
+// reverse steps [a, b) with the state of step a in Xa (owned by the caller);
+// chain: the split snapshots come from the forward run (no advance)
+static int reverse_range(bx_adj* A, const double* Xa, long long a, long long b, double* lam,
+                         bool chain) {
   const long long l = b - a;
   if (l <= 0) return BX_OK;
   if (l == 1) return rev_step(A, Xa, A->step_nsrc[a], A->dts[a], lam);
-  const int s = (int)A->pool_free.size();
+  const int s = (int)A->pool_free.size() + (chain ? A->chain_left : 0);
   if (s == 0) {
     // no snapshot left: rebuild each state from Xa (into lamB, free during reversal)
     for (long long k = b - 1; k >= a; --k) {
@@ -600,16 +840,20 @@ static int reverse_range(bx_adj* A, const double* Xa, long long a, long long b, 
     }
     return BX_OK;
   }
-  long long r = 1;
-  while (binom(s + r, s) < l) ++r;
-  long long l2 = std::min(binom(s - 1 + r, s - 1), l - 1);
-  if (l2 < 1) l2 = 1;
-  const long long m = b - l2;
-  double* slot = take_slot(A);
-  if (int rc = advance(A, Xa, a, m, slot)) return rc;
-  if (int rc = reverse_range(A, slot, m, b, lam)) return rc;
+  const long long m = a + split_of(A->sched, chain, l, s);
+  double* slot;
+  if (chain) {
+    const int k = A->chain_slot_of[m];
+    if (k < 0) return aerr(A, BX_ERR_STATE, "checkpoint chain does not match the schedule");
+    slot = A->pool[k];
+    A->chain_left -= 1;
+  } else {
+    slot = take_slot(A);
+    if (int rc = advance(A, Xa, a, m, slot)) return rc;
+  }
+  if (int rc = reverse_range(A, slot, m, b, lam, chain)) return rc;
   give_slot(A, slot);
-  return reverse_range(A, Xa, a, m, lam);
+  return reverse_range(A, Xa, a, m, lam, false);
 }
 
 extern "C" {
@@ -620,10 +864,9 @@ int bx_adj_destroy(bx_adj* A) {
   if (!A) return BX_OK;
   if (A->h && A->h->stream) cudaStreamSynchronize(A->h->stream);
   for (double* p : A->pool) cudaFree(p);
-  double* ps[] = {A->W0, A->W1, A->W2, A->XT, A->lamA, A->lamB, A->lamT, A->lamC1,
-                  A->P,  A->G,  A->LQ, A->LS,   A->GK,   A->d_dts};
+  double* ps[] = {A->W0, A->W1, A->W2, A->XT, A->lamA, A->lamB, A->lamC1,
+                  A->P,  A->PA, A->d_dts};
   for (double* p : ps) cudaFree(p);
-  cudaFree(A->SEL);
   if (A->h) bx_destroy(A->h);
   delete A;
   return BX_OK;
@@ -660,20 +903,26 @@ int bx_adj_create(const bx_params* params, int64_t nsteps, int32_t snapshots, bx
   A->pool.assign(A->snaps + 1, nullptr);
   for (int k = 0; k <= A->snaps; ++k)
     if ((rc = amalloc(A, &A->pool[k], 5 * n))) return fail(rc);
-  double** planes5[] = {&A->W0, &A->W1, &A->W2, &A->XT, &A->lamA, &A->lamB, &A->lamT, &A->lamC1};
+  double** planes5[] = {&A->W0, &A->W1, &A->W2, &A->XT, &A->lamA, &A->lamB, &A->lamC1};
   for (double** p : planes5)
     if ((rc = amalloc(A, p, 5 * n))) return fail(rc);
   if ((rc = amalloc(A, &A->P, 7 * n))) return fail(rc);
-  if ((rc = amalloc(A, &A->G, 36 * n))) return fail(rc);
-  if ((rc = amalloc(A, &A->LQ, 7 * n))) return fail(rc);
-  if ((rc = amalloc(A, &A->LS, 18 * n))) return fail(rc);
-  if ((rc = amalloc(A, &A->GK, 10 * n))) return fail(rc);
+  if ((rc = amalloc(A, &A->PA, 7 * n))) return fail(rc);
   if ((rc = amalloc(A, &A->d_dts, nsteps))) return fail(rc);
-  if (cudaMalloc(&A->SEL, 18 * n) != cudaSuccess) {
-    A->err = "SEL allocation";
-    return fail(BX_ERR_NOMEM);
+  build_schedule(A->sched, nsteps, A->snaps);
+  A->chain_slot_of.assign(nsteps + 1, -1);
+  {
+    long long a = 0, l = nsteps;
+    int sl = A->snaps;
+    while (l > 1 && sl > 0) {
+      const long long m = split_of(A->sched, true, l, sl);
+      a += m;
+      l -= m;
+      A->chain_slot_of[a] = 1 + (int)A->chain.size();
+      A->chain.push_back(a);
+      --sl;
+    }
   }
-  A->bytes += 18 * n;
   *out = A;
   return BX_OK;
 }
@@ -698,7 +947,9 @@ int bx_adj_forward(bx_adj* A, const double* cons0, double* consT, int32_t frozen
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
   ACK(cudaEventRecord(e0, s));
-  double* X0 = A->pool[0];
+  // the unfrozen run keeps its initial state and the chain snapshots for the
+  // backward pass; frozen runs start from lamB and store nothing
+  double* X0 = frozen ? A->lamB : A->pool[0];
   ACK(cudaMemcpyAsync(X0, cons0, n5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
   // initial Courant rate and clock
   Ctrl c{};
@@ -712,6 +963,7 @@ int bx_adj_forward(bx_adj* A, const double* cons0, double* consT, int32_t frozen
   int nsrc = 1;
   for (long long k = 0; k < A->nsteps; ++k) {
     double* out = bufs[k & 1];
+    if (!frozen && A->chain_slot_of[k + 1] >= 0) out = A->pool[A->chain_slot_of[k + 1]];
     StageArgs a{};
     a.ctrl = h->d_ctrl;
     a.geom = h->d_geom;
@@ -757,7 +1009,10 @@ int bx_adj_forward(bx_adj* A, const double* cons0, double* consT, int32_t frozen
   ACK(fused_to_phase(g, cur, 2, pa, h->nghost, h->d_dst, h->d_src2, h->d_sgn2, s));
   ACK(cudaMemcpyAsync(consT, h->pa.cons, n5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
   ACK(cudaStreamSynchronize(s));
-  if (!frozen) A->have_forward = true;
+  if (!frozen) {
+    A->have_forward = true;
+    A->chain_valid = true;
+  }
   return BX_OK;
 }
 
@@ -777,12 +1032,18 @@ int bx_adj_backward(bx_adj* A, const double* lamT, double* lam0) {
   ACK(cudaEventRecord(e0, s));
   A->fwd_steps_in_bwd = 0;
   A->pool_free.clear();
-  for (int k = 1; k <= A->snaps; ++k) A->pool_free.push_back(k);
+  const bool chain = A->chain_valid;
+  for (int k = A->snaps; k >= 1; --k)
+    if (!chain || k > (int)A->chain.size()) A->pool_free.push_back(k);
+  A->chain_left = chain ? (int)A->chain.size() : 0;
   double* lam = lam0;
   ACK(cudaMemcpyAsync(lam, lamT, n5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
   // the reference cons after the run is src(C2_T): its adjoint first
   k_adj_src_vjp<<<ablk(g.ng), AB, 0, s>>>(g, A->XT, 1, lam);
-  if (int r = reverse_range(A, A->pool[0], 0, A->nsteps, lam)) return r;
+  // the chain snapshots are overwritten while reversing: a later backward
+  // without a new forward rebuilds them
+  A->chain_valid = false;
+  if (int r = reverse_range(A, A->pool[0], 0, A->nsteps, lam, chain)) return r;
   ACK(cudaEventRecord(e1, s));
   ACK(cudaEventSynchronize(e1));
   float ms = 0.f;

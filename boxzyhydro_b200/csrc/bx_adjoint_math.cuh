@@ -45,24 +45,26 @@ __device__ __forceinline__ void hll_vjp(const FaceState& L, const FaceState& R, 
   const double t2 = fmax(0.0, b1);
   const double am = fmax(t2, b2);
   const int sam = (b2 > t2) ? 2 : (b1 > 0.0 ? 1 : 0);
-  const double D = ap + am;
-  double F[5], gN[5], gD = 0.0, gap = 0.0, gam_ = 0.0;
+  const double iD = 1.0 / (ap + am);
+  const double apm = ap * am;
+  double gN[5], gD = 0.0, gap = 0.0, gam_ = 0.0;
   for (int k = 0; k < 5; ++k) {
-    F[k] = (ap * fl[k] + am * fr[k] - ap * am * (sr[k] - sl[k])) / D;
-    gN[k] = gF[k] / D;
-    gD -= gN[k] * F[k];
+    const double ds = sr[k] - sl[k];
+    const double F = fma(ap, fl[k], fma(am, fr[k], -apm * ds)) * iD;
+    gN[k] = gF[k] * iD;
+    gD = fma(-gN[k], F, gD);
   }
   gap = gD;
   gam_ = gD;
   double gfl[5], gfr[5], gsl[5], gsr[5];
   for (int k = 0; k < 5; ++k) {
     const double ds = sr[k] - sl[k];
-    gap += gN[k] * (fl[k] - am * ds);
-    gam_ += gN[k] * (fr[k] - ap * ds);
+    gap = fma(gN[k], fma(-am, ds, fl[k]), gap);
+    gam_ = fma(gN[k], fma(-ap, ds, fr[k]), gam_);
     gfl[k] = gN[k] * ap;
     gfr[k] = gN[k] * am;
-    gsr[k] = -gN[k] * ap * am;
-    gsl[k] = gN[k] * ap * am;
+    gsl[k] = gN[k] * apm;
+    gsr[k] = -gsl[k];
   }
   double gvl = 0, gvr = 0, gcl = 0, gcr = 0;
   if (sap == 1) { gvr += gap; gcr += gap; }
@@ -71,31 +73,31 @@ __device__ __forceinline__ void hll_vjp(const FaceState& L, const FaceState& R, 
   else if (sam == 2) { gcl += gam_; gvl -= gam_; }
   double gpl = 0, gpr = 0, gdl = 0, gdr = 0, gel = 0, ger = 0;
   double gul[3] = {0, 0, 0}, gur[3] = {0, 0, 0};
-  // sound speeds
-  if (cl > 0.0) { gpl += gcl * cl / (2.0 * pl); gdl -= gcl * cl / (2.0 * dl); }
-  if (cr > 0.0) { gpr += gcr * cr / (2.0 * pr); gdr -= gcr * cr / (2.0 * dr); }
-  // fluxes
-  gdl += gfl[0] * vl; gsl[0] += 0.0; gvl += gfl[0] * sl[0];
-  gdr += gfr[0] * vr; gvr += gfr[0] * sr[0];
+  // c = sqrt(gam p / d): dc/dp = c/(2p), dc/dd = -c/(2d)
+  if (cl > 0.0) { const double h = kHalf * gcl * cl; gpl += h / pl; gdl -= h / dl; }
+  if (cr > 0.0) { const double h = kHalf * gcr * cr; gpr += h / pr; gdr -= h / dr; }
+  // fluxes: f0 = d v, f(1+j) = [j == DIR] p + s(1+j) v, f4 = (s4 + p) v
+  gdl = fma(gfl[0], vl, gdl); gvl = fma(gfl[0], sl[0], gvl);
+  gdr = fma(gfr[0], vr, gdr); gvr = fma(gfr[0], sr[0], gvr);
   for (int j = 0; j < 3; ++j) {
     if (j == DIR) { gpl += gfl[1 + j]; gpr += gfr[1 + j]; }
-    gsl[1 + j] += gfl[1 + j] * vl; gvl += gfl[1 + j] * sl[1 + j];
-    gsr[1 + j] += gfr[1 + j] * vr; gvr += gfr[1 + j] * sr[1 + j];
+    gsl[1 + j] = fma(gfl[1 + j], vl, gsl[1 + j]); gvl = fma(gfl[1 + j], sl[1 + j], gvl);
+    gsr[1 + j] = fma(gfr[1 + j], vr, gsr[1 + j]); gvr = fma(gfr[1 + j], sr[1 + j], gvr);
   }
-  gsl[4] += gfl[4] * vl; gpl += gfl[4] * vl; gvl += gfl[4] * (sl[4] + pl);
-  gsr[4] += gfr[4] * vr; gpr += gfr[4] * vr; gvr += gfr[4] * (sr[4] + pr);
-  // fl[0] = sl[0]*vl with sl[0] = dl was taken as dl*vl above (gfl0 -> gdl)
-  // conserved face variables
+  gsl[4] = fma(gfl[4], vl, gsl[4]); gpl = fma(gfl[4], vl, gpl); gvl = fma(gfl[4], sl[4] + pl, gvl);
+  gsr[4] = fma(gfr[4], vr, gsr[4]); gpr = fma(gfr[4], vr, gpr); gvr = fma(gfr[4], sr[4] + pr, gvr);
+  // conserved face variables s0 = d, s(1+j) = d u_j, s4 = e + d K/2
   gdl += gsl[0]; gdr += gsr[0];
   for (int j = 0; j < 3; ++j) {
-    gdl += gsl[1 + j] * ul[j]; gul[j] += gsl[1 + j] * dl;
-    gdr += gsr[1 + j] * ur[j]; gur[j] += gsr[1 + j] * dr;
+    gdl = fma(gsl[1 + j], ul[j], gdl); gul[j] = fma(gsl[1 + j], dl, gul[j]);
+    gdr = fma(gsr[1 + j], ur[j], gdr); gur[j] = fma(gsr[1 + j], dr, gur[j]);
   }
-  gel += gsl[4]; gdl += gsl[4] * kHalf * Kl;
-  ger += gsr[4]; gdr += gsr[4] * kHalf * Kr;
+  gel += gsl[4]; gdl = fma(gsl[4], kHalf * Kl, gdl);
+  ger += gsr[4]; gdr = fma(gsr[4], kHalf * Kr, gdr);
+  const double hdl = gsl[4] * dl, hdr = gsr[4] * dr;
   for (int j = 0; j < 3; ++j) {
-    gul[j] += gsl[4] * dl * ul[j];
-    gur[j] += gsr[4] * dr * ur[j];
+    gul[j] = fma(hdl, ul[j], gul[j]);
+    gur[j] = fma(hdr, ur[j], gur[j]);
   }
   gul[DIR] += gvl;
   gur[DIR] += gvr;

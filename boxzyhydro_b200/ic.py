@@ -179,6 +179,26 @@ def turbulent_box(n: int = 256, seed: int = 1234, sigma_ln: float = 0.5, mach: f
     return _assemble(hp, rho, v, p)
 
 
+def sod_blob_box(n: int = 128, seed: int = 4, amp: float = 0.05, width: float = 0.08,
+                 gamma: float = 1.6666666666666667, cfl: float = 0.4, blob: bool = True) -> State:
+    """Sod state split on x at the box centre ((rho,p) = (1,1) | (0.125,0.1), v=0) in
+    an n^3-interior box with outflow walls, times a seeded Gaussian density blob
+    rho *= 1 + amp*exp(-|r-r0|^2/(2 width^2)) with r0 uniform in [0.3,0.7]^3 of the
+    unit box (pressure unchanged).  blob=False gives the unperturbed state."""
+    hp = turbulent_params(n, gamma, cfl)
+    rng = np.random.default_rng(seed)
+    r0 = rng.uniform(0.3, 0.7, 3)
+    c = (np.arange(n) + 0.5) / n
+    zz, yy, xx = np.meshgrid(c, c, c, indexing="ij")
+    rho = np.where(xx < 0.5, 1.0, 0.125)
+    p = np.where(xx < 0.5, 1.0, 0.1)
+    if blob:
+        r2 = (xx - r0[0]) ** 2 + (yy - r0[1]) ** 2 + (zz - r0[2]) ** 2
+        rho = rho * (1.0 + amp * np.exp(-r2 / (2.0 * width * width)))
+    v = [np.zeros((n, n, n)) for _ in range(3)]
+    return _assemble(hp, rho, v, p)
+
+
 def riemann_params(side: int, gamma: float, cfl: float = 0.1) -> HydroParams:
     d = 1.0 / side
     return HydroParams(nx=side + 4, ny=side + 4, nz=side + 4, dx=d, dy=d, dz=d, cfl=cfl,
