@@ -282,12 +282,14 @@ def batched_arm(args, rank, world, local):
 
 
 def adjoint_arm(args, rank, world, local):
-    """C4/C5: discrete adjoint of an n^3 run of `steps` steps.  Loss
-    0.5*||rho(T) - rho_target||^2 over interior cells, rho_target from the run of
-    the unperturbed state; gradient w.r.t. the initial rho, m, E.  Reports the
-    adjoint/forward device-time ratio, device memory, recomputed steps and the
-    agreement with central finite differences (dt sequence held fixed) along
-    seeded random directions."""
+    """Discrete adjoint of an n^3 run of `steps` steps.  Loss
+    0.5*||rho(T) - rho_target||^2 over interior cells; rho_target is the run of
+    the unperturbed state (x-split state) or 1.01*rho(T) (turbulent state).
+    Gradient w.r.t. the initial rho, m, E.  Reports the adjoint/forward
+    device-time ratio, the engine's device bytes and the peak device memory in
+    use (cudaMemGetInfo), the recomputed steps and the agreement with central
+    finite differences (dt sequence held fixed) along seeded random
+    directions.  --snapshots 0 sizes the snapshot pool to the free HBM."""
     import numpy as np
     import torch
 
@@ -296,77 +298,108 @@ def adjoint_arm(args, rank, world, local):
     from boxzyhydro_b200.adjoint import AdjointEngine
 
     torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
     n = args.n
     if args.adj_ic == "blob":
         st = ic.sod_blob_box(n=n, seed=args.seed)
-        st0 = ic.sod_blob_box(n=n, seed=args.seed, blob=False)
         ic_name = "x-split Sod state + seeded 5% Gaussian density blob, outflow walls"
     else:
         st = ic.turbulent_box(n=n, seed=args.seed)
-        st0 = None
         ic_name = "lognormal/solenoidal turbulent state, outflow walls"
     hp = st.params
-    dev = torch.device("cuda", local)
+    ng = hp.ngrid
+    plane = ng * 8
     m = torch.tensor(G.boundary_flags(hp.nx, hp.ny, hp.nz) == 0, device=dev)
-    eng = AdjointEngine(hp, args.steps, args.snapshots)
+    c0 = torch.tensor(np.ascontiguousarray(st.cons.T), device=dev)
+    del st
+    snaps = args.snapshots
+    if snaps <= 0:
+        # engine: 7 state sets + 14 scratch planes + (snaps + 1) state sets;
+        # this arm, beside c0: gradient, direction, perturbed state, output and
+        # one density plane (21 planes)
+        free = torch.cuda.mem_get_info(dev)[0]
+        fixed = (7 * 5 + 14 + 5 + 21) * plane + (6 << 30)
+        snaps = int(max(1, min(args.steps, (free - fixed) // (5 * plane))))
+    peak = [0]
+
+    def used():
+        f, t = torch.cuda.mem_get_info(dev)
+        peak[0] = max(peak[0], t - f)
+
+    eng = AdjointEngine(hp, args.steps, snaps)
     stream = torch.cuda.Stream()
     eng.set_stream(stream.cuda_stream)
+    used()
 
     def run(c, frozen):
         out = torch.empty_like(c)
         torch.cuda.synchronize()
         eng.forward_ptr(c.data_ptr(), out.data_ptr(), frozen=frozen)
+        torch.cuda.synchronize()
+        used()
         return out
 
-    c0 = torch.tensor(np.ascontiguousarray(st.cons.T), device=dev)
-    del st
-    if st0 is not None:
-        target = run(torch.tensor(np.ascontiguousarray(st0.cons.T), device=dev), False)[0].clone()
+    if args.adj_ic == "blob":
+        st0 = ic.sod_blob_box(n=n, seed=args.seed, blob=False)
+        t0 = torch.tensor(np.ascontiguousarray(st0.cons.T), device=dev)
         del st0
-    else:
-        target = None
+        out = run(t0, False)
+        target = out[0].clone()
+        del out, t0
     cT = run(c0, False)
-    if target is None:
-        target = cT[0] * 1.01
-    lamT = torch.zeros_like(cT)
-    lamT[0] = (cT[0] - target) * m
-    loss = 0.5 * float(torch.sum(lamT[0] ** 2))
     stats_fwd = eng.stats()
-    grad = torch.empty_like(cT)
+    if args.adj_ic != "blob":
+        target = cT[0] * 1.01
+    lamT = cT
+    lamT[0] = (cT[0] - target) * m
+    lamT[1:] = 0.0
+    del cT
+    loss = 0.5 * float(torch.sum(lamT[0] ** 2))
+    grad = torch.empty_like(lamT)
     torch.cuda.synchronize()
     eng.backward_ptr(lamT.data_ptr(), grad.data_ptr())
     torch.cuda.synchronize()
+    used()
     stt = eng.stats()
+    del lamT
     ratio = stt["ms_backward"] / stats_fwd["ms_forward"]
     # finite differences with the frozen dt sequence
     gen = torch.Generator(device=dev)
     gen.manual_seed(args.seed + 99)
     scale = torch.tensor([1.0, 0.3, 0.3, 0.3, 2.0], device=dev, dtype=torch.float64)[:, None]
     rel = []
+    h = 1e-7
     for k in range(args.fd_dirs):
-        v = torch.randn(cT.shape, generator=gen, device=dev, dtype=torch.float64) * scale * m
-        h = 1e-7
-        lp = run(c0 + h * v, True)[0]
-        lm = run(c0 - h * v, True)[0]
-        fd = float(torch.sum(((lp - target) ** 2 - (lm - target) ** 2) * m)) * 0.5 / (2 * h)
+        v = torch.randn(c0.shape, generator=gen, device=dev, dtype=torch.float64)
+        v.mul_(scale).mul_(m)
         adj = float(torch.sum(grad * v))
+        vals = []
+        for sgn in (1.0, -1.0):
+            x = torch.add(c0, v, alpha=sgn * h)
+            out = run(x, True)
+            del x
+            vals.append(float(torch.sum((out[0] - target) ** 2 * m)))
+            del out
+        fd = (vals[0] - vals[1]) * 0.5 / (2 * h)
         rel.append(abs(fd - adj) / max(abs(adj), 1e-300))
+        del v
     line = {
         "metric": "adjoint/forward time ratio", "value": ratio, "unit": "x",
         "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": 0,
         "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"discrete adjoint, {n}^3 interior, gamma=5/3, {ic_name}, "
                                f"{args.steps} steps, loss 0.5||rho(T)-rho_target||^2",
-                   "snapshots": args.snapshots},
+                   "snapshots": snaps},
         "ms_forward": stats_fwd["ms_forward"], "ms_backward": stt["ms_backward"],
         "forward_cell_updates_per_s": hp.n_active() * args.steps / (stats_fwd["ms_forward"] * 1e-3),
         "recomputed_steps": stt["recomputed_steps"],
         "recompute_fraction": stt["recomputed_steps"] / args.steps,
-        "device_bytes": stt["device_bytes"],
-        "peak_device_bytes_torch": torch.cuda.max_memory_allocated(dev),
+        "engine_device_bytes": stt["device_bytes"],
+        "peak_device_bytes_in_use": peak[0],
         "loss": loss,
-        "fd_check": {"directions": args.fd_dirs, "h": 1e-7, "max_rel_diff": max(rel) if rel else None,
-                     "median_rel_diff": float(np.median(rel)) if rel else None},
+        "fd_check": {"directions": args.fd_dirs, "h": h, "max_rel_diff": max(rel) if rel else None,
+                     "median_rel_diff": float(np.median(rel)) if rel else None,
+                     "per_direction": rel},
     }
     eng.close()
     if rank == 0:

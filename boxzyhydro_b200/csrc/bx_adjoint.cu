@@ -876,7 +876,7 @@ int bx_adj_create(const bx_params* params, int64_t nsteps, int32_t snapshots, bx
   if (!params || !out || nsteps <= 0 || snapshots < 1)
     return aerr(nullptr, BX_ERR_ARG, "bad arguments");
   bx_adj* A = new bx_adj();
-  if (int r = bx_create(params, &A->h)) {
+  if (int r = bx_create_lean(params, &A->h)) {
     g_adj_err = bx_last_error(nullptr);
     delete A;
     return r;
@@ -1005,9 +1005,7 @@ int bx_adj_forward(bx_adj* A, const double* cons0, double* consT, int32_t frozen
                 "values); the adjoint of this run is not defined by the fused stages");
   ACK(cudaMemcpyAsync(A->XT, cur, n5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
   // reference cons after the run: one source more, ghosts filled
-  PhaseArrays pa = h->pa;
-  ACK(fused_to_phase(g, cur, 2, pa, h->nghost, h->d_dst, h->d_src2, h->d_sgn2, s));
-  ACK(cudaMemcpyAsync(consT, h->pa.cons, n5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  ACK(fused_to_cons(g, cur, 2, consT, h->nghost, h->d_dst, h->d_src2, h->d_sgn2, s));
   ACK(cudaStreamSynchronize(s));
   if (!frozen) {
     A->have_forward = true;

@@ -81,6 +81,8 @@ static std::vector<Tile> make_tiles(const Geom& g, int box, int slots) {
   return tiles;
 }
 
+static int create_handle(const bx_params* params, bx_handle** out, bool lean);
+
 extern "C" {
 
 const char* bx_version(void) { return "boxzy-b200 1.0 (sm_100a, FP64)"; }
@@ -91,6 +93,18 @@ const char* bx_last_error(bx_handle* h) {
 }
 
 int bx_create(const bx_params* params, bx_handle** out) {
+  return create_handle(params, out, false);
+}
+
+}  // extern "C"
+
+int bx_create_lean(const bx_params* params, bx_handle** out) {
+  return create_handle(params, out, true);
+}
+
+// lean: geometry, ghost tables, tiles, control block and stream only (no state
+// planes); for engines that keep their own planes and call the stage kernels
+static int create_handle(const bx_params* params, bx_handle** out, bool lean) {
   if (!params || !out) return set_err(nullptr, BX_ERR_ARG, "null argument");
   const bx_params& P = *params;
   if (P.h2stat != -1)
@@ -130,16 +144,18 @@ int bx_create(const bx_params* params, bx_handle** out) {
   } while (0)
   CKC(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
   h->own_stream = true;
-  for (int k = 0; k < 3; ++k) CKC(dalloc((void**)&h->buf[k], 5 * ng * sizeof(double)));
-  CKC(dalloc((void**)&h->pa.cons, 5 * ng * sizeof(double)));
-  CKC(dalloc((void**)&h->pa.cons_old, 5 * ng * sizeof(double)));
-  CKC(dalloc((void**)&h->pa.u, 3 * ng * sizeof(double)));
-  CKC(dalloc((void**)&h->pa.p, ng * sizeof(double)));
-  CKC(dalloc((void**)&h->pa.adindx, ng * sizeof(double)));
-  CKC(dalloc((void**)&h->pa.gtmp, 5 * (size_t)h->nghost * sizeof(double)));
-  CKC(cudaMemset(h->pa.cons, 0, 5 * ng * sizeof(double)));
-  CKC(cudaMemset(h->pa.u, 0, 3 * ng * sizeof(double)));
-  CKC(cudaMemset(h->pa.p, 0, ng * sizeof(double)));
+  if (!lean) {
+    for (int k = 0; k < 3; ++k) CKC(dalloc((void**)&h->buf[k], 5 * ng * sizeof(double)));
+    CKC(dalloc((void**)&h->pa.cons, 5 * ng * sizeof(double)));
+    CKC(dalloc((void**)&h->pa.cons_old, 5 * ng * sizeof(double)));
+    CKC(dalloc((void**)&h->pa.u, 3 * ng * sizeof(double)));
+    CKC(dalloc((void**)&h->pa.p, ng * sizeof(double)));
+    CKC(dalloc((void**)&h->pa.adindx, ng * sizeof(double)));
+    CKC(dalloc((void**)&h->pa.gtmp, 5 * (size_t)h->nghost * sizeof(double)));
+    CKC(cudaMemset(h->pa.cons, 0, 5 * ng * sizeof(double)));
+    CKC(cudaMemset(h->pa.u, 0, 3 * ng * sizeof(double)));
+    CKC(cudaMemset(h->pa.p, 0, ng * sizeof(double)));
+  }
   const int n = h->nghost;
   CKC(dalloc((void**)&h->d_dst, n * sizeof(int32_t)));
   CKC(dalloc((void**)&h->d_src1, n * sizeof(int32_t)));
@@ -174,6 +190,8 @@ int bx_create(const bx_params* params, bx_handle** out) {
   *out = h;
   return BX_OK;
 }
+
+extern "C" {
 
 int bx_destroy(bx_handle* h) {
   if (!h) return BX_OK;

@@ -43,5 +43,8 @@ struct bx_handle {
 // planes of one grid (plane stride `ps`), `nsrc` sources short of the
 // reference state, with the given clock.  The batched path uses it to continue
 // a box on a handle of its own.
+// a handle with geometry, ghost tables, tiles, control block and stream but no
+// state planes (for engines that hold their own planes)
+int bx_create_lean(const bx_params* params, bx_handle** out);
 int bx_handle_adopt_fused(bx_handle* h, const double* planes, long long ps, int nsrc,
                           const bx::Ctrl& clock);

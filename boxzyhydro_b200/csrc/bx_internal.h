@@ -131,6 +131,9 @@ cudaError_t phase_courant_finish(Ctrl* ctrl, cudaStream_t s);
 cudaError_t phase_copy_old(const Geom& g, PhaseArrays& a, cudaStream_t s);
 
 // fused <-> phase representation changes
+cudaError_t fused_to_cons(const Geom& g, const double* X, int nsrc, double* cons, int nghost,
+                          const int32_t* dst, const int32_t* src2, const uint8_t* sgn2,
+                          cudaStream_t s);
 cudaError_t fused_to_phase(const Geom& g, const double* X, int nsrc, PhaseArrays& a, int nghost,
                            const int32_t* dst, const int32_t* src2, const uint8_t* sgn2,
                            cudaStream_t s, long long xps = 0);

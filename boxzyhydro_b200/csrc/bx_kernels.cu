@@ -961,6 +961,16 @@ cudaError_t fused_to_phase(const Geom& g, const double* X, int nsrc, PhaseArrays
   k_f2p_prims<<<nblk(g.ng), PB, 0, s>>>(g, a);
   return cudaGetLastError();
 }
+// the reference cons only (no primitives) of the fused state X into cons
+cudaError_t fused_to_cons(const Geom& g, const double* X, int nsrc, double* cons, int nghost,
+                          const int32_t* dst, const int32_t* src2, const uint8_t* sgn2,
+                          cudaStream_t s) {
+  PhaseArrays a{};
+  a.cons = cons;
+  k_f2p_interior<<<nblk(g.ng), PB, 0, s>>>(g, X, g.ng, nsrc, a);
+  if (nghost > 0) k_fill_resolved<<<nblk(nghost), PB, 0, s>>>(nghost, dst, src2, sgn2, cons, g.ng);
+  return cudaGetLastError();
+}
 // does a box's plane set hold a state the fused stages start from
 // (interior rho >= 1e-4 and finite, ghosts = two-sweep fill of the interior)?
 __global__ void k_box_check_cells(Geom g, const double* X, long long ps, Ctrl* ctrl) {
