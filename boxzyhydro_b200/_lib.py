@@ -65,6 +65,8 @@ def lib():
         "bx_get_clock": (C.c_int, [H, dp, dp, dp, i64p]),
         "bx_step": (C.c_int, [H, C.c_double, i32p]),
         "bx_run": (C.c_int, [H, C.c_double, C.c_int64, i64p]),
+        "bx_write_celldump": (C.c_int, [H, C.c_char_p, vp]),
+        "bx_read_celldump": (C.c_int, [H, C.c_char_p, vp, dp, i64p]),
         "bx_state": (C.c_int, [H]),
         "bx_velocity": (C.c_int, [H]),
         "bx_courant": (C.c_int, [H, dp]),

@@ -56,7 +56,7 @@ static cudaError_t dalloc(void** p, size_t bytes) {
   return cudaMalloc(p, bytes);
 }
 
-// ---- tiles: 32x8 column tiles times z chunks sized so the launch fills the GPU
+// ---- tiles: TX x TY column tiles times z chunks sized so the launch fills the GPU
 static std::vector<Tile> make_tiles(const Geom& g, int box, int slots) {
   const int NAx = g.ax1 - g.ax0, NAy = g.ay1 - g.ay0, NAz = g.az1 - g.az0;
   const int tx = (NAx + TX - 1) / TX, ty = (NAy + TY - 1) / TY;

@@ -2,7 +2,7 @@
 //
 // All boxes share three pooled plane sets (each box's cells at its own offset),
 // one table of per-box geometry and clocks, and one tile list that covers every
-// box: 32x8 interior column tiles (z split into chunks of at most 32 planes for
+// box: TX x TY interior column tiles (z split into chunks of at most 32 planes for
 // large boxes), ordered by decreasing work so that the block scheduler hands the
 // longest tiles out first.  A step is four launches for the whole ensemble --
 // per-box dt control, stage 0, stage 1, per-box clock advance -- the same stage

@@ -3,7 +3,7 @@
 // Two kernel families compute the same reference step:
 //
 //  * Fused stage kernels (k_stage<0|1>): one launch per SSP-RK2 stage.  A block
-//    owns a 32x8 column tile of interior cells and marches through a z range.
+//    owns a TX x TY column tile of interior cells and marches through a z range.
 //    For each z plane it stages primitives of the tile plus a two-cell x/y halo
 //    in shared memory, builds the limited MUSCL face states once per cell and
 //    direction, computes every x/y face flux once, carries the z-direction
@@ -184,7 +184,7 @@ __device__ __forceinline__ double warp_max(double v) {
 }  // namespace
 
 // ------------------------------------------------------------------ stage kernel
-// One tile of one stage.  FULL: the tile is a whole 32x8 block of interior
+// One tile of one stage.  FULL: the tile is a whole TX x TY block of interior
 // columns, so its extents are compile-time constants.
 template <int STAGE, bool POW2, bool THREED, bool FULL>
 __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, const Geom& g,
@@ -248,7 +248,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
       }
       put_prim(SP, (ty + 2) * PW + (tx + 2), Pk);
     }
-    for (int i = tid; i < nhalo; i += TX * TY) {
+    // halo cells go first to the threads without a column of their own
+    for (int i = (tid + NT - TX * TY) % NT; i < nhalo; i += NT) {
       int cx, cy;
       if (i < 4 * h) {
         cy = i >> 2;
@@ -278,7 +279,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
     __syncthreads();
 
     // ---- B: x and y face states of the plane
-    for (int i = tid; i < nxs + nys; i += TX * TY) {
+    for (int i = tid; i < nxs + nys; i += NT) {
       FaceState mi, pl;
       if (i < nxs) {
         const int cy = i / (w + 2), cx = i % (w + 2) - 1;
@@ -314,7 +315,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
     __syncthreads();
 
     // ---- C: x and y face fluxes (face f lies between cells f-1 and f)
-    for (int i = tid; i < nxf + nyf; i += TX * TY) {
+    for (int i = tid; i < nxf + nyf; i += NT) {
       double F[5];
       if (i < nxf) {
         const int cy = i / (w + 1), f = i % (w + 1);
@@ -409,7 +410,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
   if (tid == 0) {
     unsigned f = 0;
     double r = 0.0;
-    for (int k = 0; k < TX * TY / 32; ++k) {
+    for (int k = 0; k < NT / 32; ++k) {
       f |= red_flags[k];
       r = fmax(r, red_rate[k]);
     }
@@ -422,11 +423,11 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
 // cell sizes are multiplications by exact reciprocals), 0 = otherwise (cdiv,
 // exact for any spacing)
 template <int STAGE, int PM, bool THREED>
-__global__ void __launch_bounds__(TX* TY, 2) k_stage(StageArgs a) {
+__global__ void __launch_bounds__(NT, 2) k_stage(StageArgs a) {
   extern __shared__ double sm[];
   __shared__ Geom sg;
-  __shared__ double red_rate[TX * TY / 32];
-  __shared__ unsigned red_flags[TX * TY / 32];
+  __shared__ double red_rate[NT / 32];
+  __shared__ unsigned red_flags[NT / 32];
   const Tile t = a.tiles[blockIdx.x];
   if (threadIdx.x == 0) sg = a.geom[t.box];
   __syncthreads();
@@ -457,7 +458,7 @@ static cudaError_t launch_stage_t(const StageArgs& a, int ntiles, cudaStream_t s
     attr_set = true;
   }
   if (ntiles <= 0) return cudaSuccess;
-  k_stage<STAGE, PM, THREED><<<ntiles, TX * TY, smem, s>>>(a);
+  k_stage<STAGE, PM, THREED><<<ntiles, NT, smem, s>>>(a);
   return cudaGetLastError();
 }
 
@@ -1063,7 +1064,7 @@ int stage_blocks_per_sm(int stage, int pm, bool threed) {
     fn = pm == 1 ? (threed ? (const void*)k_stage<1, 1, true> : (const void*)k_stage<1, 1, false>)
                  : (threed ? (const void*)k_stage<1, 0, true> : (const void*)k_stage<1, 0, false>);
   cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, TX * TY, smem) != cudaSuccess) {
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, NT, smem) != cudaSuccess) {
     cudaGetLastError();
     return 1;
   }

@@ -10,6 +10,7 @@ boundary in the reference layout: cons (ng,5), u (ng,3), p (ng,).
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -105,6 +106,23 @@ class Hydro:
 
     def set_dt(self, dt):
         self._c(lib().bx_set_dt(self._h, float(dt)))
+
+    # ---- celldump files (write_files.f90:55-63, read_hydro.f90:122-187)
+    def write_celldump(self, path, phi=None):
+        """state() on the arrays, then the celldump of the handle's state."""
+        ph = _arr(phi, self.ng, 1)
+        self._c(lib().bx_write_celldump(self._h, os.fsencode(path),
+                                        None if ph is None else ph.ctypes.data_as(C.c_void_p)))
+
+    def read_celldump(self, path, want_phi=False):
+        """Restart from a celldump: returns (time, step[, phi])."""
+        ph = np.empty(self.ng) if want_phi else None
+        t = C.c_double()
+        st = C.c_int64()
+        self._c(lib().bx_read_celldump(self._h, os.fsencode(path),
+                                       None if ph is None else ph.ctypes.data_as(C.c_void_p),
+                                       C.byref(t), C.byref(st)))
+        return (t.value, st.value, ph) if want_phi else (t.value, st.value)
 
     # ---- the reference's subroutines
     def state(self):

@@ -102,6 +102,23 @@ int bx_step(bx_handle *h, double endtime, int32_t *ran);
 /* Repeat bx_step until time >= endtime or nsteps steps ran. */
 int bx_run(bx_handle *h, double endtime, int64_t nsteps, int64_t *steps_taken);
 
+/* celldump files (Fortran unformatted sequential, 4-byte record markers as built
+ * with -frecord-marker=4): readtest=1234, (time, step), the 8 units of
+ * units.f90:10-17, then per cell (x, y, z, rho, p, u1, u2, u3, phi, E, muc, boundary).
+ *
+ * bx_write_celldump replaces write_files.f90:28-65 (hydro part): it applies
+ * state() to the handle's arrays first (write_files.f90:32, with the same effect
+ * on them), then writes the arrays with the handle's clock.  phi: ngrid host
+ * doubles, or NULL for zeros (phi is zero without gravity, main.f90:185).
+ *
+ * bx_read_celldump replaces read_hydro.f90:122-187 plus main.f90:196-199: reads
+ * rho, p, u, E, rebuilds m = u*rho, resets the outermost cell layer to
+ * (small_rho, 0, 0, 0, small_eps), uploads, applies state() and sets the clock to
+ * the file's time and step with dtold = 0.  phi (ngrid host doubles), time and
+ * step receive the file's values when not NULL. */
+int bx_write_celldump(bx_handle *h, const char *path, const double *phi);
+int bx_read_celldump(bx_handle *h, const char *path, double *phi, double *time, int64_t *step);
+
 /* Per-phase entry points on the handle's module arrays, for bisection against the
  * reference.  They act exactly like the subroutines they replace. */
 int bx_state(bx_handle *h);                /* state.f90:6-89 (H2STAT=-1 branch) */
