@@ -77,6 +77,7 @@ def lib():
         "bx_save_cons_old": (C.c_int, [H]),
         "bx_set_dt": (C.c_int, [H, C.c_double]),
         "bx_set_gforce": (C.c_int, [H, vp]),
+        "bx_set_phi": (C.c_int, [H, vp]),
         "bx_status": (C.c_int, [H, C.POINTER(C.c_uint32), i32p]),
         "bx_device_cons": (C.c_int, [H, C.POINTER(C.c_void_p), i64p]),
         "bx_ghost_plan": (C.c_int, [C.POINTER(BxParams), i64p, vp, vp, vp, vp, vp, i32p]),

@@ -447,6 +447,20 @@ int bx_set_gforce(bx_handle* h, const double* gforce) {
   return BX_OK;
 }
 
+int bx_set_phi(bx_handle* h, const double* phi) {
+  CHECK_H();
+  if (!phi) return bx_set_gforce(h, nullptr);
+  const long long n = h->g.ng;
+  if (!h->pa.gforce) CK(dalloc((void**)&h->pa.gforce, 3 * n * sizeof(double)));
+  if (int r = to_phase(h)) return r;
+  double* tmp = staging(h);
+  CK(cudaMemcpyAsync(tmp, phi, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
+  CK(phase_calc_gforce(h->g, tmp, h->pa.gforce, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
+  h->gforce_set = true;
+  return BX_OK;
+}
+
 int bx_status(bx_handle* h, uint32_t* bits, int32_t* last_path) {
   CHECK_H();
   if (bits) *bits = h->status;

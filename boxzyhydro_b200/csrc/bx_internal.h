@@ -141,6 +141,7 @@ cudaError_t phase_state(const Geom& g, PhaseArrays& a, Ctrl* ctrl, cudaStream_t 
 cudaError_t phase_velocity(const Geom& g, PhaseArrays& a, Ctrl* ctrl, cudaStream_t s);
 cudaError_t phase_courant(const Geom& g, PhaseArrays& a, Ctrl* ctrl, cudaStream_t s);
 cudaError_t phase_source(const Geom& g, PhaseArrays& a, Ctrl* ctrl, double mult, cudaStream_t s);
+cudaError_t phase_calc_gforce(const Geom& g, const double* phi, double* gforce, cudaStream_t s);
 cudaError_t phase_ghost(int nghost, const int32_t* dst, const int32_t* src, const uint8_t* sgn,
                         PhaseArrays& a, long long ng, cudaStream_t s);
 cudaError_t phase_flux(const Geom& g, PhaseArrays& a, Ctrl* ctrl, int avg, cudaStream_t s);

@@ -933,6 +933,32 @@ cudaError_t phase_courant_finish(Ctrl* ctrl, cudaStream_t s) {
   k_phase_courant_finish<<<1, 1, 0, s>>>(ctrl);
   return cudaGetLastError();
 }
+// calc_gforce (utils.f90:549-571): central differences of the potential on
+// interior cells, g = -(phi(+) - phi(-))/(2 d) per axis; the z neighbours of a
+// grid without z ghost layers are the cell itself.  Ghost rows are set to zero
+// (source() reads interior cells only).
+__global__ void k_calc_gforce(Geom g, const double* phi, double* gf) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= g.ng) return;
+  const long long n = g.ng;
+  const int x = (int)(i % g.nx), y = (int)((i / g.nx) % g.ny), z = (int)(i / g.sz);
+  if (is_ghost(g, x, y, z)) {
+    gf[i] = 0.0;
+    gf[n + i] = 0.0;
+    gf[2 * n + i] = 0.0;
+    return;
+  }
+  const long long sz = g.threed ? g.sz : 0;
+  gf[i] = -(phi[i + 1] - phi[i - 1]) / (2.0 * g.dx);
+  gf[n + i] = -(phi[i + g.sy] - phi[i - g.sy]) / (2.0 * g.dy);
+  gf[2 * n + i] = -(phi[i + sz] - phi[i - sz]) / (2.0 * g.dz);
+}
+
+cudaError_t phase_calc_gforce(const Geom& g, const double* phi, double* gforce, cudaStream_t s) {
+  k_calc_gforce<<<nblk(g.ng), PB, 0, s>>>(g, phi, gforce);
+  return cudaGetLastError();
+}
+
 cudaError_t phase_source(const Geom& g, PhaseArrays& a, Ctrl* ctrl, double mult, cudaStream_t s) {
   k_phase_source<<<nblk(g.ng), PB, 0, s>>>(g, a, ctrl, mult);
   return cudaGetLastError();

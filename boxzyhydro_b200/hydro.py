@@ -84,6 +84,11 @@ class Hydro:
         g = _arr(g3, self.ng, 3)
         self._c(lib().bx_set_gforce(self._h, None if g is None else g.ctypes.data_as(C.c_void_p)))
 
+    def set_phi(self, phi):
+        """Gravitational potential from the host's solver: gforce by calc_gforce."""
+        ph = _arr(phi, self.ng, 1)
+        self._c(lib().bx_set_phi(self._h, None if ph is None else ph.ctypes.data_as(C.c_void_p)))
+
     def set_stream(self, stream_ptr):
         self._c(lib().bx_set_stream(self._h, C.c_void_p(stream_ptr) if stream_ptr else None))
 

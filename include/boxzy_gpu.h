@@ -136,6 +136,13 @@ int bx_set_dt(bx_handle *h, double dt);    /* the module variable dt (grid_commo
  * NULL restores the zero force of a run without a gravity solver. */
 int bx_set_gforce(bx_handle *h, const double *gforce);
 
+/* The gravity coupling of a run with a potential solver (main.f90:143-149,477-483
+ * under USEPOTENTIAL): phi(ngrid) from the host's solver, turned into gforce on the
+ * device by calc_gforce (utils.f90:549-571, central differences on interior cells).
+ * Call it whenever the solver updates phi (each step); NULL removes the force.
+ * Steps with a force run the per-phase kernels. */
+int bx_set_phi(bx_handle *h, const double *phi);
+
 /* Status bits accumulated since the last call (BX_STATUS_*) and the path the
  * last step took (0 = per-phase kernels, 1 = fused stage kernels). */
 int bx_status(bx_handle *h, uint32_t *status_bits, int32_t *last_path);

@@ -139,6 +139,20 @@ class Oracle:
         g = None if g3 is None else np.ascontiguousarray(g3, dtype=np.float64)
         lib().ox_set_gforce(self._h, _ptr(g))
 
+    def calc_gforce(self, phi):
+        """utils.f90:549-571 (calc_gforce): gforce = -(phi(b+) - phi(b-))/(2 d) on
+        interior cells through the neighbour table (b(3)/b(4) x, b(1)/b(2) y,
+        b(5)/b(6) z); ghost rows zero."""
+        b, nb = self.grid_info()
+        m = b == 0
+        P = self.params
+        phi = np.asarray(phi, dtype=np.float64)
+        g = np.zeros((self.ng, 3))
+        g[m, 0] = -(phi[nb[m, 2]] - phi[nb[m, 3]]) / (2.0 * P.dx)
+        g[m, 1] = -(phi[nb[m, 0]] - phi[nb[m, 1]]) / (2.0 * P.dy)
+        g[m, 2] = -(phi[nb[m, 4]] - phi[nb[m, 5]]) / (2.0 * P.dz)
+        return g
+
     def get_cons_old(self):
         c = np.empty((self.ng, 5))
         lib().ox_get_cons_old(self._h, _ptr(c))
