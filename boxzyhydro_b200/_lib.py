@@ -32,7 +32,7 @@ class BxParams(C.Structure):
         ("cfl", C.c_double), ("small_rho", C.c_double), ("small_eps", C.c_double),
         ("vlimit", C.c_double), ("gammafix", C.c_double), ("muc", C.c_double),
         ("rgas", C.c_double), ("no_outflow", C.c_int32 * 6), ("fluxangmom", C.c_int32),
-        ("flags", C.c_int32),
+        ("flags", C.c_int32), ("yoffset", C.c_double),
     ]
 
 
@@ -140,4 +140,5 @@ def make_params(hp, flags=0) -> BxParams:
         p.no_outflow[k] = 1 if w else 0
     p.fluxangmom = 1 if hp.fluxangmom else 0
     p.flags = int(flags)
+    p.yoffset = float(hp.yoffset)
     return p

@@ -884,8 +884,8 @@ int bx_adj_create(const bx_params* params, int64_t nsteps, int32_t snapshots, bx
   if (!A->h->eligible) {
     bx_adj_destroy(A);
     return aerr(nullptr, BX_ERR_UNSUPPORTED,
-                "the adjoint follows the fused stage kernels; this grid's ghost fill does not "
-                "resolve within two sweeps");
+                "the adjoint follows the fused stage kernels, which this grid does not run "
+                "(ghost fill not resolved within two sweeps, or fluxangmom)");
   }
   const long long n = A->h->g.ng;
   A->ng = n;

@@ -109,8 +109,6 @@ static int create_handle(const bx_params* params, bx_handle** out, bool lean) {
   const bx_params& P = *params;
   if (P.h2stat != -1)
     return set_err(nullptr, BX_ERR_UNSUPPORTED, "only H2STAT=-1 (fixed gamma) is supported");
-  if (P.fluxangmom)
-    return set_err(nullptr, BX_ERR_UNSUPPORTED, "fluxangmom=.true. is not supported");
   if (P.nx < 5 || P.ny < 5 || P.nz < 1 || (P.nz >= 6 && P.nz < 5))
     return set_err(nullptr, BX_ERR_ARG, "grid too small: need nx,ny>=5");
   if ((long long)P.nx * P.ny * P.nz >= (1ll << 31))
@@ -126,7 +124,9 @@ static int create_handle(const bx_params* params, bx_handle** out, bool lean) {
   h->P = P;
   fill_geom(P, h->g);
   build_ghost_tables(P, h->T);
-  h->eligible = h->T.resolved2 && h->T.face_rule_ok && !(P.flags & BX_FLAG_PHASE_ONLY);
+  // flux_ang runs on the per-phase kernels only
+  h->eligible = h->T.resolved2 && h->T.face_rule_ok && !(P.flags & BX_FLAG_PHASE_ONLY) &&
+                !P.fluxangmom;
   const long long ng = h->g.ng;
   h->nghost = (int)h->T.dst.size();
   auto fail = [&](int code) {
@@ -250,7 +250,8 @@ static int push_clock(bx_handle* h) {
 }
 
 static int ensure_states(bx_handle* h) {
-  if (!h->pa.states) CK(dalloc((void**)&h->pa.states, 42 * h->g.ng * sizeof(double)));
+  if (!h->pa.states)
+    CK(dalloc((void**)&h->pa.states, (h->g.ang ? 54 : 42) * h->g.ng * sizeof(double)));
   return BX_OK;
 }
 

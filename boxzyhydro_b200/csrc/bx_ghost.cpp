@@ -65,6 +65,8 @@ void fill_geom(const bx_params& P, Geom& g) {
   g.cfl = P.cfl;
   g.muc = P.muc;
   g.rgas = P.rgas;
+  g.ang = P.fluxangmom ? 1 : 0;
+  g.yoff = P.yoffset;
 }
 
 namespace {

@@ -62,6 +62,8 @@ struct Geom {
   double ayz, axz, axy, vol, ivol;
   double gam, gm1, small_rho, small_eps, vlimit, cfl;
   double muc, rgas;
+  int ang;                 // flux_ang.f90 in place of flux.f90 (fluxangmom)
+  double yoff;             // yoffset of the angular-momentum transforms
 };
 
 // Work item of the tiled stage kernel: one 32x8 column tile and a z range of a box.

@@ -724,7 +724,41 @@ __global__ void k_ghost_scatter(int nghost, const int32_t* dst, const double* tm
 // flux.f90:47-116: slopes and interface states of every cell.
 // states layout: [(dir*2+side)*7 + q][cell], side 0 = minus, 1 = plus,
 // q = rho, u1, u2, u3, p, eps, gamma.
+// cell centre of cell i (init_grid.f90:84-92)
+__device__ __forceinline__ void cell_xy(const Geom& g, long long i, double& x, double& y) {
+  const int ix = (int)(i % g.nx), iy = (int)((i / g.nx) % g.ny);
+  x = g.dx * ((double)(ix + 1) - ((double)g.nx + 1.0) / 2.0);
+  y = g.dy * ((double)(iy + 1) - ((double)g.ny + 1.0) / 2.0);
+}
+
+// flux_ang.f90:44-62: (m1, m2) -> (radial momentum, angular momentum) about the
+// z axis through (0, -yoffset), on cons and (stage 1) cons_old
+__global__ void k_ang_to(Geom g, PhaseArrays a, int avg) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= g.ng) return;
+  const long long n = g.ng;
+  double x, y;
+  cell_xy(g, i, x, y);
+  y = y + g.yoff;
+  const double r = sqrt(x * x + y * y);
+  double m1 = a.cons[n + i], m2 = a.cons[2 * n + i];
+  a.cons[n + i] = (m1 * x + m2 * y) / r;
+  a.cons[2 * n + i] = x * m2 - y * m1;
+  if (avg > 0) {
+    m1 = a.cons_old[n + i];
+    m2 = a.cons_old[2 * n + i];
+    a.cons_old[n + i] = (m1 * x + m2 * y) / r;
+    a.cons_old[2 * n + i] = x * m2 - y * m1;
+  }
+}
+
+// flux.f90:253-482 (and flux_ang.f90:301-518 when ANG): slopes and face states
+// of every cell.  States: [(dir*2 + side)*NQ + k] planes, side 0 minus, 1 plus;
+// k = rho, u1, u2, u3, p, eps, gamma (and, with ANG, the radial and angular
+// momenta of the transformed cons(2), cons(3)).
+template <bool ANG>
 __global__ void k_phase_states(Geom g, PhaseArrays a, Ctrl* ctrl) {
+  constexpr int NQ = ANG ? 9 : 7;
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= g.ng) return;
   const long long n = g.ng;
@@ -741,7 +775,7 @@ __global__ void k_phase_states(Geom g, PhaseArrays a, Ctrl* ctrl) {
   for (int dir = 0; dir < 3; ++dir) {
     const long long im = ghost ? i : i - st[dir], ip = ghost ? i : i + st[dir];
     const long long idx3[3] = {im, i, ip};
-    double sl[7];
+    double sl[NQ];
     for (int k = 0; k < 3; ++k)
       sl[1 + k] = slope3(u[k * n + im], u[k * n + i], u[k * n + ip]);
     double eps[3];
@@ -753,38 +787,81 @@ __global__ void k_phase_states(Geom g, PhaseArrays a, Ctrl* ctrl) {
     sl[0] = slope3(c[im], c[i], c[ip]);
     sl[5] = slope3(eps[0], eps[1], eps[2]);
     sl[6] = slope3(a.adindx[im], a.adindx[i], a.adindx[ip]);
+    if (ANG) {
+      sl[7] = slope3(c[n + im], c[n + i], c[n + ip]);
+      sl[NQ - 1] = slope3(c[2 * n + im], c[2 * n + i], c[2 * n + ip]);
+    }
     const double ud = u[dir * n + i];
     const double lp = fmax(ud + sound, 0.0) * dt / ds[dir];
     const double lm = fmin(ud - sound, 0.0) * dt / ds[dir];
-    const double q[7] = {d0, u[i], u[n + i], u[2 * n + i], a.p[i], eps0, a.adindx[i]};
-    for (int k = 0; k < 7; ++k) {
+    double q[NQ];
+    q[0] = d0; q[1] = u[i]; q[2] = u[n + i]; q[3] = u[2 * n + i];
+    q[4] = a.p[i]; q[5] = eps0; q[6] = a.adindx[i];
+    if (ANG) {
+      q[7] = c[n + i];
+      q[NQ - 1] = c[2 * n + i];
+    }
+    for (int k = 0; k < NQ; ++k) {
       const double mi = q[k] + kHalf * (-1.0 - lm) * sl[k];
       const double pl = q[k] + kHalf * (1.0 - lp) * sl[k];
-      a.states[((dir * 2 + 0) * 7 + k) * n + i] = mi + 0.0 * (dt * kHalf / ds[dir]);
-      a.states[((dir * 2 + 1) * 7 + k) * n + i] = pl + 0.0 * (dt * kHalf / ds[dir]);
+      // the zero transverse terms of flux.f90:391-479 (not applied to the
+      // momenta of flux_ang)
+      const bool tr = k < 7;
+      a.states[((dir * 2 + 0) * NQ + k) * n + i] = tr ? mi + 0.0 * (dt * kHalf / ds[dir]) : mi;
+      a.states[((dir * 2 + 1) * NQ + k) * n + i] = tr ? pl + 0.0 * (dt * kHalf / ds[dir]) : pl;
     }
   }
 }
 
+// HLL flux through the face between cells lc and rc in direction dir
+// (flux.f90:487-590); with ANG the momenta are the transformed ones and the
+// pressure terms follow flux_ang.f90:523-618 at the updated cell's centre (x, y,
+// r, without yoffset)
+template <bool ANG>
 __device__ __forceinline__ void phase_face(const double* S, long long n, int dir, long long lc,
-                                           long long rc, double F[5]) {
+                                           long long rc, double x, double y, double r,
+                                           double F[5]) {
+  constexpr int NQ = ANG ? 9 : 7;
   // plus state of the low cell, minus state of the high cell (flux.f90:504-530)
-  const double* Lp = S + ((dir * 2 + 1) * 7) * n;
-  const double* Rm = S + ((dir * 2 + 0) * 7) * n;
+  const double* Lp = S + ((dir * 2 + 1) * NQ) * n;
+  const double* Rm = S + ((dir * 2 + 0) * NQ) * n;
   const double dl = Lp[lc], vxl = Lp[n + lc], vyl = Lp[2 * n + lc], vzl = Lp[3 * n + lc],
                pl = Lp[4 * n + lc], el = Lp[5 * n + lc], gl = Lp[6 * n + lc];
   const double dr = Rm[rc], vxr = Rm[n + rc], vyr = Rm[2 * n + rc], vzr = Rm[3 * n + rc],
                pr = Rm[4 * n + rc], er = Rm[5 * n + rc], gr = Rm[6 * n + rc];
   double sl[5], sr[5], fl[5], fr[5];
-  sl[0] = dl; sl[1] = dl * vxl; sl[2] = dl * vyl; sl[3] = dl * vzl;
+  sl[0] = dl;
+  sr[0] = dr;
+  if (ANG) {
+    sl[1] = Lp[7 * n + lc]; sl[2] = Lp[(NQ - 1) * n + lc];
+    sr[1] = Rm[7 * n + rc]; sr[2] = Rm[(NQ - 1) * n + rc];
+  } else {
+    sl[1] = dl * vxl; sl[2] = dl * vyl;
+    sr[1] = dr * vxr; sr[2] = dr * vyr;
+  }
+  sl[3] = dl * vzl;
   sl[4] = el + kHalf * dl * (vxl * vxl + vyl * vyl + vzl * vzl);
-  sr[0] = dr; sr[1] = dr * vxr; sr[2] = dr * vyr; sr[3] = dr * vzr;
+  sr[3] = dr * vzr;
   sr[4] = er + kHalf * dr * (vxr * vxr + vyr * vyr + vzr * vzr);
   for (int k = 0; k < 5; ++k) { fl[k] = 0.0; fr[k] = 0.0; }
   double vl, vr;
-  if (dir == 0) { vr = vxr; vl = vxl; fl[1] = pl; fr[1] = pr; }
-  else if (dir == 1) { vr = vyr; vl = vyl; fl[2] = pl; fr[2] = pr; }
-  else { vr = vzr; vl = vzl; fl[3] = pl; fr[3] = pr; }
+  if (ANG) {
+    if (dir == 0) {
+      vr = vxr; vl = vxl;
+      fl[1] = pl * x / r; fr[1] = pr * x / r;
+      fl[2] = -(pl * y); fr[2] = -(pr * y);
+    } else if (dir == 1) {
+      vr = vyr; vl = vyl;
+      fl[1] = pl * y / r; fr[1] = pr * y / r;
+      fl[2] = pl * x; fr[2] = pr * x;
+    } else {
+      vr = vzr; vl = vzl; fl[3] = pl; fr[3] = pr;
+    }
+  } else {
+    if (dir == 0) { vr = vxr; vl = vxl; fl[1] = pl; fr[1] = pr; }
+    else if (dir == 1) { vr = vyr; vl = vyl; fl[2] = pl; fr[2] = pr; }
+    else { vr = vzr; vl = vzl; fl[3] = pl; fr[3] = pr; }
+  }
   fl[0] = sl[0] * vl;
   fl[1] = fl[1] + sl[1] * vl;
   fl[2] = fl[2] + sl[2] * vl;
@@ -802,20 +879,27 @@ __device__ __forceinline__ void phase_face(const double* S, long long n, int dir
   for (int k = 0; k < 5; ++k) F[k] = (ap * fl[k] + am * fr[k] - ap * am * (sr[k] - sl[k])) / (ap + am);
 }
 
-// flux.f90:121-230: face fluxes of interior cells, update of every cell, floors
+// flux.f90:121-230 (flux_ang.f90:149-276 with ANG): face fluxes of interior
+// cells, update of every cell, (ANG) momenta back to (m1, m2), floors
+template <bool ANG>
 __global__ void k_phase_update(Geom g, PhaseArrays a, Ctrl* ctrl, int avg) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= g.ng) return;
   const long long n = g.ng;
   const int x = (int)(i % g.nx), y = (int)((i / g.nx) % g.ny), z = (int)(i / g.sz);
   const double dt = ctrl->dt;
+  double cx = 0.0, cy = 0.0, cr = 0.0;
+  if (ANG) {
+    cell_xy(g, i, cx, cy);
+    cr = sqrt(cx * cx + cy * cy);
+  }
   double ft[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
   if (!is_ghost(g, x, y, z)) {
     const long long st[3] = {1, g.sy, g.threed ? g.sz : 0};
     double fm[3][5], fp[3][5];
     for (int dir = 0; dir < 3; ++dir) {
-      phase_face(a.states, n, dir, i - st[dir], i, fm[dir]);
-      phase_face(a.states, n, dir, i, i + st[dir], fp[dir]);
+      phase_face<ANG>(a.states, n, dir, i - st[dir], i, cx, cy, cr, fm[dir]);
+      phase_face<ANG>(a.states, n, dir, i, i + st[dir], cx, cy, cr, fp[dir]);
     }
     for (int k = 0; k < 5; ++k)
       ft[k] = -(g.ayz * (fp[0][k] - fm[0][k]) + g.axz * (fp[1][k] - fm[1][k]) +
@@ -825,6 +909,18 @@ __global__ void k_phase_update(Geom g, PhaseArrays a, Ctrl* ctrl, int avg) {
   for (int k = 0; k < 5; ++k) {
     const double c = a.cons[k * n + i];
     v[k] = avg == 0 ? c + ft[k] : kHalf * (a.cons_old[k * n + i] + c + ft[k]);
+  }
+  if (ANG) {
+    // flux_ang.f90:247-270, about the axis through (0, -yoffset)
+    const double ty = cy + g.yoff, tr = sqrt(cx * cx + ty * ty);
+    const double rmom = v[1], angmom = v[2];
+    v[1] = (rmom * cx - angmom * ty / tr) / tr;
+    v[2] = (rmom * ty + angmom * cx / tr) / tr;
+    if (avg > 0) {
+      const double ro = a.cons_old[n + i], ao = a.cons_old[2 * n + i];
+      a.cons_old[n + i] = (ro * cx - ao * ty / tr) / tr;
+      a.cons_old[2 * n + i] = (ro * ty + ao * cx / tr) / tr;
+    }
   }
   floors(v[0], v[1], v[2], v[3], v[4], g.small_rho, g.small_eps);
   bool bad = false;
@@ -971,8 +1067,14 @@ cudaError_t phase_ghost(int nghost, const int32_t* dst, const int32_t* src, cons
   return cudaGetLastError();
 }
 cudaError_t phase_flux(const Geom& g, PhaseArrays& a, Ctrl* ctrl, int avg, cudaStream_t s) {
-  k_phase_states<<<nblk(g.ng), PB, 0, s>>>(g, a, ctrl);
-  k_phase_update<<<nblk(g.ng), PB, 0, s>>>(g, a, ctrl, avg);
+  if (g.ang) {
+    k_ang_to<<<nblk(g.ng), PB, 0, s>>>(g, a, avg);
+    k_phase_states<true><<<nblk(g.ng), PB, 0, s>>>(g, a, ctrl);
+    k_phase_update<true><<<nblk(g.ng), PB, 0, s>>>(g, a, ctrl, avg);
+  } else {
+    k_phase_states<false><<<nblk(g.ng), PB, 0, s>>>(g, a, ctrl);
+    k_phase_update<false><<<nblk(g.ng), PB, 0, s>>>(g, a, ctrl, avg);
+  }
   return cudaGetLastError();
 }
 cudaError_t phase_copy_old(const Geom& g, PhaseArrays& a, cudaStream_t s) {

@@ -97,8 +97,6 @@ class HydroParams:
     def validate(self) -> None:
         if self.h2stat != -1:
             raise ValueError("only the fixed-gamma EOS (H2STAT=-1) is on the GPU path")
-        if self.fluxangmom:
-            raise ValueError("fluxangmom=.true. (flux_ang.f90) is not on the GPU path")
         if self.nx < 5 or self.ny < 5:
             raise ValueError("nx and ny must be >= 5 (two ghost layers per side)")
         if self.nz >= 6 and self.nz < 5:
@@ -186,6 +184,4 @@ def unsupported_groups(groups: Dict[str, Dict[str, object]]) -> List[str]:
     eos = groups.get("eos_input", {})
     if int(eos.get("h2stat", 0)) != -1:
         out.append("eos_input:H2STAT (tabulated EOS)")
-    if bool(groups.get("grid_params", {}).get("fluxangmom", False)):
-        out.append("grid_params:fluxangmom")
     return out

@@ -59,8 +59,10 @@ typedef struct bx_params {
   double muc;             /* mean molecular weight, eos.f90:144 */
   double rgas;            /* scale%rgas of get_units, units.f90:17 */
   int32_t no_outflow[6];  /* grid_params no_outflow_xl,xr,yl,yr,zl,zr (reflective walls) */
-  int32_t fluxangmom;     /* grid_params fluxangmom; must be 0 */
+  int32_t fluxangmom;     /* grid_params fluxangmom: 1 = flux_ang.f90 in place of flux.f90
+                             (angular-momentum fluxing, per-phase kernels) */
   int32_t flags;          /* BX_FLAG_* */
+  double yoffset;         /* grid_params yoffset (flux_ang.f90:46,251) */
 } bx_params;
 
 typedef struct bx_handle bx_handle;

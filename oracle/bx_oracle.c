@@ -43,6 +43,8 @@ struct ox_sim {
   double *slope_u, *slope_p, *slope_d, *slope_e, *slope_g;             /* (3[,3],ng) */
   double *st_u_p, *st_u_m, *st_p_p, *st_p_m, *st_d_p, *st_d_m, *st_e_p, *st_e_m, *st_g_p,
       *st_g_m;
+  /* flux_ang: slopes and states of the transformed momenta (init_grid.f90:56-63) */
+  double *slope_rmom, *slope_amom, *st_rmom_p, *st_rmom_m, *st_amom_p, *st_amom_m;
   double time, dt, dtold, dtrate, maxv;
   int64_t step;
 };
@@ -78,7 +80,9 @@ ox_sim *ox_create(const ox_params *prm) {
   s->st_u_p = (double *)calloc(ng * 9, sizeof(double));
   s->st_u_m = (double *)calloc(ng * 9, sizeof(double));
   double **a3[] = {&s->slope_p, &s->slope_d, &s->slope_e, &s->slope_g, &s->st_p_p, &s->st_p_m,
-                   &s->st_d_p, &s->st_d_m, &s->st_e_p, &s->st_e_m, &s->st_g_p, &s->st_g_m};
+                   &s->st_d_p, &s->st_d_m, &s->st_e_p, &s->st_e_m, &s->st_g_p, &s->st_g_m,
+                   &s->slope_rmom, &s->slope_amom, &s->st_rmom_p, &s->st_rmom_m,
+                   &s->st_amom_p, &s->st_amom_m};
   for (unsigned k = 0; k < sizeof(a3) / sizeof(a3[0]); ++k)
     *a3[k] = (double *)calloc(ng * 3, sizeof(double));
 
@@ -159,7 +163,8 @@ void ox_destroy(ox_sim *s) {
                   s->cons, s->cons_old, s->fluxtmp, s->u, s->p, s->adindx, s->muc_array,
                   s->gforce, s->slope_u, s->slope_p, s->slope_d, s->slope_e, s->slope_g,
                   s->st_u_p, s->st_u_m, s->st_p_p, s->st_p_m, s->st_d_p, s->st_d_m,
-                  s->st_e_p, s->st_e_m, s->st_g_p, s->st_g_m};
+                  s->st_e_p, s->st_e_m, s->st_g_p, s->st_g_m, s->slope_rmom, s->slope_amom,
+                  s->st_rmom_p, s->st_rmom_m, s->st_amom_p, s->st_amom_m};
   for (unsigned k = 0; k < sizeof(ptrs) / sizeof(ptrs[0]); ++k) free(ptrs[k]);
   free(s);
 }
@@ -666,6 +671,197 @@ void ox_flux(ox_sim *s, int avg) {
   ox_set_ghost_cells(s);
 }
 
+/* ---------------------------------------------------------------- flux_ang.f90 */
+/* grid(igrid)%x, %y (init_grid.f90:88,92) */
+static inline double cell_x(const ox_sim *s, int64_t i) {
+  return s->P.dx * ((double)s->ix[i] - ((double)s->P.nx + ONE) / TWO);
+}
+static inline double cell_y(const ox_sim *s, int64_t i) {
+  return s->P.dy * ((double)s->iy[i] - ((double)s->P.ny + ONE) / TWO);
+}
+
+/* flux_ang.f90:301-345: calculate_slopes plus the slopes of the transformed momenta */
+static void calculate_slopes_ang(ox_sim *s, const int64_t idx[3], int idir) {
+  calculate_slopes(s, idx, idir);
+  const double *c = s->cons;
+  const int64_t i2 = idx[1];
+  s->slope_rmom[3 * i2 + idir] = slope(c[5 * idx[0] + 1], c[5 * idx[1] + 1], c[5 * idx[2] + 1]);
+  s->slope_amom[3 * i2 + idir] = slope(c[5 * idx[0] + 2], c[5 * idx[1] + 2], c[5 * idx[2] + 2]);
+}
+
+/* flux_ang.f90:349-518: calculate_states plus the states of the transformed
+ * momenta (which take no transverse term) */
+static void calculate_states_ang(ox_sim *s, int64_t idx) {
+  calculate_states(s, idx);
+  const double *c = s->cons, *u = s->u + 3 * idx;
+  const double dt = s->dt;
+  const double ds[3] = {s->P.dx, s->P.dy, s->P.dz};
+  const double sound = sqrt(s->p[idx] * s->adindx[idx] / c[5 * idx]);
+  for (int idim = 0; idim < 3; ++idim) {
+    const double lambda_p = fmax_f(u[idim] + sound, ZERO) * dt / ds[idim];
+    const double lambda_m = fmin_f(u[idim] - sound, ZERO) * dt / ds[idim];
+    interface_muscl(c[5 * idx + 1], lambda_m, lambda_p, s->slope_rmom[3 * idx + idim],
+                    &s->st_rmom_m[3 * idx + idim], &s->st_rmom_p[3 * idx + idim]);
+    interface_muscl(c[5 * idx + 2], lambda_m, lambda_p, s->slope_amom[3 * idx + idim],
+                    &s->st_amom_m[3 * idx + idim], &s->st_amom_p[3 * idx + idim]);
+  }
+}
+
+/* flux_ang.f90:523-618; x, y, r of the updated cell isten[1] (no yoffset) */
+static void get_fluxes_ang(const ox_sim *s, const int64_t isten[3], int idir, double fhll[2][5]) {
+  const int64_t idx = isten[1];
+  const double x = cell_x(s, idx), y = cell_y(s, idx);
+  const double r = sqrt(x * x + y * y);
+  for (int m_or_p = 0; m_or_p <= 1; ++m_or_p) {
+    const int64_t a = isten[m_or_p], b = isten[1 + m_or_p];
+    double dl = s->st_d_p[3 * a + idir], pl = s->st_p_p[3 * a + idir];
+    double el = s->st_e_p[3 * a + idir], gl = s->st_g_p[3 * a + idir];
+    double vxl = s->st_u_p[9 * a + 3 * idir + 0], vyl = s->st_u_p[9 * a + 3 * idir + 1],
+           vzl = s->st_u_p[9 * a + 3 * idir + 2];
+    double sl[5], sr[5], fl[5], fr[5];
+    sl[0] = dl;
+    sl[1] = s->st_rmom_p[3 * a + idir];
+    sl[2] = s->st_amom_p[3 * a + idir];
+    sl[3] = dl * vzl;
+    sl[4] = el + HALF * dl * (vxl * vxl + vyl * vyl + vzl * vzl);
+    double dr = s->st_d_m[3 * b + idir], pr = s->st_p_m[3 * b + idir];
+    double er = s->st_e_m[3 * b + idir], gr = s->st_g_m[3 * b + idir];
+    double vxr = s->st_u_m[9 * b + 3 * idir + 0], vyr = s->st_u_m[9 * b + 3 * idir + 1],
+           vzr = s->st_u_m[9 * b + 3 * idir + 2];
+    sr[0] = dr;
+    sr[1] = s->st_rmom_m[3 * b + idir];
+    sr[2] = s->st_amom_m[3 * b + idir];
+    sr[3] = dr * vzr;
+    sr[4] = er + HALF * dr * (vxr * vxr + vyr * vyr + vzr * vzr);
+    for (int k = 0; k < 5; ++k) { fl[k] = ZERO; fr[k] = ZERO; }
+    double vr, vl;
+    if (idir == 0) {
+      vr = vxr; vl = vxl;
+      fl[1] = pl * x / r; fr[1] = pr * x / r;
+      fl[2] = -(pl * y); fr[2] = -(pr * y);
+    } else if (idir == 1) {
+      vr = vyr; vl = vyl;
+      fl[1] = pl * y / r; fr[1] = pr * y / r;
+      fl[2] = pl * x; fr[2] = pr * x;
+    } else {
+      vr = vzr; vl = vzl; fl[3] = pl; fr[3] = pr;
+    }
+    fl[0] = sl[0] * vl;
+    fl[1] = fl[1] + sl[1] * vl;
+    fl[2] = fl[2] + sl[2] * vl;
+    fl[3] = fl[3] + sl[3] * vl;
+    fl[4] = (sl[4] + pl) * vl;
+    fr[0] = sr[0] * vr;
+    fr[1] = fr[1] + sr[1] * vr;
+    fr[2] = fr[2] + sr[2] * vr;
+    fr[3] = fr[3] + sr[3] * vr;
+    fr[4] = (sr[4] + pr) * vr;
+    flux_hll(fl, fr, sl, sr, gl, gr, dl, dr, pl, pr, vl, vr, fhll[m_or_p]);
+  }
+}
+
+/* flux_ang.f90:6-281 */
+void ox_flux_ang(ox_sim *s, int avg) {
+  const int64_t ng = s->ng;
+  const double dx = s->P.dx, dy = s->P.dy, dz = s->P.dz, dt = s->dt;
+  const double areaxy = dy * dx, areayz = dy * dz, areaxz = dx * dz, vol = dx * dy * dz;
+  /* flux_ang.f90:44-62: (m1, m2) -> (rmom, angmom) */
+#pragma omp parallel for schedule(static)
+  for (int64_t ig = 0; ig < ng; ++ig) {
+    const double x = cell_x(s, ig), y = cell_y(s, ig) + s->P.yoffset;
+    const double r = sqrt(x * x + y * y);
+    double *c = s->cons + 5 * ig;
+    double angmom = x * c[2] - y * c[1];
+    double rmom = (c[1] * x + c[2] * y) / r;
+    c[1] = rmom;
+    c[2] = angmom;
+    if (avg > 0) {
+      double *o = s->cons_old + 5 * ig;
+      angmom = x * o[2] - y * o[1];
+      rmom = (o[1] * x + o[2] * y) / r;
+      o[1] = rmom;
+      o[2] = angmom;
+    }
+  }
+  /* flux_ang.f90:69-106 slopes */
+#pragma omp parallel for schedule(static)
+  for (int64_t ig = 0; ig < ng; ++ig) {
+    for (int k = 0; k < 9; ++k) s->slope_u[9 * ig + k] = ZERO;
+    for (int k = 0; k < 3; ++k) {
+      s->slope_p[3 * ig + k] = ZERO; s->slope_d[3 * ig + k] = ZERO;
+      s->slope_e[3 * ig + k] = ZERO; s->slope_g[3 * ig + k] = ZERO;
+      s->slope_rmom[3 * ig + k] = ZERO; s->slope_amom[3 * ig + k] = ZERO;
+    }
+    for (int k = 0; k < 5; ++k) s->fluxtmp[5 * ig + k] = ZERO;
+    int64_t b[6];
+    for (int k = 0; k < 6; ++k) b[k] = (s->bnd[ig] > 0) ? ig : s->ineigh[6 * ig + k];
+    int64_t isten[3];
+    isten[0] = b[3]; isten[1] = ig; isten[2] = b[2]; calculate_slopes_ang(s, isten, 0);
+    isten[0] = b[1]; isten[1] = ig; isten[2] = b[0]; calculate_slopes_ang(s, isten, 1);
+    isten[0] = b[5]; isten[1] = ig; isten[2] = b[4]; calculate_slopes_ang(s, isten, 2);
+  }
+  /* flux_ang.f90:112-141 states */
+#pragma omp parallel for schedule(static)
+  for (int64_t ig = 0; ig < ng; ++ig) calculate_states_ang(s, ig);
+  /* flux_ang.f90:146-223 fluxes (anchors inactive, as in flux.f90) */
+#pragma omp parallel for schedule(static)
+  for (int64_t ig = 0; ig < ng; ++ig) {
+    if (s->bnd[ig] > 0) continue;
+    const int64_t *b = s->ineigh + 6 * ig;
+    double fx[2][5], fy[2][5], fz[2][5];
+    int64_t isten[3];
+    isten[0] = b[3]; isten[1] = ig; isten[2] = b[2]; get_fluxes_ang(s, isten, 0, fx);
+    isten[0] = b[1]; isten[1] = ig; isten[2] = b[0]; get_fluxes_ang(s, isten, 1, fy);
+    isten[0] = b[5]; isten[1] = ig; isten[2] = b[4]; get_fluxes_ang(s, isten, 2, fz);
+    for (int d = 0; d < 5; ++d)
+      s->fluxtmp[5 * ig + d] = -(areayz * (fx[1][d] - fx[0][d]) + areaxz * (fy[1][d] - fy[0][d]) +
+                                 areaxy * (fz[1][d] - fz[0][d])) * dt / vol;
+  }
+  /* flux_ang.f90:230-245 update */
+  if (avg == 0) {
+#pragma omp parallel for schedule(static)
+    for (int64_t ig = 0; ig < ng; ++ig)
+      for (int d = 0; d < 5; ++d) s->cons[5 * ig + d] = s->cons[5 * ig + d] + s->fluxtmp[5 * ig + d];
+  } else {
+#pragma omp parallel for schedule(static)
+    for (int64_t ig = 0; ig < ng; ++ig)
+      for (int d = 0; d < 5; ++d)
+        s->cons[5 * ig + d] =
+            HALF * (s->cons_old[5 * ig + d] + s->cons[5 * ig + d] + s->fluxtmp[5 * ig + d]);
+  }
+  /* flux_ang.f90:255-270: back to (m1, m2) */
+#pragma omp parallel for schedule(static)
+  for (int64_t ig = 0; ig < ng; ++ig) {
+    const double x = cell_x(s, ig), y = cell_y(s, ig) + s->P.yoffset;
+    const double r = sqrt(x * x + y * y);
+    double *c = s->cons + 5 * ig;
+    double angmom = c[2], rmom = c[1];
+    c[1] = (rmom * x - angmom * y / r) / r;
+    c[2] = (rmom * y + angmom * x / r) / r;
+    if (avg > 0) {
+      double *o = s->cons_old + 5 * ig;
+      angmom = o[2];
+      rmom = o[1];
+      o[1] = (rmom * x - angmom * y / r) / r;
+      o[2] = (rmom * y + angmom * x / r) / r;
+    }
+  }
+  /* flux_ang.f90:272-278 floors */
+#pragma omp parallel for schedule(static)
+  for (int64_t ig = 0; ig < ng; ++ig) {
+    double *c = s->cons + 5 * ig;
+    c[0] = fmax_f(c[0], s->P.small_rho);
+    if (c[4] < ZERO) c[4] = HALF * (c[1] * c[1] + c[2] * c[2] + c[3] * c[3]) / c[0] + s->P.small_eps;
+  }
+  ox_set_ghost_cells(s);
+}
+
+/* main.f90:343-346,365-368: flux or flux_ang */
+static void flux_step(ox_sim *s, int avg) {
+  if (s->P.fluxangmom) ox_flux_ang(s, avg);
+  else ox_flux(s, avg);
+}
+
 /* main.f90:327-333 */
 void ox_save_cons_old(ox_sim *s) {
   memcpy(s->cons_old, s->cons, s->ng * 5 * sizeof(double));
@@ -689,11 +885,11 @@ int ox_step(ox_sim *s, double endtime) {
   ox_velocity(s);
   ox_save_cons_old(s);
   s->dt = s->dt * TWO;
-  ox_flux(s, 0);
+  flux_step(s, 0);
   ox_set_ghost_cells(s);
   ox_state(s);
   ox_velocity(s);
-  ox_flux(s, 1);
+  flux_step(s, 1);
   ox_set_ghost_cells(s);
   ox_state(s);
   ox_velocity(s);
@@ -722,11 +918,11 @@ void ox_step_dt(ox_sim *s, double dt_full) {
   ox_velocity(s);
   ox_save_cons_old(s);
   s->dt = s->dt * TWO;
-  ox_flux(s, 0);
+  flux_step(s, 0);
   ox_set_ghost_cells(s);
   ox_state(s);
   ox_velocity(s);
-  ox_flux(s, 1);
+  flux_step(s, 1);
   ox_set_ghost_cells(s);
   ox_state(s);
   ox_velocity(s);

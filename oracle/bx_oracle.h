@@ -37,6 +37,9 @@ typedef struct ox_params {
   int32_t no_outflow[6];   /* xl, xr, yl, yr, zl, zr (parameters.f90:32-37) */
   int32_t racy_ghosts;     /* 1: parallel ghost loop like the reference (timing only) */
   int32_t pad;
+  int32_t fluxangmom;      /* parameters.f90:31: flux_ang.f90 in place of flux.f90 */
+  int32_t pad2;
+  double yoffset;          /* parameters.f90:30 */
 } ox_params;
 
 typedef struct ox_sim ox_sim;
@@ -68,6 +71,7 @@ void ox_courant(ox_sim *s);
 void ox_source(ox_sim *s, int siter);
 void ox_set_ghost_cells(ox_sim *s);
 void ox_flux(ox_sim *s, int avg);
+void ox_flux_ang(ox_sim *s, int avg); /* flux_ang.f90:6-281 */
 void ox_save_cons_old(ox_sim *s);
 
 /* one iteration of the main loop (main.f90:212-545); returns 0 if it ran,

@@ -29,6 +29,7 @@ class OxParams(C.Structure):
         ("vlimit", C.c_double), ("gammafix", C.c_double),
         ("muc", C.c_double), ("rgas", C.c_double),
         ("no_outflow", C.c_int32 * 6), ("racy_ghosts", C.c_int32), ("pad", C.c_int32),
+        ("fluxangmom", C.c_int32), ("pad2", C.c_int32), ("yoffset", C.c_double),
     ]
 
 
@@ -66,6 +67,7 @@ def lib():
             getattr(L, fn).argtypes = [P]
         L.ox_source.argtypes = [P, C.c_int]
         L.ox_flux.argtypes = [P, C.c_int]
+        L.ox_flux_ang.argtypes = [P, C.c_int]
         L.ox_step.argtypes = [P, C.c_double]
         L.ox_step.restype = C.c_int
         L.ox_step_dt.argtypes = [P, C.c_double]
@@ -106,6 +108,8 @@ class Oracle:
         for k, w in enumerate(params.no_outflow):
             op.no_outflow[k] = 1 if w else 0
         op.racy_ghosts = 1 if racy_ghosts else 0
+        op.fluxangmom = 1 if getattr(params, "fluxangmom", False) else 0
+        op.yoffset = float(getattr(params, "yoffset", 0.0))
         self._h = L.ox_create(C.byref(op))
         self.ng = int(L.ox_ngrid(self._h))
         self.params = params
@@ -201,7 +205,11 @@ class Oracle:
         lib().ox_set_ghost_cells(self._h)
 
     def flux(self, avg):
-        lib().ox_flux(self._h, int(avg))
+        """flux(avg), or flux_ang(avg) when fluxangmom is set (main.f90:343-346)."""
+        if getattr(self.params, "fluxangmom", False):
+            lib().ox_flux_ang(self._h, int(avg))
+        else:
+            lib().ox_flux(self._h, int(avg))
 
     def save_cons_old(self):
         lib().ox_save_cons_old(self._h)

@@ -41,7 +41,7 @@ def test_library_version_string():
 
 def test_bx_params_layout_matches_header():
     # 4 int32, 10 doubles, 6+2 int32 -> 16 + 80 + 32 bytes, no padding
-    assert ctypes.sizeof(_lib.BxParams) == 128
+    assert ctypes.sizeof(_lib.BxParams) == 136
     assert _lib.BxParams.no_outflow.offset == 96 and _lib.BxParams.flags.offset == 124
 
 

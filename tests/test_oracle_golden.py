@@ -109,3 +109,21 @@ def test_oracle_sod_x_stays_one_dimensional():
     c3 = c.reshape(hp.nz, hp.ny, hp.nx, 5)[zs, ys, xs]
     assert np.array_equal(c3, np.broadcast_to(c3[:1, :1], c3.shape))
     assert np.all(c3[..., 2:4] == 0.0)
+
+
+def test_flux_ang_keeps_a_uniform_state_at_rest():
+    """flux_ang.f90: the pressure terms of the radial and angular momentum fluxes
+    cancel between the two faces of a cell for a uniform state, so a state at
+    rest stays exactly at rest (self-check of the oracle's restatement)."""
+    import dataclasses
+
+    from tests.helpers import small_random_box
+    st = small_random_box(nx=12, ny=10, nz=8, amp=0.0, seed=0)
+    hp = dataclasses.replace(st.params, fluxangmom=True, yoffset=0.25)
+    o = O.Oracle(hp)
+    o.set_state(st.cons, st.u, st.p, st.adindx)
+    for _ in range(3):
+        o.step()
+    c, u, p, _ = o.get_state()
+    assert np.array_equal(c, st.cons) and np.all(u == 0.0)
+    o.close()
