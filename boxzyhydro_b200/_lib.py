@@ -36,6 +36,17 @@ class BxParams(C.Structure):
     ]
 
 
+class BxEosTable(C.Structure):
+    _fields_ = [
+        ("neos", C.c_int32), ("neos_rho", C.c_int32),
+        ("log_rho_eos_low", C.c_double), ("drho_eos", C.c_double),
+        ("density_unit", C.c_double), ("tk_bgrnd", C.c_double),
+        ("eng_table2", C.c_void_p), ("gamma_table2", C.c_void_p),
+        ("muc_table2", C.c_void_p), ("tk_table2", C.c_void_p),
+        ("rho_table", C.c_void_p), ("deng_eos_array", C.c_void_p),
+    ]
+
+
 _lib = None
 
 
@@ -78,6 +89,7 @@ def lib():
         "bx_set_dt": (C.c_int, [H, C.c_double]),
         "bx_set_gforce": (C.c_int, [H, vp]),
         "bx_set_phi": (C.c_int, [H, vp]),
+        "bx_set_eos_table": (C.c_int, [H, C.POINTER(BxEosTable)]),
         "bx_status": (C.c_int, [H, C.POINTER(C.c_uint32), i32p]),
         "bx_device_cons": (C.c_int, [H, C.POINTER(C.c_void_p), i64p]),
         "bx_ghost_plan": (C.c_int, [C.POINTER(BxParams), i64p, vp, vp, vp, vp, vp, i32p]),

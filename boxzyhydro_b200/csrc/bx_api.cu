@@ -107,8 +107,8 @@ int bx_create_lean(const bx_params* params, bx_handle** out) {
 static int create_handle(const bx_params* params, bx_handle** out, bool lean) {
   if (!params || !out) return set_err(nullptr, BX_ERR_ARG, "null argument");
   const bx_params& P = *params;
-  if (P.h2stat != -1)
-    return set_err(nullptr, BX_ERR_UNSUPPORTED, "only H2STAT=-1 (fixed gamma) is supported");
+  if (P.h2stat < -1)
+    return set_err(nullptr, BX_ERR_ARG, "H2STAT must be -1 (fixed gamma) or >= 0 (tables)");
   if (P.nx < 5 || P.ny < 5 || P.nz < 1 || (P.nz >= 6 && P.nz < 5))
     return set_err(nullptr, BX_ERR_ARG, "grid too small: need nx,ny>=5");
   if ((long long)P.nx * P.ny * P.nz >= (1ll << 31))
@@ -126,7 +126,7 @@ static int create_handle(const bx_params* params, bx_handle** out, bool lean) {
   build_ghost_tables(P, h->T);
   // flux_ang runs on the per-phase kernels only
   h->eligible = h->T.resolved2 && h->T.face_rule_ok && !(P.flags & BX_FLAG_PHASE_ONLY) &&
-                !P.fluxangmom;
+                !P.fluxangmom && P.h2stat == -1;
   const long long ng = h->g.ng;
   h->nghost = (int)h->T.dst.size();
   auto fail = [&](int code) {
@@ -205,6 +205,8 @@ int bx_destroy(bx_handle* h) {
   cudaFree(h->pa.gforce);
   cudaFree(h->pa.states);
   cudaFree(h->pa.gtmp);
+  cudaFree(h->pa.muc);
+  cudaFree(h->d_eos);
   cudaFree(h->d_dst);
   cudaFree(h->d_src1);
   cudaFree(h->d_src2);
@@ -373,6 +375,8 @@ int bx_set_dt(bx_handle* h, double dt) {
 // ---- per-phase entry points
 int bx_state(bx_handle* h) {
   CHECK_H();
+  if (h->g.tab && !h->pa.muc)
+    return set_err(h, BX_ERR_STATE, "H2STAT >= 0: bx_set_eos_table must come first");
   if (int r = to_phase(h)) return r;
   CK(phase_state(h->g, h->pa, h->d_ctrl, h->stream));
   return pull_clock(h);
@@ -445,6 +449,43 @@ int bx_set_gforce(bx_handle* h, const double* gforce) {
   CK(aos_to_soa(tmp, h->pa.gforce, n, 3, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   h->gforce_set = true;
+  return BX_OK;
+}
+
+int bx_set_eos_table(bx_handle* h, const bx_eos_table* t) {
+  CHECK_H();
+  if (!t || t->neos < 2 || t->neos_rho < 1 || !t->eng_table2 || !t->gamma_table2 ||
+      !t->muc_table2 || !t->tk_table2 || !t->rho_table || !t->deng_eos_array)
+    return set_err(h, BX_ERR_ARG, "incomplete EOS table (need neos >= 2, neos_rho >= 1)");
+  if (!h->g.tab) return set_err(h, BX_ERR_STATE, "the grid was created with H2STAT = -1");
+  if (int r = to_phase(h)) return r;
+  const long long n2 = (long long)t->neos * t->neos_rho, nr = t->neos_rho;
+  cudaFree(h->d_eos);
+  h->d_eos = nullptr;
+  CK(dalloc((void**)&h->d_eos, (4 * n2 + 2 * nr) * sizeof(double)));
+  const double* src[4] = {t->eng_table2, t->gamma_table2, t->muc_table2, t->tk_table2};
+  for (int k = 0; k < 4; ++k)
+    CK(cudaMemcpy(h->d_eos + k * n2, src[k], n2 * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_eos + 4 * n2, t->rho_table, nr * sizeof(double), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(h->d_eos + 4 * n2 + nr, t->deng_eos_array, nr * sizeof(double),
+                cudaMemcpyHostToDevice));
+  if (!h->pa.muc) {
+    CK(dalloc((void**)&h->pa.muc, h->g.ng * sizeof(double)));
+    CK(cudaMemset(h->pa.muc, 0, h->g.ng * sizeof(double)));
+  }
+  EosDev& e = h->pa.eos;
+  e.neos = t->neos;
+  e.neos_rho = t->neos_rho;
+  e.log_rho_low = t->log_rho_eos_low;
+  e.drho = t->drho_eos;
+  e.density_unit = t->density_unit;
+  e.tk_bgrnd = t->tk_bgrnd;
+  e.eng2 = h->d_eos;
+  e.gam2 = h->d_eos + n2;
+  e.muc2 = h->d_eos + 2 * n2;
+  e.tk2 = h->d_eos + 3 * n2;
+  e.rho = h->d_eos + 4 * n2;
+  e.deng = h->d_eos + 4 * n2 + nr;
   return BX_OK;
 }
 
@@ -568,6 +609,8 @@ static int enter_fused(bx_handle* h) {
 int bx_step(bx_handle* h, double endtime, int32_t* ran) {
   CHECK_H();
   if (ran) *ran = 0;
+  if (h->g.tab && !h->pa.muc)
+    return set_err(h, BX_ERR_STATE, "H2STAT >= 0: bx_set_eos_table must come first");
   if (h->gforce_set && h->mode == 1) {
     if (int r = to_phase(h)) return r;
   }

@@ -9,6 +9,8 @@
 //   3: the units record, 8 x float64 in the order of derived_types.f90:14-15
 //      (length, time, mass, density, rgas, eps, kelvin, vel), units.f90:10-17
 //   4..ngrid+3: float64 x, y, z, rho, p, u1, u2, u3, phi, E, muc; int32 boundary
+#include <cuda_runtime.h>
+
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -103,6 +105,16 @@ int bx_write_celldump(bx_handle* h, const char* path, const double* phi) {
   double time = 0.0, dt = 0.0, dtold = 0.0;
   int64_t step = 0;
   if (int r = bx_get_clock(h, &time, &dt, &dtold, &step)) return r;
+  // muc_array: the tables' mu per cell (H2STAT >= 0), else the constant muc
+  std::vector<double> mucv;
+  if (h->pa.muc) {
+    mucv.resize(ng);
+    if (cudaMemcpy(mucv.data(), h->pa.muc, ng * sizeof(double), cudaMemcpyDeviceToHost) !=
+        cudaSuccess) {
+      h->err = "muc download failed";
+      return BX_ERR_CUDA;
+    }
+  }
   FILE* f = std::fopen(path, "wb");
   if (!f) {
     h->err = std::string("cannot open ") + path + " for writing";
@@ -127,7 +139,7 @@ int bx_write_celldump(bx_handle* h, const char* path, const double* phi) {
       for (int ix = 1; ix <= P.nx; ++ix, ++i) {
         const double v[11] = {centre(P.dx, ix, P.nx), y, z, cons[5 * i], p[i], u[3 * i],
                               u[3 * i + 1], u[3 * i + 2], phi ? phi[i] : 0.0, cons[5 * i + 4],
-                              P.muc};
+                              mucv.empty() ? P.muc : mucv[i]};
         const int32_t b = boundary_flag(P, ix, iy, iz);
         std::memcpy(rec, v, 88);
         std::memcpy(rec + 88, &b, 4);

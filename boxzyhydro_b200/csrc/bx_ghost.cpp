@@ -66,6 +66,7 @@ void fill_geom(const bx_params& P, Geom& g) {
   g.muc = P.muc;
   g.rgas = P.rgas;
   g.ang = P.fluxangmom ? 1 : 0;
+  g.tab = P.h2stat >= 0 ? 1 : 0;
   g.yoff = P.yoffset;
 }
 

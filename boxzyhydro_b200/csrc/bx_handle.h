@@ -36,15 +36,16 @@ struct bx_handle {
   double ms_stage[2] = {0.0, 0.0};
   long long n_stage = 0;
   long long launches = 0;  // kernels of this library launched on the handle's stream
+  double* d_eos = nullptr;  // device copy of the tabulated EOS (H2STAT >= 0)
   std::string err;
 };
 
+// a handle with geometry, ghost tables, tiles, control block and stream but no
+// state planes (for engines that hold their own planes)
+int bx_create_lean(const bx_params* params, bx_handle** out);
 // Take over a fused state held elsewhere on the device: the five conserved
 // planes of one grid (plane stride `ps`), `nsrc` sources short of the
 // reference state, with the given clock.  The batched path uses it to continue
 // a box on a handle of its own.
-// a handle with geometry, ghost tables, tiles, control block and stream but no
-// state planes (for engines that hold their own planes)
-int bx_create_lean(const bx_params* params, bx_handle** out);
 int bx_handle_adopt_fused(bx_handle* h, const double* planes, long long ps, int nsrc,
                           const bx::Ctrl& clock);

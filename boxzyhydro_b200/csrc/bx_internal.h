@@ -63,6 +63,7 @@ struct Geom {
   double gam, gm1, small_rho, small_eps, vlimit, cfl;
   double muc, rgas;
   int ang;                 // flux_ang.f90 in place of flux.f90 (fluxangmom)
+  int tab;                 // tabulated EOS (H2STAT >= 0)
   double yoff;             // yoffset of the angular-momentum transforms
 };
 
@@ -128,6 +129,14 @@ cudaError_t launch_dt(Ctrl* ctrl, int nbox, cudaStream_t s);
 cudaError_t launch_end(Ctrl* ctrl, int nbox, cudaStream_t s);
 
 // phase kernels (one reference subroutine each, full arrays)
+// tabulated EOS on the device (H2STAT >= 0): tables of the eos module
+struct EosDev {
+  int neos, neos_rho;
+  double log_rho_low, drho, density_unit, tk_bgrnd;
+  const double *eng2, *gam2, *muc2, *tk2;  // (neos, neos_rho), neos fastest
+  const double *rho, *deng;                // (neos_rho)
+};
+
 struct PhaseArrays {
   double* cons;     // 5*ng SoA
   double* cons_old; // 5*ng
@@ -137,6 +146,8 @@ struct PhaseArrays {
   double* gforce;   // 3*ng or null (zero force)
   double* states;   // 42*ng scratch for flux
   double* gtmp;     // 5*nghost scratch for the ghost fill
+  double* muc;      // ng (H2STAT >= 0: muc_array of state(); else null)
+  EosDev eos;       // valid when muc is set
 };
 
 cudaError_t phase_state(const Geom& g, PhaseArrays& a, Ctrl* ctrl, cudaStream_t s);

@@ -595,6 +595,46 @@ __device__ __forceinline__ bool is_ghost(const Geom& g, int x, int y, int z) {
 }
 
 // state.f90:29-87, fixed gamma
+// get_gamma2 (eos.f90:653-699): gamma, mu and T from the tables by the specific
+// internal energy eng = eps/rho, linear in eng within the density row irho, then
+// linear in rho towards row irho+1.  eps is clamped like the reference's.
+__device__ void get_gamma2(const EosDev& e, double& eps, double rho, double& tk, double& m,
+                           double& gam) {
+  int irho = min((int)((log10(rho * e.density_unit) - e.log_rho_low) / e.drho) + 1, e.neos_rho);
+  if (irho < 1) irho = 1;
+  int irhop = irho + 1;
+  if (irhop > e.neos_rho) irhop = irho;
+  const long long ne = e.neos;
+  auto at = [&](const double* t, int ie, int ir) { return t[(ie - 1) + (ir - 1) * ne]; };
+  double eng = eps / rho;
+  int ientry = (int)((log10(eng) - log10(at(e.eng2, 1, irho))) / e.deng[irho - 1]) + 1;
+  if (ientry > e.neos - 1) {
+    ientry = e.neos - 1;
+    eng = at(e.eng2, e.neos, irho);
+    eps = eng * rho;
+  }
+  if (ientry < 1 || eng < at(e.eng2, 1, irho)) {
+    ientry = 1;
+    eng = at(e.eng2, 1, irho);
+    eps = eng * rho;
+  }
+  auto lin = [&](const double* t, int ir) {
+    return at(t, ientry, ir) + (at(t, ientry + 1, ir) - at(t, ientry, ir)) /
+                                   (at(e.eng2, ientry + 1, ir) - at(e.eng2, ientry, ir)) *
+                                   (eng - at(e.eng2, ientry, ir));
+  };
+  gam = lin(e.gam2, irho);
+  m = lin(e.muc2, irho);
+  tk = lin(e.tk2, irho);
+  if (!(e.rho[irho - 1] == e.rho[irhop - 1])) {
+    const double gamp = lin(e.gam2, irhop), mp = lin(e.muc2, irhop), tkp = lin(e.tk2, irhop);
+    const double slope = 1.0 / (e.rho[irhop - 1] - e.rho[irho - 1]) * (rho - e.rho[irho - 1]);
+    gam = gam + (gamp - gam) * slope;
+    m = m + (mp - m) * slope;
+    tk = tk + (tkp - tk) * slope;
+  }
+}
+
 __global__ void k_phase_state(Geom g, PhaseArrays a, Ctrl* ctrl) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= g.ng) return;
@@ -603,6 +643,33 @@ __global__ void k_phase_state(Geom g, PhaseArrays a, Ctrl* ctrl) {
   const double u1 = a.u[i], u2 = a.u[n + i], u3 = a.u[2 * n + i];
   const double ekin = kin_rho_u(d, u1, u2, u3);
   double eps = fmax(a.cons[4 * n + i] - ekin, g.small_eps);
+  if (g.tab) {
+    // state.f90:60-79
+    double tk, m, gam;
+    if (g.nz == 1) {
+      // disk: surface density over twice the scale height
+      const int ix = (int)(i % g.nx), iy = (int)((i / g.nx) % g.ny);
+      const double x = g.dx * ((double)(ix + 1) - ((double)g.nx + 1.0) / 2.0);
+      const double y = g.dy * ((double)(iy + 1) - ((double)g.ny + 1.0) / 2.0);
+      const double hscale = sqrt((a.adindx[i] - 1.0) * eps / (2.0 * ekin) * (x * x + y * y));
+      eps = eps / (2.0 * hscale);
+      const double rho = d / (2.0 * hscale);
+      get_gamma2(a.eos, eps, rho, tk, m, gam);
+    } else {
+      get_gamma2(a.eos, eps, d, tk, m, gam);
+    }
+    a.muc[i] = m;
+    a.adindx[i] = gam;
+    double p = (d * tk * g.rgas / m);
+    if (d < kLowRho) {
+      p = g.rgas * a.eos.tk_bgrnd / g.muc * d;
+      eps = p / (g.gam - 1.0);
+      a.cons[4 * n + i] = eps + ekin;
+      atomicOr(&ctrl->flags, (unsigned)kFlagLowRho);
+    }
+    a.p[i] = p;
+    return;
+  }
   a.adindx[i] = g.gam;
   if (d < kLowRho) {
     const double tk = fmin(5e3, a.p[i] / (d * g.rgas) * g.muc);

@@ -84,6 +84,24 @@ class Hydro:
         g = _arr(g3, self.ng, 3)
         self._c(lib().bx_set_gforce(self._h, None if g is None else g.ctypes.data_as(C.c_void_p)))
 
+    def set_eos_table(self, tab):
+        """Tables of the eos module for H2STAT >= 0 (dict with neos, neos_rho,
+        log_rho_eos_low, drho_eos, density_unit, tk_bgrnd and the arrays
+        eng_table2, gamma_table2, muc_table2, tk_table2 of shape (neos, neos_rho)
+        and rho_table, deng_eos_array of neos_rho)."""
+        keep = {k: np.asfortranarray(tab[k], dtype=np.float64)
+                for k in ("eng_table2", "gamma_table2", "muc_table2", "tk_table2",
+                          "rho_table", "deng_eos_array")}
+        t = _lib.BxEosTable()
+        t.neos, t.neos_rho = int(tab["neos"]), int(tab["neos_rho"])
+        t.log_rho_eos_low = float(tab["log_rho_eos_low"])
+        t.drho_eos = float(tab["drho_eos"])
+        t.density_unit = float(tab["density_unit"])
+        t.tk_bgrnd = float(tab["tk_bgrnd"])
+        for k, a in keep.items():
+            setattr(t, k, a.ctypes.data)
+        self._c(lib().bx_set_eos_table(self._h, C.byref(t)))
+
     def set_phi(self, phi):
         """Gravitational potential from the host's solver: gforce by calc_gforce."""
         ph = _arr(phi, self.ng, 1)

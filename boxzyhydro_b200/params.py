@@ -95,8 +95,8 @@ class HydroParams:
         return ax * ay * az
 
     def validate(self) -> None:
-        if self.h2stat != -1:
-            raise ValueError("only the fixed-gamma EOS (H2STAT=-1) is on the GPU path")
+        if self.h2stat < -1:
+            raise ValueError("H2STAT must be -1 (fixed gamma) or >= 0 (tabulated EOS)")
         if self.nx < 5 or self.ny < 5:
             raise ValueError("nx and ny must be >= 5 (two ghost layers per side)")
         if self.nz >= 6 and self.nz < 5:
@@ -176,12 +176,3 @@ def params_from_groups(groups: Dict[str, Dict[str, object]]) -> HydroParams:
                     v = float(v)
                 setattr(hp, name, v)
     return hp
-
-
-def unsupported_groups(groups: Dict[str, Dict[str, object]]) -> List[str]:
-    """Keys that select physics outside the GPU hydro path."""
-    out = []
-    eos = groups.get("eos_input", {})
-    if int(eos.get("h2stat", 0)) != -1:
-        out.append("eos_input:H2STAT (tabulated EOS)")
-    return out

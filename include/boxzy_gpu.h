@@ -14,12 +14,14 @@
  *  - Host arrays use the reference layout: cons(5,ngrid), u(3,ngrid) and
  *    p(ngrid), Fortran column-major, i.e. 5 (resp. 3, 1) doubles per cell, cells
  *    in igrid order (ix fastest).  A Fortran caller passes its allocatable
- *    arrays directly.
+ *    arrays directly (assumed-size dummies of a bind(c) interface).
  *  - Calls on one handle are single-threaded (outside OpenMP parallel regions or
  *    under !$OMP MASTER).  Each handle owns one CUDA stream unless one is given.
- *  - Only the fixed-gamma EOS (H2STAT=-1) and Cartesian fluxing
- *    (fluxangmom=.false.) are supported; other settings return
- *    BX_ERR_UNSUPPORTED from bx_create.
+ *  - Grids with the fixed-gamma EOS (H2STAT=-1), Cartesian fluxing and a zero
+ *    or no gravitational force step on the fused stage kernels; the tabulated
+ *    EOS (H2STAT>=0, bx_set_eos_table), angular-momentum fluxing
+ *    (fluxangmom=1) and a force (bx_set_gforce, bx_set_phi) step on the
+ *    per-phase kernels, with the same results as the reference's subroutines.
  */
 #ifndef BOXZY_GPU_H
 #define BOXZY_GPU_H
@@ -49,7 +51,8 @@ extern "C" {
 typedef struct bx_params {
   int32_t nx, ny, nz;     /* grid_params nx,ny,nz: cells incl. two ghost layers per side
                              (z ghosts only when nz>=6), init_grid.f90:18,76-107 */
-  int32_t h2stat;         /* eos_input H2STAT; must be -1 (state.f90:49-59) */
+  int32_t h2stat;         /* eos_input H2STAT: -1 fixed gamma (state.f90:49-59); >= 0
+                             tabulated EOS (state.f90:60-79, bx_set_eos_table) */
   double dx, dy, dz;      /* grid_params dx,dy,dz */
   double cfl;             /* hydro cfl (courant.f90:182) */
   double small_rho;       /* hydro small_rho (flux.f90:225) */
@@ -120,6 +123,25 @@ int bx_run(bx_handle *h, double endtime, int64_t nsteps, int64_t *steps_taken);
  * step receive the file's values when not NULL. */
 int bx_write_celldump(bx_handle *h, const char *path, const double *phi);
 int bx_read_celldump(bx_handle *h, const char *path, double *phi, double *time, int64_t *step);
+
+/* Tabulated EOS (H2STAT >= 0): the tables of the reference's eos module, built on
+ * the host by its own calc_eos_table (eos.f90:127-520) after initialize_eos
+ * (eos.f90:30-51), in Fortran order (energy index fastest).  state() then takes
+ * gamma, mu and T from them by get_gamma2 (eos.f90:653-699) as state.f90:60-79
+ * does (including the disk scale-height branch for nz == 1).  Such grids run the
+ * per-phase kernels; bx_set_eos_table must come before the first step. */
+typedef struct bx_eos_table {
+  int32_t neos;            /* NEOS = NEOS_T: entries per density (eng_table2 rows) */
+  int32_t neos_rho;        /* NEOS_RHO */
+  double log_rho_eos_low;  /* eos module log_rho_eos_low */
+  double drho_eos;         /* drho_eos */
+  double density_unit;     /* scl%density (units.f90:12) */
+  double tk_bgrnd;         /* parameters tk_bgrnd (state.f90:74) */
+  const double *eng_table2, *gamma_table2, *muc_table2, *tk_table2; /* (neos, neos_rho) */
+  const double *rho_table;       /* (neos_rho) */
+  const double *deng_eos_array;  /* (neos_rho) */
+} bx_eos_table;
+int bx_set_eos_table(bx_handle *h, const bx_eos_table *t);
 
 /* Per-phase entry points on the handle's module arrays, for bisection against the
  * reference.  They act exactly like the subroutines they replace. */

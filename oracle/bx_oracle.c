@@ -47,6 +47,10 @@ struct ox_sim {
   double *slope_rmom, *slope_amom, *st_rmom_p, *st_rmom_m, *st_amom_p, *st_amom_m;
   double time, dt, dtold, dtrate, maxv;
   int64_t step;
+  /* eos module tables (H2STAT >= 0) */
+  int32_t neos, neos_rho;
+  double log_rho_eos_low, drho_eos, density_unit, tk_bgrnd;
+  double *eng_table2, *gamma_table2, *muc_table2, *tk_table2, *rho_table, *deng_eos_array;
 };
 
 static inline double fmax_f(double a, double b) { return a > b ? a : b; }
@@ -164,7 +168,9 @@ void ox_destroy(ox_sim *s) {
                   s->gforce, s->slope_u, s->slope_p, s->slope_d, s->slope_e, s->slope_g,
                   s->st_u_p, s->st_u_m, s->st_p_p, s->st_p_m, s->st_d_p, s->st_d_m,
                   s->st_e_p, s->st_e_m, s->st_g_p, s->st_g_m, s->slope_rmom, s->slope_amom,
-                  s->st_rmom_p, s->st_rmom_m, s->st_amom_p, s->st_amom_m};
+                  s->st_rmom_p, s->st_rmom_m, s->st_amom_p, s->st_amom_m,
+                  s->eng_table2, s->gamma_table2, s->muc_table2, s->tk_table2, s->rho_table,
+                  s->deng_eos_array};
   for (unsigned k = 0; k < sizeof(ptrs) / sizeof(ptrs[0]); ++k) free(ptrs[k]);
   free(s);
 }
@@ -243,6 +249,75 @@ double ox_muc(double xabun, double yabun, double zabun, double mu_z) {
 }
 
 /* ---------------------------------------------------------------- state.f90:29-87 */
+void ox_set_eos_table(ox_sim *s, const ox_eos_table *t) {
+  const int64_t n2 = (int64_t)t->neos * t->neos_rho;
+  double **dst[4] = {&s->eng_table2, &s->gamma_table2, &s->muc_table2, &s->tk_table2};
+  const double *src[4] = {t->eng_table2, t->gamma_table2, t->muc_table2, t->tk_table2};
+  for (int k = 0; k < 4; ++k) {
+    free(*dst[k]);
+    *dst[k] = (double *)malloc(n2 * sizeof(double));
+    memcpy(*dst[k], src[k], n2 * sizeof(double));
+  }
+  free(s->rho_table);
+  free(s->deng_eos_array);
+  s->rho_table = (double *)malloc(t->neos_rho * sizeof(double));
+  s->deng_eos_array = (double *)malloc(t->neos_rho * sizeof(double));
+  memcpy(s->rho_table, t->rho_table, t->neos_rho * sizeof(double));
+  memcpy(s->deng_eos_array, t->deng_eos_array, t->neos_rho * sizeof(double));
+  s->neos = t->neos;
+  s->neos_rho = t->neos_rho;
+  s->log_rho_eos_low = t->log_rho_eos_low;
+  s->drho_eos = t->drho_eos;
+  s->density_unit = t->density_unit;
+  s->tk_bgrnd = t->tk_bgrnd;
+}
+void ox_get_muc(const ox_sim *s, double *muc) {
+  memcpy(muc, s->muc_array, s->ng * sizeof(double));
+}
+
+/* eos.f90:653-699 get_gamma2; tables (ientry, irho) 1-based, ientry fastest */
+static void get_gamma2(const ox_sim *s, double *eps, double rho, double *tk, double *m,
+                       double *gam) {
+#define TAB(t, ie, ir) (t)[((ie) - 1) + (int64_t)((ir) - 1) * s->neos]
+  int irho = (int)((log10(rho * s->density_unit) - s->log_rho_eos_low) / s->drho_eos) + 1;
+  if (irho > s->neos_rho) irho = s->neos_rho;
+  if (irho < 1) irho = 1;
+  int irhop = irho + 1;
+  if (irhop > s->neos_rho) irhop = irho;
+  double eng = *eps / rho;
+  int ientry =
+      (int)((log10(eng) - log10(TAB(s->eng_table2, 1, irho))) / s->deng_eos_array[irho - 1]) + 1;
+  if (ientry > s->neos - 1) {
+    ientry = s->neos - 1;
+    eng = TAB(s->eng_table2, s->neos, irho);
+    *eps = eng * rho;
+  }
+  if (ientry < 1 || eng < TAB(s->eng_table2, 1, irho)) {
+    ientry = 1;
+    eng = TAB(s->eng_table2, 1, irho);
+    *eps = eng * rho;
+  }
+  const double *E = s->eng_table2;
+#define LIN(t, ir)                                                                        \
+  (TAB(t, ientry, ir) + (TAB(t, ientry + 1, ir) - TAB(t, ientry, ir)) /                  \
+                            (TAB(E, ientry + 1, ir) - TAB(E, ientry, ir)) *              \
+                            (eng - TAB(E, ientry, ir)))
+  *gam = LIN(s->gamma_table2, irho);
+  *m = LIN(s->muc_table2, irho);
+  *tk = LIN(s->tk_table2, irho);
+  if (!(s->rho_table[irho - 1] == s->rho_table[irhop - 1])) {
+    const double gamp = LIN(s->gamma_table2, irhop), mp = LIN(s->muc_table2, irhop),
+                 tkp = LIN(s->tk_table2, irhop);
+    const double slope =
+        ONE / (s->rho_table[irhop - 1] - s->rho_table[irho - 1]) * (rho - s->rho_table[irho - 1]);
+    *gam = *gam + (gamp - *gam) * slope;
+    *m = *m + (mp - *m) * slope;
+    *tk = *tk + (tkp - *tk) * slope;
+  }
+#undef LIN
+#undef TAB
+}
+
 void ox_state(ox_sim *s) {
   const double gam = s->P.gammafix, muc = s->P.muc, rgas = s->P.rgas, seps = s->P.small_eps;
   double *c = s->cons, *u = s->u, *p = s->p;
@@ -251,6 +326,29 @@ void ox_state(ox_sim *s) {
     double *ci = c + 5 * i, *ui = u + 3 * i;
     double ekin = ci[0] * HALF * (ui[0] * ui[0] + ui[1] * ui[1] + ui[2] * ui[2]);
     double eps = fmax_f(ci[4] - ekin, seps);
+    if (s->P.h2stat != -1) {
+      /* state.f90:60-79 */
+      double tk, m, gg;
+      if (s->P.nz == 1) {
+        const double x = s->P.dx * ((double)s->ix[i] - ((double)s->P.nx + ONE) / TWO);
+        const double y = s->P.dy * ((double)s->iy[i] - ((double)s->P.ny + ONE) / TWO);
+        const double hscale = sqrt((s->adindx[i] - ONE) * eps / (TWO * ekin) * (x * x + y * y));
+        eps = eps / (TWO * hscale);
+        const double rho = ci[0] / (TWO * hscale);
+        get_gamma2(s, &eps, rho, &tk, &m, &gg);
+      } else {
+        get_gamma2(s, &eps, ci[0], &tk, &m, &gg);
+      }
+      s->muc_array[i] = m;
+      s->adindx[i] = gg;
+      p[i] = (ci[0] * tk * rgas / s->muc_array[i]);
+      if (ci[0] < 1e-4) {
+        p[i] = rgas * s->tk_bgrnd / muc * ci[0];
+        eps = p[i] / (gam - ONE);
+        ci[4] = eps + ekin;
+      }
+      continue;
+    }
     s->adindx[i] = gam;
     s->muc_array[i] = muc;
     if (ci[0] < 1e-4) {

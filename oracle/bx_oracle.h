@@ -30,7 +30,7 @@ extern "C" {
 
 typedef struct ox_params {
   int32_t nx, ny, nz;
-  int32_t h2stat;          /* only -1 (fixed gamma) is supported */
+  int32_t h2stat;          /* -1 fixed gamma; >= 0 tables (ox_set_eos_table) */
   double dx, dy, dz;
   double cfl, small_rho, small_eps, vlimit, gammafix;
   double muc, rgas;        /* eos.f90:144 and units.f90:17 */
@@ -43,6 +43,17 @@ typedef struct ox_params {
 } ox_params;
 
 typedef struct ox_sim ox_sim;
+
+/* tables of the eos module for H2STAT >= 0 (eos.f90:30-51), energy index fastest */
+typedef struct ox_eos_table {
+  int32_t neos, neos_rho;
+  double log_rho_eos_low, drho_eos, density_unit, tk_bgrnd;
+  const double *eng_table2, *gamma_table2, *muc_table2, *tk_table2;
+  const double *rho_table, *deng_eos_array;
+} ox_eos_table;
+/* copies the tables; state() then follows state.f90:60-79 */
+void ox_set_eos_table(ox_sim *s, const ox_eos_table *t);
+void ox_get_muc(const ox_sim *s, double *muc);
 
 ox_sim *ox_create(const ox_params *p);
 void ox_destroy(ox_sim *s);

@@ -75,6 +75,8 @@ def lib():
         L.ox_run.restype = C.c_int64
         L.ox_set_threads.argtypes = [C.c_int]
         L.ox_rgas_code_units.restype = C.c_double
+        L.ox_set_eos_table.argtypes = [P, C.c_void_p]
+        L.ox_get_muc.argtypes = [P, C.c_void_p]
         L.ox_muc.restype = C.c_double
         L.ox_muc.argtypes = [C.c_double] * 4
         _lib = L
@@ -83,6 +85,17 @@ def lib():
 
 def _ptr(a):
     return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+class OxEosTable(C.Structure):
+    _fields_ = [
+        ("neos", C.c_int32), ("neos_rho", C.c_int32),
+        ("log_rho_eos_low", C.c_double), ("drho_eos", C.c_double),
+        ("density_unit", C.c_double), ("tk_bgrnd", C.c_double),
+        ("eng_table2", C.c_void_p), ("gamma_table2", C.c_void_p),
+        ("muc_table2", C.c_void_p), ("tk_table2", C.c_void_p),
+        ("rho_table", C.c_void_p), ("deng_eos_array", C.c_void_p),
+    ]
 
 
 class Oracle:
@@ -156,6 +169,26 @@ class Oracle:
         g[m, 1] = -(phi[nb[m, 0]] - phi[nb[m, 1]]) / (2.0 * P.dy)
         g[m, 2] = -(phi[nb[m, 4]] - phi[nb[m, 5]]) / (2.0 * P.dz)
         return g
+
+    def set_eos_table(self, tab):
+        """tab: dict of the eos module's tables (see boxzyhydro_b200.eos_table)."""
+        keep = {k: np.asfortranarray(tab[k], dtype=np.float64)
+                for k in ("eng_table2", "gamma_table2", "muc_table2", "tk_table2",
+                          "rho_table", "deng_eos_array")}
+        t = OxEosTable()
+        t.neos, t.neos_rho = int(tab["neos"]), int(tab["neos_rho"])
+        t.log_rho_eos_low = float(tab["log_rho_eos_low"])
+        t.drho_eos = float(tab["drho_eos"])
+        t.density_unit = float(tab["density_unit"])
+        t.tk_bgrnd = float(tab["tk_bgrnd"])
+        for k, a in keep.items():
+            setattr(t, k, a.ctypes.data)
+        lib().ox_set_eos_table(self._h, C.byref(t))
+
+    def muc_array(self):
+        m = np.empty(self.ng)
+        lib().ox_get_muc(self._h, _ptr(m))
+        return m
 
     def get_cons_old(self):
         c = np.empty((self.ng, 5))

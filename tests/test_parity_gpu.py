@@ -190,17 +190,17 @@ def test_upload_download_roundtrip_and_clock():
     assert not g.step(endtime=0.25)   # time >= endtime: the loop exits
 
 
-def test_unsupported_configurations_fail_loudly():
+def test_bad_configurations_fail_loudly():
     hp = small_random_box().params
-    hp.h2stat = 0
+    hp.h2stat = -2
     with pytest.raises(ValueError):
         Hydro(hp)
     from boxzyhydro_b200 import _lib
     import ctypes as C
     p = _lib.make_params(small_random_box().params)
-    p.h2stat = 0
+    p.h2stat = -2
     h = C.c_void_p()
-    assert _lib.lib().bx_create(C.byref(p), C.byref(h)) == 3
+    assert _lib.lib().bx_create(C.byref(p), C.byref(h)) == 1
     p.h2stat = -1
     p.nx = 3
     assert _lib.lib().bx_create(C.byref(p), C.byref(h)) == 1
