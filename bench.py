@@ -327,6 +327,8 @@ def adjoint_arm(args, rank, world, local):
         peak[0] = max(peak[0], t - f)
 
     eng = AdjointEngine(hp, args.steps, snaps)
+    if args.keep_stage0:
+        eng.keep_stage0(True)
     stream = torch.cuda.Stream()
     eng.set_stream(stream.cuda_stream)
     used()
@@ -389,7 +391,7 @@ def adjoint_arm(args, rank, world, local):
         "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"discrete adjoint, {n}^3 interior, gamma=5/3, {ic_name}, "
                                f"{args.steps} steps, loss 0.5||rho(T)-rho_target||^2",
-                   "snapshots": snaps},
+                   "snapshots": snaps, "keep_stage0": bool(args.keep_stage0)},
         "ms_forward": stats_fwd["ms_forward"], "ms_backward": stt["ms_backward"],
         "forward_cell_updates_per_s": hp.n_active() * args.steps / (stats_fwd["ms_forward"] * 1e-3),
         "recomputed_steps": stt["recomputed_steps"],
@@ -424,6 +426,7 @@ def main():
     ap.add_argument("--snapshots", type=int, default=15)
     ap.add_argument("--fd-dirs", type=int, default=16, dest="fd_dirs")
     ap.add_argument("--adj-ic", default="blob", choices=["blob", "turb"], dest="adj_ic")
+    ap.add_argument("--keep-stage0", action="store_true", dest="keep_stage0")
     ap.add_argument("--nbox", type=int, default=4096)
     ap.add_argument("--check-boxes", type=int, default=16, dest="check_boxes")
     ap.add_argument("--loop-sample", type=int, default=8, dest="loop_sample")

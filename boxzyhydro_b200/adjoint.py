@@ -45,6 +45,11 @@ class AdjointEngine:
         except Exception:
             pass
 
+    def keep_stage0(self, enable=True):
+        """Keep every step's stage-0 result from the next forward (memory for
+        speed: the backward then skips recomputing stage 0)."""
+        self._c(lib().bx_adj_keep_stage0(self._h, 1 if enable else 0))
+
     def set_stream(self, ptr):
         self._c(lib().bx_adj_set_stream(self._h, C.c_void_p(ptr) if ptr else None))
 

@@ -637,6 +637,10 @@ struct bx_adj {
   std::vector<int> chain_slot_of;  // per step index: pool slot holding it, or -1
   bool chain_valid = false;
   int chain_left = 0;
+  // optional: the stage-0 result C1 of every step, kept by the unfrozen forward
+  // so the backward skips its recomputation (nsteps state sets)
+  double* c1pool = nullptr;
+  bool c1_valid = false;
   // work planes
   double *W0 = nullptr, *W1 = nullptr, *W2 = nullptr;  // C0', C1, scratch state
   double* XT = nullptr;  // state after the last step of the forward run (C2_T)
@@ -757,15 +761,22 @@ static int rev_stage(bx_adj* A, int stage, const double* SA, const double* SB, c
 }
 
 // lam (adjoint of the step output, C2) -> lam (adjoint of the step input X)
-static int rev_step(bx_adj* A, const double* X, int nsrc, double dt, double* lam) {
+static int rev_step(bx_adj* A, const double* X, long long k, double* lam) {
   bx_handle* h = A->h;
   const Geom& g = h->g;
   cudaStream_t s = h->stream;
-  // recompute C0' and C1
+  const int nsrc = A->step_nsrc[k];
+  const double dt = A->dts[k];
+  // C0' and C1 of step k (C1 kept by the forward run, or recomputed)
   k_adj_src<<<ablk(g.ng), AB, 0, s>>>(g, X, nsrc, A->W0);
-  if (int r = fwd_step(A, X, nsrc, dt, nullptr, true)) return r;  // W1 <- C1
+  const double* C1 = A->W1;
+  if (A->c1pool && A->c1_valid) {
+    C1 = A->c1pool + k * 5 * g.ng;
+  } else {
+    if (int r = fwd_step(A, X, nsrc, dt, nullptr, true)) return r;  // W1 <- C1
+  }
   // stage 1 reads lam/2; writes lamC1 (adjoint of C1) and lamA (of C0')
-  if (int r = rev_stage(A, 1, A->W1, A->W0, lam, kHalf, dt, lam, A->lamC1, A->lamA, X, nsrc))
+  if (int r = rev_stage(A, 1, C1, A->W0, lam, kHalf, dt, lam, A->lamC1, A->lamA, X, nsrc))
     return r;
   // stage 0 reads lamC1; lam <- adjoint of X through the sources
   if (int r = rev_stage(A, 0, A->W0, A->W0, A->lamC1, 1.0, dt, A->lamA, lam, nullptr, X, nsrc))
@@ -830,13 +841,13 @@ static int reverse_range(bx_adj* A, const double* Xa, long long a, long long b, 
                          bool chain) {
   const long long l = b - a;
   if (l <= 0) return BX_OK;
-  if (l == 1) return rev_step(A, Xa, A->step_nsrc[a], A->dts[a], lam);
+  if (l == 1) return rev_step(A, Xa, a, lam);
   const int s = (int)A->pool_free.size() + (chain ? A->chain_left : 0);
   if (s == 0) {
     // no snapshot left: rebuild each state from Xa (into lamB, free during reversal)
     for (long long k = b - 1; k >= a; --k) {
       if (int r = advance(A, Xa, a, k, A->lamB)) return r;
-      if (int r = rev_step(A, A->lamB, A->step_nsrc[k], A->dts[k], lam)) return r;
+      if (int r = rev_step(A, A->lamB, k, lam)) return r;
     }
     return BX_OK;
   }
@@ -867,6 +878,7 @@ int bx_adj_destroy(bx_adj* A) {
   double* ps[] = {A->W0, A->W1, A->W2, A->XT, A->lamA, A->lamB, A->lamC1,
                   A->P,  A->PA, A->d_dts};
   for (double* p : ps) cudaFree(p);
+  cudaFree(A->c1pool);
   if (A->h) bx_destroy(A->h);
   delete A;
   return BX_OK;
@@ -927,6 +939,25 @@ int bx_adj_create(const bx_params* params, int64_t nsteps, int32_t snapshots, bx
   return BX_OK;
 }
 
+int bx_adj_keep_stage0(bx_adj* A, int32_t enable) {
+  if (!A) return aerr(A, BX_ERR_ARG, "bad arguments");
+  if (enable && !A->c1pool) {
+    const size_t bytes = (size_t)A->nsteps * 5 * A->ng * sizeof(double);
+    if (cudaMalloc(&A->c1pool, bytes) != cudaSuccess) {
+      cudaGetLastError();
+      A->c1pool = nullptr;
+      return aerr(A, BX_ERR_NOMEM, "no room for the stage-0 results of every step");
+    }
+    A->bytes += bytes;
+  } else if (!enable && A->c1pool) {
+    cudaFree(A->c1pool);
+    A->c1pool = nullptr;
+    A->bytes -= (size_t)A->nsteps * 5 * A->ng * sizeof(double);
+  }
+  A->c1_valid = false;  // filled by the next unfrozen forward run
+  return BX_OK;
+}
+
 int bx_adj_set_stream(bx_adj* A, void* s) {
   if (!A) return BX_ERR_ARG;
   return bx_set_stream(A->h, s);
@@ -977,9 +1008,9 @@ int bx_adj_forward(bx_adj* A, const double* cons0, double* consT, int32_t frozen
       k_record_dt<<<1, 1, 0, s>>>(h->d_ctrl, A->d_dts, k);
     }
     a.X = cur;
-    a.out = A->W1;
+    a.out = (!frozen && A->c1pool) ? A->c1pool + k * n5 : A->W1;
     ACK(launch_stage(0, g.pow2 ? 1 : 0, g.threed != 0, a, h->ntiles, s));
-    a.Y = A->W1;
+    a.Y = a.out;
     a.out = out;
     ACK(launch_stage(1, g.pow2 ? 1 : 0, g.threed != 0, a, h->ntiles, s));
     if (!frozen) ACK(launch_end(h->d_ctrl, 1, s));
@@ -1010,6 +1041,7 @@ int bx_adj_forward(bx_adj* A, const double* cons0, double* consT, int32_t frozen
   if (!frozen) {
     A->have_forward = true;
     A->chain_valid = true;
+    A->c1_valid = A->c1pool != nullptr;
   }
   return BX_OK;
 }

@@ -230,6 +230,10 @@ typedef struct bx_adj bx_adj;
 int bx_adj_create(const bx_params *params, int64_t nsteps, int32_t snapshots, bx_adj **out);
 int bx_adj_destroy(bx_adj *a);
 int bx_adj_set_stream(bx_adj *a, void *cuda_stream);
+/* enable != 0: the next unfrozen forward keeps the stage-0 result of every step
+ * (nsteps x 5 x ngrid doubles more), and backward passes use them instead of
+ * recomputing stage 0 of each step; BX_ERR_NOMEM if they do not fit. */
+int bx_adj_keep_stage0(bx_adj *a, int32_t enable);
 /* frozen=0: dt by the CFL rule (main.f90:266-281) and recorded; frozen=1: the recorded
  * dt sequence (for finite differences).  BX_ERR_STATE if a guard fired. */
 int bx_adj_forward(bx_adj *a, const double *cons0, double *consT, int32_t frozen);

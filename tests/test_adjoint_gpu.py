@@ -138,6 +138,22 @@ def test_checkpoint_schedules_agree():
         eng.close()
 
 
+def test_kept_stage0_results_give_the_same_gradient():
+    st, eng = setup(nsteps=5, snaps=2)
+    hp = st.params
+    fwd(eng, st.cons, frozen=False)
+    rng = np.random.default_rng(5)
+    lamT = rand_dir(hp, rng, np.ones(5))
+    ref = bwd(eng, lamT)
+    r0 = eng.stats()["recomputed_steps"]
+    eng.keep_stage0(True)
+    fwd(eng, st.cons, frozen=False)
+    got = bwd(eng, lamT)
+    assert np.array_equal(got, ref)
+    assert eng.stats()["recomputed_steps"] == r0
+    eng.close()
+
+
 def test_torch_autograd_function():
     torch = _torch()
     st, eng = setup()
