@@ -72,6 +72,7 @@ def lib():
         "bx_set_stream": (C.c_int, [H, vp]),
         "bx_upload": (C.c_int, [H, vp, vp, vp]),
         "bx_download": (C.c_int, [H, vp, vp, vp]),
+        "bx_upload_conserved": (C.c_int, [H, vp]),
         "bx_set_clock": (C.c_int, [H, C.c_double, C.c_double, C.c_int64]),
         "bx_get_clock": (C.c_int, [H, dp, dp, dp, i64p]),
         "bx_step": (C.c_int, [H, C.c_double, i32p]),

@@ -259,10 +259,8 @@ static int ensure_states(bx_handle* h) {
 
 static int bx_adindx_fill(bx_handle* h) {
   // adindx(:) = gammafix, as state() sets it (state.f90:50)
-  std::vector<double> gam(h->g.ng, h->P.gammafix);
-  CK(cudaMemcpyAsync(h->pa.adindx, gam.data(), h->g.ng * sizeof(double), cudaMemcpyHostToDevice,
-                     h->stream));
-  CK(cudaStreamSynchronize(h->stream));
+  CK(fill_const(h->pa.adindx, h->g.ng, h->P.gammafix, h->stream));
+  h->launches += 1;
   return BX_OK;
 }
 
@@ -315,6 +313,34 @@ int bx_upload(bx_handle* h, const double* cons, const double* u, const double* p
       // adindx = gammafix is what state() leaves; set it like the other path does
       return enter_fused(h);
     }
+  }
+  return bx_adindx_fill(h);
+}
+
+int bx_upload_conserved(bx_handle* h, const double* cons) {
+  CHECK_H();
+  if (!cons) return set_err(h, BX_ERR_ARG, "cons is required");
+  if (h->g.tab) return set_err(h, BX_ERR_STATE, "H2STAT >= 0: upload u and p with bx_upload");
+  const long long n = h->g.ng;
+  cudaStream_t s = h->stream;
+  double* tmp = staging(h);
+  CK(cudaMemcpyAsync(tmp, cons, 5 * n * sizeof(double), cudaMemcpyHostToDevice, s));
+  CK(aos_to_soa(tmp, h->pa.cons, n, 5, s));
+  // u = m/rho (velocity() ran last) and p of state() with that u
+  CK(prims_from_cons(h->g, h->pa, s));
+  h->launches += 2;
+  h->mode = 0;
+  if (h->eligible && !h->gforce_set) {
+    if (int r = pull_clock(h)) return r;
+    h->clock.flags = 0;
+    if (int r = push_clock(h)) return r;
+    CK(check_clean(h->g, h->pa, h->nghost, h->d_dst, h->d_src2, h->d_sgn2, h->d_ctrl, s));
+    h->launches += 2;
+    if (int r = pull_clock(h)) return r;
+    const bool clean = !(h->clock.flags & kFlagNotClean);
+    h->clock.flags = 0;
+    if (int r = push_clock(h)) return r;
+    if (clean) return enter_fused(h);
   }
   return bx_adindx_fill(h);
 }

@@ -185,6 +185,8 @@ cudaError_t check_clean(const Geom& g, const PhaseArrays& a, int nghost, const i
 
 // AoS host layout <-> SoA device layout
 cudaError_t aos_to_soa(const double* aos, double* soa, long long n, int k, cudaStream_t s);
+cudaError_t prims_from_cons(const Geom& g, PhaseArrays& a, cudaStream_t s);
+cudaError_t fill_const(double* a, long long n, double v, cudaStream_t s);
 cudaError_t soa_to_aos(const double* soa, double* aos, long long n, int k, cudaStream_t s);
 
 }  // namespace bx

@@ -1157,6 +1157,21 @@ cudaError_t fused_to_phase(const Geom& g, const double* X, int nsrc, PhaseArrays
   k_f2p_prims<<<nblk(g.ng), PB, 0, s>>>(g, a);
   return cudaGetLastError();
 }
+__global__ void k_fill_const(double* a, long long n, double v) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i < n) a[i] = v;
+}
+cudaError_t fill_const(double* a, long long n, double v, cudaStream_t s) {
+  k_fill_const<<<nblk(n), PB, 0, s>>>(a, n, v);
+  return cudaGetLastError();
+}
+
+// velocity and pressure arrays from the conserved variables alone
+cudaError_t prims_from_cons(const Geom& g, PhaseArrays& a, cudaStream_t s) {
+  k_f2p_prims<<<nblk(g.ng), PB, 0, s>>>(g, a);
+  return cudaGetLastError();
+}
+
 // the reference cons only (no primitives) of the fused state X into cons
 cudaError_t fused_to_cons(const Geom& g, const double* X, int nsrc, double* cons, int nghost,
                           const int32_t* dst, const int32_t* src2, const uint8_t* sgn2,

@@ -69,6 +69,11 @@ class Hydro:
         ptr = lambda a: None if a is None else a.ctypes.data_as(C.c_void_p)
         self._c(lib().bx_upload(self._h, ptr(c), ptr(uu), ptr(pp)))
 
+    def upload_conserved(self, cons):
+        """State at a step boundary from cons alone (u = m/rho, p from state())."""
+        c = _arr(cons, self.ng, 5)
+        self._c(lib().bx_upload_conserved(self._h, c.ctypes.data_as(C.c_void_p)))
+
     def upload_state(self, st):
         self.upload(st.cons, st.u, st.p)
 

@@ -204,3 +204,23 @@ def test_bad_configurations_fail_loudly():
     p.h2stat = -1
     p.nx = 3
     assert _lib.lib().bx_create(C.byref(p), C.byref(h)) == 1
+
+
+def test_upload_conserved_continues_bit_for_bit():
+    """A step-boundary state given by cons alone (u = m/rho, p from state())
+    continues exactly like the handle it came from."""
+    st = small_random_box(nx=20, ny=14, nz=12, walls=(0,) * 6, seed=12)
+    o, g = make_pair(st)
+    step_both(o, g, 2)
+    c, u, p = g.download()
+    g2 = Hydro(st.params)
+    g2.upload_conserved(c)
+    clk = g.clock()
+    g2.set_clock(time=clk["time"], dtold=clk["dtold"], step=clk["step"])
+    c2, u2, p2 = g2.download()
+    assert np.array_equal(c2, c) and np.array_equal(u2, u) and np.array_equal(p2, p)
+    for _ in range(3):
+        g.step()
+        g2.step()
+    assert g2.status()[1] == 1
+    assert np.array_equal(g.download()[0], g2.download()[0])
