@@ -191,7 +191,7 @@ __device__ __forceinline__ void cons_vjp(const Geom& g, int stage, const double*
 // barrier-separated phases of different blocks overlap.
 struct RShape {
   int NL, W, NQ, NS, NF, ND, nseg, threads;
-  size_t r1, r2, r3, smem;  // region sizes in doubles; smem in bytes
+  size_t r1, r2, r3, r4, smem;  // region sizes in doubles; smem in bytes
 };
 
 static RShape rshape(int Lc, int wmax, int target) {
@@ -204,9 +204,19 @@ static RShape rshape(int Lc, int wmax, int target) {
   r.r1 = (size_t)std::max(7 * r.NQ + 5 * r.NS, 13 * r.ND) * r.NL;
   r.r2 = (size_t)21 * r.NS * r.NL;
   r.r3 = (size_t)12 * r.NF * r.NL;
-  r.smem = (r.r1 + r.r2 + r.r3) * sizeof(double) + (size_t)r.NS * r.NL * sizeof(int);
+  r.r4 = (size_t)7 * r.W * r.NL;  // PA of the segment, fetched while the block computes
+  r.smem = (r.r1 + r.r2 + r.r3 + r.r4) * sizeof(double) + (size_t)r.NS * r.NL * sizeof(int);
   return r;
 }
+
+// asynchronous global -> shared copies (cp.async): the segment's PA values are
+// in flight while the block forms states and face derivatives
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
 template <int DIR>
 __device__ __forceinline__ int rsx(int l, int j, int M, int NL) {
@@ -222,7 +232,8 @@ k_rdir(Geom g, const double* P, const double* lamL, double lscale, double dt, do
   double* r1 = sm;
   double* r2 = sm + sh.r1;
   double* r3 = r2 + sh.r2;
-  int* sel_s = reinterpret_cast<int*>(r3 + sh.r3);
+  double* pa_s = r3 + sh.r3;  // [7][NL*W]
+  int* sel_s = reinterpret_cast<int*>(pa_s + sh.r4);
   double* lm_s = r1 + 7 * NL * NQ;  // lives in r1 beside the primitives until P4
   const long long n = g.ng;
   const int zlo = g.threed ? g.az0 : 0, zhi = g.threed ? g.az1 : g.nz;
@@ -248,6 +259,18 @@ k_rdir(Geom g, const double* P, const double* lamL, double lscale, double dt, do
   };
   auto valid = [&](int c) { return c >= lo - 1 && c <= hi; };
   auto inner = [&](int c) { return c >= lo && c < hi; };
+
+  // P0: start fetching PA of the segment's cells (used in P5)
+  for (int t = threadIdx.x; t < NL * W; t += blockDim.x) {
+    const int l = DIR == 0 ? t / W : t % NL, j = DIR == 0 ? t % W : t / NL;
+    const int c = s0 + j;
+    bool ok;
+    const long long b = line_base(l, ok);
+    if (!(ok && valid(c))) continue;
+    const long long i = b + c * st;
+    for (int q = 0; q < 7; ++q) cp_async8(pa_s + q * NL * W + t, PA + q * n + i);
+  }
+  cp_async_commit();
 
   // P1: primitives
   for (int t = threadIdx.x; t < NL * NQ; t += blockDim.x) {
@@ -390,6 +413,8 @@ k_rdir(Geom g, const double* P, const double* lamL, double lscale, double dt, do
   }
   __syncthreads();
   // P5: gather and accumulate
+  cp_async_wait_all();
+  __syncthreads();
   for (int t = threadIdx.x; t < NL * W; t += blockDim.x) {
     const int l = DIR == 0 ? t / W : t % NL, j = DIR == 0 ? t % W : t / NL;
     const int c = s0 + j;
@@ -416,7 +441,7 @@ k_rdir(Geom g, const double* P, const double* lamL, double lscale, double dt, do
     }
     const long long i = b + c * st;
 #pragma unroll
-    for (int q = 0; q < 7; ++q) PA[q * n + i] += acc[q];
+    for (int q = 0; q < 7; ++q) PA[q * n + i] = pa_s[q * NL * W + t] + acc[q];
   }
 }
 
