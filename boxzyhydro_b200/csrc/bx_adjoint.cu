@@ -489,11 +489,26 @@ __device__ __noinline__ void ghost_fold(const Geom& g, const double* SA, const d
 template <int STAGE>
 __global__ void k_rcell(Geom g, const double* SA, const double* SB, const double* P,
                         const double* PA, const double* lin, double* o1, double* o2,
-                        const double* X, int nsrc) {
-  const int x = g.ax0 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int y = g.ay0 + blockIdx.y;
-  const int z = (g.threed ? g.az0 : 0) + blockIdx.z;
-  if (x >= g.ax1) return;
+                        const double* X, int nsrc, int xedge) {
+  // xedge = 0: the columns between the two x-edge columns (every warp takes the
+  // ghost path together or not at all); xedge = 1: the two x-edge columns
+  int x, y, z;
+  if (xedge) {
+    // one thread per x-edge cell: t = side + 2 (y + nyi z)
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int nyi = g.ay1 - g.ay0, nzi = g.threed ? g.az1 - g.az0 : g.nz;
+    if (t >= 2ll * nyi * nzi) return;
+    const int side = (int)(t & 1);
+    if (side == 1 && g.ax1 - 1 == g.ax0) return;
+    x = side ? g.ax1 - 1 : g.ax0;
+    y = g.ay0 + (int)((t >> 1) % nyi);
+    z = (g.threed ? g.az0 : 0) + (int)((t >> 1) / nyi);
+  } else {
+    x = g.ax0 + 1 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (x >= g.ax1 - 1) return;
+    y = g.ay0 + blockIdx.y;
+    z = (g.threed ? g.az0 : 0) + blockIdx.z;
+  }
   const long long i = x + (long long)y * g.sy + (long long)z * g.sz;
   const long long n = g.ng;
   double gq[7], a[10], gA[5], gB[5];
@@ -770,17 +785,22 @@ static int rev_stage(bx_adj* A, int stage, const double* SA, const double* SB, c
   const dim3 pgrid((unsigned)((g.nx + tp - 1) / tp), (unsigned)g.ny, (unsigned)g.nz);
   k_r1_prims<<<pgrid, tp, 0, s>>>(g, stage, SA, SB, A->P);
   // interior cells
-  const int nxi = g.ax1 - g.ax0, tc = std::min(256, ((nxi + 31) / 32) * 32);
-  const dim3 cgrid((unsigned)((nxi + tc - 1) / tc), (unsigned)(g.ay1 - g.ay0),
+  const int nxm = std::max(1, g.ax1 - g.ax0 - 2), tc = std::min(256, ((nxm + 31) / 32) * 32);
+  const dim3 cgrid((unsigned)((nxm + tc - 1) / tc), (unsigned)(g.ay1 - g.ay0),
                    (unsigned)(g.threed ? g.az1 - g.az0 : g.nz));
+  const long long nedge = 2ll * cgrid.y * cgrid.z;
+  const dim3 egrid((unsigned)((nedge + 127) / 128));
   ACK(cudaMemsetAsync(A->PA, 0, 7 * n * sizeof(double), s));
   ACK(launch_rdir<0>(g, A->P, lamL, lscale, dt, A->PA, s));
   ACK(launch_rdir<1>(g, A->P, lamL, lscale, dt, A->PA, s));
   if (g.threed) ACK(launch_rdir<2>(g, A->P, lamL, lscale, dt, A->PA, s));
-  if (stage == 1)
-    k_rcell<1><<<cgrid, tc, 0, s>>>(g, SA, SB, A->P, A->PA, lin, o1, o2, X, nsrc);
-  else
-    k_rcell<0><<<cgrid, tc, 0, s>>>(g, SA, SB, A->P, A->PA, lin, o1, o2, X, nsrc);
+  if (stage == 1) {
+    k_rcell<1><<<cgrid, tc, 0, s>>>(g, SA, SB, A->P, A->PA, lin, o1, o2, X, nsrc, 0);
+    k_rcell<1><<<egrid, 128, 0, s>>>(g, SA, SB, A->P, A->PA, lin, o1, o2, X, nsrc, 1);
+  } else {
+    k_rcell<0><<<cgrid, tc, 0, s>>>(g, SA, SB, A->P, A->PA, lin, o1, o2, X, nsrc, 0);
+    k_rcell<0><<<egrid, 128, 0, s>>>(g, SA, SB, A->P, A->PA, lin, o1, o2, X, nsrc, 1);
+  }
   ACK(cudaGetLastError());
   return BX_OK;
 }
