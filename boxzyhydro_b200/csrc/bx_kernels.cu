@@ -129,7 +129,11 @@ constexpr int NSX = TY * (TX + 2);    // x-state cells
 constexpr int NSY = (TY + 2) * TX;    // y-state cells
 constexpr int NFX = TY * (TX + 1);    // x faces
 constexpr int NFY = (TY + 1) * TX;    // y faces
-constexpr int SMEM_DOUBLES = 7 * NP + 12 * NSX + 12 * NSY;
+// per-thread z-pipeline slots (3-D): the z flux below and above the own cell
+// (5 + 5) and the plus z-state carried to the next plane (6), kept in shared
+// memory so the x/y phases have the registers
+constexpr int NZS = 16;
+constexpr int SMEM_DOUBLES = 7 * NP + 12 * NSX + 12 * NSY + NZS * NT;
 static_assert(5 * NFX + 5 * NFY <= 7 * NP, "face fluxes alias the primitive plane");
 
 __device__ __forceinline__ void put_prim(double* SP, int i, const Prim& q) {
@@ -195,6 +199,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
   double* SY = SX + 12 * NSX;         // [12][TY+2][TX] y states
   double* FX = sm;                    // [5][TY][TX+1] x face fluxes (aliases SP)
   double* FY = sm + 5 * NFX;          // [5][TY+1][TX] y face fluxes
+  double* ZS = SY + 12 * NSY;         // [16][NT]: Fzm 0-4, Fzp 5-9, plus state 10-15
   const double dt = C->dt;
   const int nsrc = a.nsrc > 0 ? a.nsrc : C->nsrc;
 
@@ -216,8 +221,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
 
   // z pipeline of the own column (3-D grids)
   Prim Pk, Pk1;
-  FaceState plusk;
-  double Fzm[5];
+  auto zs = [&](int k) -> double& { return ZS[k * NT + threadIdx.x]; };
 
   const int z0 = g.az0 + t.z0, z1 = g.az0 + t.z1;
   if (THREED && own) {
@@ -231,15 +235,19 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
     } else {
       dir_states<POW2>(Pm2, Pm1, Pk, Pm1.u3, dt, g.dz, idz, mm, pm);
     }
+    FaceState plusk;
+    double Fzm[5];
     dir_states<POW2>(Pm1, Pk, Pk1, Pk.u3, dt, g.dz, idz, m0, plusk);
     hll_flux<2>(pm, m0, g.gam, Fzm);
+    for (int q = 0; q < 5; ++q) zs(q) = Fzm[q];
+    zs(10) = plusk.d; zs(11) = plusk.u1; zs(12) = plusk.u2; zs(13) = plusk.u3;
+    zs(14) = plusk.p; zs(15) = plusk.e;
   }
 
   for (int z = (THREED ? z0 : g.az0 + t.z0); z < (THREED ? z1 : g.az0 + t.z1); ++z) {
     // ---- A: primitives of plane z (own from the pipeline, halo computed here)
     Prim P2;
     FaceState mz1, pz1;
-    double Fzp[5];
     if (own) {
       if (THREED) {
         P2 = load_prim<STAGE>(a, g, gx, gy, z + 2, flags, nsrc);
@@ -274,7 +282,12 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
       } else {
         dir_states<POW2>(Pk, Pk1, P2, Pk1.u3, dt, g.dz, idz, mz1, pz1);
       }
+      const FaceState plusk{zs(10), zs(11), zs(12), zs(13), zs(14), zs(15)};
+      double Fzp[5];
       hll_flux<2>(plusk, mz1, g.gam, Fzp);
+      for (int q = 0; q < 5; ++q) zs(5 + q) = Fzp[q];
+      zs(10) = pz1.d; zs(11) = pz1.u1; zs(12) = pz1.u2; zs(13) = pz1.u3;
+      zs(14) = pz1.p; zs(15) = pz1.e;
     }
     __syncthreads();
 
@@ -347,7 +360,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         const double dfx = FX[q * NFX + ty * (TX + 1) + tx + 1] - FX[q * NFX + ty * (TX + 1) + tx];
         const double dfy = FY[q * NFY + (ty + 1) * TX + tx] - FY[q * NFY + ty * TX + tx];
         double sum = g.ayz * dfx + g.axz * dfy;
-        if (THREED) sum = sum + g.axy * (Fzp[q] - Fzm[q]);
+        if (THREED) sum = sum + g.axy * (zs(5 + q) - zs(q));
         ft[q] = POW2 ? -sum * dt * g.ivol : cdiv(-sum * dt, g.vol, g.ivol);
       }
       Cons c0 = load_cons(a.X, PS, g, gx, gy, z);
@@ -390,8 +403,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
       for (int q = 0; q < 5; ++q) a.out[q * PS + o] = n[q];
       if (THREED) {
 #pragma unroll
-        for (int q = 0; q < 5; ++q) Fzm[q] = Fzp[q];
-        plusk = pz1;
+        for (int q = 0; q < 5; ++q) zs(q) = zs(5 + q);
         Pk = Pk1;
         Pk1 = P2;
       }
