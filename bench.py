@@ -129,6 +129,23 @@ def cpu_sample(st, steps=3, threads=None):
     return cells * steps / dt, threads, dt
 
 
+def max_over_ranks(ms, world, device=None):
+    """The slowest rank's time (the timing rule for N > 1: every rank takes its
+    device time between barriers, the job's time is the maximum)."""
+    if world <= 1:
+        return float(ms)
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def weak_value(world, units_per_rank, steps, ms):
+    """Whole-job throughput of N replicas: units of all ranks / the job's time."""
+    return world * units_per_rank * steps / (ms * 1e-3)
+
+
 def reference_arm(args, rank):
     if rank != 0:
         return 0
@@ -183,6 +200,12 @@ def batched_arm(args, rank, world, local):
     from boxzyhydro_b200.hydro import Hydro
 
     torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    # each rank advances an ensemble of its own (seeded by rank): replicas
     spec = ic.riemann_ensemble_spec(nbox=args.nbox, seed=args.seed + rank)
     free, _ = torch.cuda.mem_get_info()
     budget = 0.80 * free
@@ -230,7 +253,8 @@ def batched_arm(args, rank, world, local):
             maxdiff = max(maxdiff, d)
             checked += 1
         b.close()
-    value = args.nbox * args.steps / (total_ms * 1e-3)
+    total_ms = max_over_ranks(total_ms, world, "cuda")
+    value = weak_value(world, args.nbox, args.steps, total_ms)
 
     # single-grid path looped over a stratified sample, extrapolated by size
     sizes = sorted({s["side"] for s in spec})
@@ -253,8 +277,8 @@ def batched_arm(args, rank, world, local):
             ms_list.append(e0.elapsed_time(e1))
             h.close()
         per_size_ms[side] = sum(ms_list) / len(ms_list)
-    loop_ms = sum(per_size_ms[s["side"]] for s in spec)
-    loop_value = args.nbox * args.steps / (loop_ms * 1e-3)
+    loop_ms = max_over_ranks(sum(per_size_ms[s["side"]] for s in spec), world, "cuda")
+    loop_value = weak_value(world, args.nbox, args.steps, loop_ms)
     cells = sum(s["side"] ** 3 for s in spec)
     line = {
         "metric": "batched boxes/s", "value": value, "unit": "box-steps/s", "n_gpus": world,
@@ -266,7 +290,7 @@ def batched_arm(args, rank, world, local):
                                "random split axis, gamma in {1.4,5/3}, CFL 0.1, outflow walls, "
                                f"{args.steps} steps after {args.warmup} warm-up",
                    "interior_cells": cells, "chunks": len(chunks),
-                   "cell_updates_per_s": cells * args.steps / (total_ms * 1e-3)},
+                   "cell_updates_per_s": weak_value(world, cells, args.steps, total_ms)},
         "loop_single_grid": {"value": loop_value, "unit": "box-steps/s",
                              "ms_per_box_run_by_side": per_size_ms,
                              "sample_per_side": args.loop_sample},
@@ -278,6 +302,8 @@ def batched_arm(args, rank, world, local):
     }
     if rank == 0:
         print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
     return 0
 
 
@@ -297,6 +323,8 @@ def adjoint_arm(args, rank, world, local):
     from boxzyhydro_b200 import ic
     from boxzyhydro_b200.adjoint import AdjointEngine
 
+    if rank != 0:
+        return 0  # one GPU: the adjoint runs on rank 0 only
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     n = args.n
@@ -487,14 +515,10 @@ def main():
     torch.cuda.synchronize()
     clocks = sampler.stop()
     barrier()
-    ms = e0.elapsed_time(e1)
-    if world > 1:
-        t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(e0.elapsed_time(e1), world, "cuda")
     prof = g.profile_read()
     bits, path = g.status()
-    value = world * cells * args.steps / (ms * 1e-3)
+    value = weak_value(world, cells, args.steps, ms)
 
     # ---- roofline of the dominant stage kernel
     hbm, hbm_src = measured_hbm()
@@ -562,12 +586,7 @@ def main():
                 body()
             a1.record(stream)
             a1.synchronize()
-            ms = a0.elapsed_time(a1)
-            if world > 1:
-                t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-                dist.all_reduce(t, op=dist.ReduceOp.MAX)
-                ms = float(t.item())
-            return ms
+            return max_over_ranks(a0.elapsed_time(a1), world, "cuda")
 
         def cons_only():
             g._c(L.bx_upload_conserved(g._h, hc.ctypes.data))
@@ -582,12 +601,12 @@ def main():
         ems = timed(cons_only, args.e2e_steps)
         fms = timed(full_arrays, max(2, args.e2e_steps // 2))
         nfull = max(2, args.e2e_steps // 2)
-        e2e = {"value": world * cells * args.e2e_steps / (ems * 1e-3), "unit": UNIT,
+        e2e = {"value": weak_value(world, cells, args.e2e_steps, ems), "unit": UNIT,
                "h2d_bytes_per_step": ng * 5 * 8, "d2h_bytes_per_step": ng * 5 * 8,
                "steps": args.e2e_steps, "ms_per_step": ems / args.e2e_steps,
                "api": "bx_upload_conserved(cons) + bx_step + bx_download(cons), pinned host",
                "reference_arrays": {
-                   "value": world * cells * nfull / (fms * 1e-3), "unit": UNIT,
+                   "value": weak_value(world, cells, nfull, fms), "unit": UNIT,
                    "h2d_bytes_per_step": ng * 9 * 8, "d2h_bytes_per_step": ng * 9 * 8,
                    "steps": nfull, "ms_per_step": fms / nfull,
                    "api": "bx_upload(cons,u,p) + bx_step + bx_download(cons,u,p), pinned host"}}
