@@ -174,11 +174,6 @@ __device__ __forceinline__ FaceState get_fs(const double* S, int n, int i) {
   f.e = S[5 * n + i];
   return f;
 }
-__device__ __forceinline__ FaceState as_face(const Prim& q) {
-  FaceState f;
-  f.d = q.d; f.u1 = q.u1; f.u2 = q.u2; f.u3 = q.u3; f.p = q.p; f.e = q.e;
-  return f;
-}
 
 __device__ __forceinline__ double warp_max(double v) {
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
