@@ -119,12 +119,16 @@ __global__ void k_r1_prims(Geom g, int stage, const double* A, const double* B, 
 // returns the adjoints of A's (gA) and, for stage 1, B's (gB) conserved values
 // at that location.  Branches (the eps floors) are taken as the forward took
 // them: eps > small_eps exactly when the floor did not fire.
-__device__ __forceinline__ void cons_vjp(const Geom& g, int stage, const double* P, long long pi,
-                                         const double* A, const double* B, int x, int y, int z,
-                                         const double gq[7], double gA[5], double gB[5]) {
-  const long long n = g.ng;
-  const double rho = P[pi], u[3] = {P[n + pi], P[2 * n + pi], P[3 * n + pi]};
-  const double p = P[4 * n + pi], e = P[5 * n + pi], cs = P[6 * n + pi];
+// the values the VJP reads: the cell's primitives, and for stage 1 A's energy
+// and B's density and momenta at the location (through the donor rule)
+struct CvIn {
+  double rho, u[3], p, e, cs, aE, bd, bm[3];
+};
+
+__device__ __forceinline__ void cons_vjp_v(const Geom& g, int stage, const CvIn& v,
+                                           const double gq[7], double gA[5], double gB[5]) {
+  const double rho = v.rho, u[3] = {v.u[0], v.u[1], v.u[2]};
+  const double p = v.p, e = v.e, cs = v.cs;
   const double ir = 1.0 / rho;
   for (int q = 0; q < 5; ++q) gA[q] = gB[q] = 0.0;
   double grho = gq[0], gu[3] = {gq[1], gq[2], gq[3]}, gp = gq[4], ge = gq[5];
@@ -138,12 +142,10 @@ __device__ __forceinline__ void cons_vjp(const Geom& g, int stage, const double*
     ge += gp * g.gm1;
   } else {
     // p = max(E - rho K(u*)/2, eps)(gam-1) with u* = m/rho of B (main.f90:351-355)
-    const C5 a = aload(A, n, g, x, y, z);
-    const C5 b = aload(B, n, g, x, y, z);
-    const double us[3] = {b.m1 / b.d, b.m2 / b.d, b.m3 / b.d};
+    const double us[3] = {v.bm[0] / v.bd, v.bm[1] / v.bd, v.bm[2] / v.bd};
     const double Ks = us[0] * us[0] + us[1] * us[1] + us[2] * us[2];
-    if (a.E - rho * kHalf * Ks > g.small_eps) {
-      const double gpg = gp * g.gm1, ib = 1.0 / b.d;
+    if (v.aE - rho * kHalf * Ks > g.small_eps) {
+      const double gpg = gp * g.gm1, ib = 1.0 / v.bd;
       gA[4] += gpg;
       grho = fma(gpg, -kHalf * Ks, grho);
       for (int j = 0; j < 3; ++j) {
@@ -165,6 +167,25 @@ __device__ __forceinline__ void cons_vjp(const Geom& g, int stage, const double*
     grho = fma(-t, u[j], grho);
   }
   gA[0] += grho;
+}
+
+// the same at (x,y,z) with the values read from memory (P at index pi)
+__device__ __forceinline__ void cons_vjp(const Geom& g, int stage, const double* P, long long pi,
+                                         const double* A, const double* B, int x, int y, int z,
+                                         const double gq[7], double gA[5], double gB[5]) {
+  const long long n = g.ng;
+  CvIn v;
+  v.rho = P[pi];
+  v.u[0] = P[n + pi]; v.u[1] = P[2 * n + pi]; v.u[2] = P[3 * n + pi];
+  v.p = P[4 * n + pi]; v.e = P[5 * n + pi]; v.cs = P[6 * n + pi];
+  v.aE = 0.0; v.bd = 1.0; v.bm[0] = v.bm[1] = v.bm[2] = 0.0;
+  if (stage == 1) {
+    const C5 a = aload(A, n, g, x, y, z);
+    const C5 b = aload(B, n, g, x, y, z);
+    v.aE = a.E;
+    v.bd = b.d; v.bm[0] = b.m1; v.bm[1] = b.m2; v.bm[2] = b.m3;
+  }
+  cons_vjp_v(g, stage, v, gq, gA, gB);
 }
 
 // ---- reverse of the faces of one direction, line by line.
@@ -511,27 +532,41 @@ __global__ void k_rcell(Geom g, const double* SA, const double* SB, const double
   }
   const long long i = x + (long long)y * g.sy + (long long)z * g.sz;
   const long long n = g.ng;
-  double gq[7], a[10], gA[5], gB[5];
-  for (int q = 0; q < 7; ++q) gq[q] = PA[q * n + i];
-  cons_vjp(g, STAGE, P, i, SA, SB, x, y, z, gq, gA, gB);
+  // every load of the cell first (an interior cell is its own donor)
+  double gq[7], a[10], gA[5], gB[5], li[5], xs[5];
+  CvIn v;
+  for (int q = 0; q < 7; ++q) gq[q] = __ldg(PA + q * n + i);
+  v.rho = __ldg(P + i);
+  v.u[0] = __ldg(P + n + i); v.u[1] = __ldg(P + 2 * n + i); v.u[2] = __ldg(P + 3 * n + i);
+  v.p = __ldg(P + 4 * n + i); v.e = __ldg(P + 5 * n + i); v.cs = __ldg(P + 6 * n + i);
+  v.aE = 0.0; v.bd = 1.0; v.bm[0] = v.bm[1] = v.bm[2] = 0.0;
+  if (STAGE == 1) {
+    v.aE = __ldg(SA + 4 * n + i);
+    v.bd = __ldg(SB + i);
+    v.bm[0] = __ldg(SB + n + i); v.bm[1] = __ldg(SB + 2 * n + i); v.bm[2] = __ldg(SB + 3 * n + i);
+  }
+  for (int q = 0; q < 5; ++q) li[q] = __ldg(lin + q * n + i);
+  if (STAGE == 0 && nsrc > 0)
+    for (int q = 0; q < 5; ++q) xs[q] = __ldg(X + q * n + i);
+  cons_vjp_v(g, STAGE, v, gq, gA, gB);
   for (int q = 0; q < 5; ++q) { a[q] = gA[q]; a[5 + q] = gB[q]; }
   const bool edge = x == g.ax0 || x == g.ax1 - 1 || y == g.ay0 || y == g.ay1 - 1 ||
                     (g.threed && (z == g.az0 || z == g.az1 - 1));
   if (edge) ghost_fold<STAGE>(g, SA, SB, P, PA, x, y, z, i, a);
   if constexpr (STAGE == 1) {
     for (int q = 0; q < 5; ++q) {
-      const double h = kHalf * lin[q * n + i];
+      const double h = kHalf * li[q];
       const double c1 = h + a[q];
       o1[q * n + i] = c1;
       o2[q * n + i] = (h + a[5 + q]) + c1;
     }
   } else {
     double l[5];
-    for (int q = 0; q < 5; ++q) l[q] = (lin[q * n + i] + a[q]) + a[5 + q];
+    for (int q = 0; q < 5; ++q) l[q] = (li[q] + a[q]) + a[5 + q];
     if (nsrc > 0) {
-      const double d = X[i], m[3] = {X[n + i], X[2 * n + i], X[3 * n + i]};
+      const double d = xs[0], m[3] = {xs[1], xs[2], xs[3]};
       double Es[3];
-      Es[0] = X[4 * n + i];
+      Es[0] = xs[4];
       for (int k = 0; k < nsrc; ++k)
         Es[k + 1] = source_energy(d, m[0], m[1], m[2], Es[k], g.small_eps);
       const double K = kin_mom(d, m[0], m[1], m[2]);
