@@ -76,10 +76,11 @@ struct Tile {
 
 // Stage-kernel tile: TX x TY interior columns per block of NT threads (NT may
 // exceed the tile: the threads without a column of their own take halo work).
-// 32x8 in 256 threads measured 5 % faster on B200 than 16x14 in 256 threads,
-// although the latter fits the x/y face-state and face-flux phases into two
+// 32x8 in 256 threads measured 5 % faster on B200 than 16x14 in 256 threads
+// (although the latter fits the x/y face-state and face-flux phases into two
 // passes of the block instead of three: the wider rows load whole 256-byte
-// segments and need fewer halo columns.
+// segments and need fewer halo columns) and 2 % faster than 32x16 in 512
+// threads (one block per SM: its barriers have no second block to hide them).
 #ifndef BX_TX
 #define BX_TX 32
 #endif

@@ -133,8 +133,9 @@ constexpr int NFY = (TY + 1) * TX;    // y faces
 // (5 + 5) and the plus z-state carried to the next plane (6), kept in shared
 // memory so the x/y phases have the registers
 constexpr int NZS = 16;
-constexpr int SMEM_DOUBLES = 7 * NP + 12 * NSX + 12 * NSY + NZS * NT;
-static_assert(5 * NFX + 5 * NFY <= 7 * NP, "face fluxes alias the primitive plane");
+// the face fluxes of phases C/D alias the primitives of phases A/B
+constexpr int NR0 = (7 * NP > 5 * (NFX + NFY)) ? 7 * NP : 5 * (NFX + NFY);
+constexpr int SMEM_DOUBLES = NR0 + 12 * NSX + 12 * NSY + NZS * NT;
 
 __device__ __forceinline__ void put_prim(double* SP, int i, const Prim& q) {
   SP[0 * NP + i] = q.d;
@@ -190,7 +191,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
                                            Ctrl* C, double* sm, double* red_rate,
                                            unsigned* red_flags) {
   double* SP = sm;                    // [7][TY+4][TX+4] primitives of the plane
-  double* SX = sm + 7 * NP;           // [12][TY][TX+2] x states (minus 0..5, plus 6..11)
+  double* SX = sm + NR0;              // [12][TY][TX+2] x states (minus 0..5, plus 6..11)
   double* SY = SX + 12 * NSX;         // [12][TY+2][TX] y states
   double* FX = sm;                    // [5][TY][TX+1] x face fluxes (aliases SP)
   double* FY = sm + 5 * NFX;          // [5][TY+1][TX] y face fluxes
@@ -430,7 +431,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
 // cell sizes are multiplications by exact reciprocals), 0 = otherwise (cdiv,
 // exact for any spacing)
 template <int STAGE, int PM, bool THREED>
-__global__ void __launch_bounds__(NT, 2) k_stage(StageArgs a) {
+__global__ void __launch_bounds__(NT, 65536 / (NT * 128)) k_stage(StageArgs a) {
   extern __shared__ double sm[];
   __shared__ Geom sg;
   __shared__ double red_rate[NT / 32];
