@@ -73,9 +73,9 @@ __device__ __forceinline__ void hll_vjp(const FaceState& L, const FaceState& R, 
   else if (sam == 2) { gcl += gam_; gvl -= gam_; }
   double gpl = 0, gpr = 0, gdl = 0, gdr = 0, gel = 0, ger = 0;
   double gul[3] = {0, 0, 0}, gur[3] = {0, 0, 0};
-  // c = sqrt(gam p / d): dc/dp = c/(2p), dc/dd = -c/(2d)
-  if (cl > 0.0) { const double h = kHalf * gcl * cl; gpl += h / pl; gdl -= h / dl; }
-  if (cr > 0.0) { const double h = kHalf * gcr * cr; gpr += h / pr; gdr -= h / dr; }
+  // c = sqrt(gam p / d): dc/dp = c/(2p) = gam/(2 d c), dc/dd = -c/(2d) = -c^2/(2 d c)
+  if (cl > 0.0) { const double t = kHalf * gcl / (dl * cl); gpl += gam * t; gdl -= cl * cl * t; }
+  if (cr > 0.0) { const double t = kHalf * gcr / (dr * cr); gpr += gam * t; gdr -= cr * cr * t; }
   // fluxes: f0 = d v, f(1+j) = [j == DIR] p + s(1+j) v, f4 = (s4 + p) v
   gdl = fma(gfl[0], vl, gdl); gvl = fma(gfl[0], sl[0], gvl);
   gdr = fma(gfr[0], vr, gdr); gvr = fma(gfr[0], sr[0], gvr);
