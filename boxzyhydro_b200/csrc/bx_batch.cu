@@ -202,12 +202,24 @@ int bx_batch_create(int32_t nbox, const bx_params* params, bx_batch** out) {
     b->h_ctrl[i].nsrc = 1;
   }
   BCKC(cudaMemcpy(b->d_ctrl, b->h_ctrl, nbox * sizeof(Ctrl), cudaMemcpyHostToDevice));
-  // tiles of every box, longest first
+  // tiles of every box, longest first.  A column tile marches through the whole
+  // box depth when the ensemble has enough columns to fill the GPU many times
+  // over (no z warm-up repeated per chunk); otherwise depths are cut into
+  // chunks of 32 planes.
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  long long ncol = 0;
+  for (int i = 0; i < nbox; ++i) {
+    const Geom& g = b->G[i];
+    ncol += (long long)((g.ax1 - g.ax0 + TX - 1) / TX) * ((g.ay1 - g.ay0 + TY - 1) / TY);
+  }
+  const bool whole = ncol >= 16ll * sms * std::max(1, stage_blocks_per_sm(1, b->pm, b->threed));
   std::vector<std::pair<long long, Tile>> tl;
   for (int i = 0; i < nbox; ++i) {
     const Geom& g = b->G[i];
     const int NAx = g.ax1 - g.ax0, NAy = g.ay1 - g.ay0, NAz = g.az1 - g.az0;
-    const int zc = g.threed ? std::min(NAz, 32) : 1;
+    const int zc = g.threed ? (whole ? NAz : std::min(NAz, 32)) : 1;
     for (int z = 0; z < NAz; z += zc)
       for (int y = 0; y < NAy; y += TY)
         for (int x = 0; x < NAx; x += TX) {
