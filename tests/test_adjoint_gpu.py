@@ -22,9 +22,10 @@ def interior_mask(hp):
     return G.boundary_flags(hp.nx, hp.ny, hp.nz) == 0
 
 
-def setup(walls=(0,) * 6, dims=(14, 12, 11), nsteps=4, snaps=2, seed=0, amp=0.25):
+def setup(walls=(0,) * 6, dims=(14, 12, 11), nsteps=4, snaps=2, seed=0, amp=0.25,
+          dx=1.0 / 16):
     st = small_random_box(nx=dims[0], ny=dims[1], nz=dims[2], walls=walls, seed=seed, amp=amp,
-                          cfl=0.4)
+                          cfl=0.4, dx=dx)
     # ghosts as the donor rule fills them, so the oracle starts from the same state
     from boxzyhydro_b200.hydro import apply_ghost_plan, ghost_plan
     pl = ghost_plan(st.params)
@@ -59,11 +60,12 @@ def rand_dir(hp, rng, scale):
     return v
 
 
-@pytest.mark.parametrize("walls,dims", [((0,) * 6, (14, 12, 11)),
-                                        ((1, 1, 1, 1, 1, 1), (40, 9, 4)),
-                                        ((0, 1, 1, 0, 0, 1), (13, 12, 10))])
-def test_dot_product(walls, dims):
-    st, eng = setup(walls, dims)
+@pytest.mark.parametrize("walls,dims,dx", [((0,) * 6, (14, 12, 11), 1.0 / 16),
+                                           ((1, 1, 1, 1, 1, 1), (40, 9, 4), 1.0 / 16),
+                                           ((0, 1, 1, 0, 0, 1), (13, 12, 10), 1.0 / 16),
+                                           ((0,) * 6, (15, 13, 12), 1.0 / 12)])
+def test_dot_product(walls, dims, dx):
+    st, eng = setup(walls, dims, dx=dx)
     hp = st.params
     consT = fwd(eng, st.cons, frozen=False)
     dts = eng.dts()
