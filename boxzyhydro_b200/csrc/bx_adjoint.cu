@@ -336,8 +336,9 @@ k_rdir(Geom g, const double* P, const double* lamL, double lscale, double dt, do
       const double a2[6] = {qp.d, qp.u1, qp.u2, qp.u3, qp.p, qp.e};
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
-        sl[q] = slope3(a0[q], a1[q], a2[q]);
-        sel |= slope_sel(a0[q], a1[q], a2[q]) << (2 * q);
+        int sq;
+        sl[q] = slope_and_sel(a0[q], a1[q], a2[q], sq);
+        sel |= sq << (2 * q);
       }
       const double ud = DIR == 0 ? qc.u1 : DIR == 1 ? qc.u2 : qc.u3;
       muscl_states<POW2>(qc, ud, sl[0], sl[1], sl[2], sl[3], sl[4], sl[5], dt, ds, ids, mi, pl);

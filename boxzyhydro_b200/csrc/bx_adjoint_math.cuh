@@ -116,6 +116,16 @@ __device__ __forceinline__ int slope_sel(double c0, double c1, double c2) {
   if (x1 <= m23) return 1;
   return x2 <= x3 ? 2 : 3;
 }
+// slope3 (the forward's value, bit for bit) and slope_sel in one evaluation
+__device__ __forceinline__ double slope_and_sel(double c0, double c1, double c2, int& sel) {
+  const double d1 = c1 - c0, d2 = c2 - c0, d3 = c2 - c1;
+  const double x1 = fabs(kTheta * d1), x2 = fabs(kHalf * d2), x3 = fabs(kTheta * d3);
+  const double m23 = fmin(x2, x3);
+  const double m = fmin(x1, m23);
+  const bool pos = (d1 > 0.0) && (d3 > 0.0), neg = (d1 < 0.0) && (d3 < 0.0);
+  sel = !(pos || neg) ? 0 : (x1 <= m23 ? 1 : (x2 <= x3 ? 2 : 3));
+  return pos ? m : (neg ? -m : 0.0);
+}
 // d slope / d (c0, c1, c2) for a selection
 __device__ __forceinline__ void slope_coef(int sel, double& k0, double& k1, double& k2) {
   k0 = k1 = k2 = 0.0;
