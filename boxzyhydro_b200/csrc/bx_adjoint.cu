@@ -455,9 +455,11 @@ k_rdir(Geom g, const double* P, const double* lamL, double lscale, double dt, do
       const int kn = rsx<DIR>(l, j + 1 + o, ND, NL);
 #pragma unroll
       for (int q = 0; q < 6; ++q) {
-        double k0, k1, k2;
-        slope_coef((sel >> (2 * q)) & 3, k0, k1, k2);
-        const double kk = o == 1 ? k0 : (o == 0 ? k1 : k2);
+        // d slope(c+o) / d q(c): c is the slope's c0 (o = +1), c1 (o = 0) or c2 (o = -1)
+        const int sq = (sel >> (2 * q)) & 3;
+        const double kk = o == 1 ? (sq == 1 ? -kTheta : (sq == 2 ? -kHalf : 0.0))
+                        : o == 0 ? (sq == 1 ? kTheta : (sq == 3 ? -kTheta : 0.0))
+                                 : (sq == 2 ? kHalf : (sq == 3 ? kTheta : 0.0));
         acc[q] += kk * r1[(7 + q) * M1 + kn];
       }
     }

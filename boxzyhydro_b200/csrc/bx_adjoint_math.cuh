@@ -105,18 +105,9 @@ __device__ __forceinline__ void hll_vjp(const FaceState& L, const FaceState& R, 
   gR = FS6{gdr, gur[0], gur[1], gur[2], gpr, ger};
 }
 
-// --- generalised minmod slope: index of the selected argument (1: theta*(c1-c0),
-// 2: half*(c2-c0), 3: theta*(c2-c1)) or 0 when the slope is zero.
-__device__ __forceinline__ int slope_sel(double c0, double c1, double c2) {
-  const double d1 = c1 - c0, d2 = c2 - c0, d3 = c2 - c1;
-  const bool pos = (d1 > 0.0) && (d3 > 0.0), neg = (d1 < 0.0) && (d3 < 0.0);
-  if (!(pos || neg)) return 0;
-  const double x1 = fabs(kTheta * d1), x2 = fabs(kHalf * d2), x3 = fabs(kTheta * d3);
-  const double m23 = fmin(x2, x3);
-  if (x1 <= m23) return 1;
-  return x2 <= x3 ? 2 : 3;
-}
-// slope3 (the forward's value, bit for bit) and slope_sel in one evaluation
+// generalised minmod slope: slope3's value (bit for bit) and the index of the
+// selected argument (1: theta*(c1-c0), 2: half*(c2-c0), 3: theta*(c2-c1); 0 when
+// the slope is zero)
 __device__ __forceinline__ double slope_and_sel(double c0, double c1, double c2, int& sel) {
   const double d1 = c1 - c0, d2 = c2 - c0, d3 = c2 - c1;
   const double x1 = fabs(kTheta * d1), x2 = fabs(kHalf * d2), x3 = fabs(kTheta * d3);
@@ -125,13 +116,6 @@ __device__ __forceinline__ double slope_and_sel(double c0, double c1, double c2,
   const bool pos = (d1 > 0.0) && (d3 > 0.0), neg = (d1 < 0.0) && (d3 < 0.0);
   sel = !(pos || neg) ? 0 : (x1 <= m23 ? 1 : (x2 <= x3 ? 2 : 3));
   return pos ? m : (neg ? -m : 0.0);
-}
-// d slope / d (c0, c1, c2) for a selection
-__device__ __forceinline__ void slope_coef(int sel, double& k0, double& k1, double& k2) {
-  k0 = k1 = k2 = 0.0;
-  if (sel == 1) { k0 = -kTheta; k1 = kTheta; }
-  else if (sel == 2) { k0 = -kHalf; k2 = kHalf; }
-  else if (sel == 3) { k1 = -kTheta; k2 = kTheta; }
 }
 
 }  // namespace bx
