@@ -723,7 +723,9 @@ struct bx_adj {
   double *W0 = nullptr, *W1 = nullptr, *W2 = nullptr;  // C0', C1, scratch state
   double* XT = nullptr;  // state after the last step of the forward run (C2_T)
   double *lamA = nullptr, *lamB = nullptr, *lamC1 = nullptr;
-  double *P = nullptr, *PA = nullptr;  // primitives and their adjoints (7 planes each)
+  // primitives and their adjoints (7 planes each); forward steps use the first
+  // 3 planes of P for the stage-0 velocity
+  double *P = nullptr, *PA = nullptr;
   double ms_fwd = 0.0, ms_bwd = 0.0;
   long long fwd_steps_in_bwd = 0;
   size_t bytes = 0;
@@ -766,6 +768,7 @@ static int fwd_step(bx_adj* A, const double* X, int nsrc, double dt, double* Y,
   a.tiles = h->d_tiles;
   a.ncells_total = h->g.ng;
   a.nsrc = nsrc;
+  a.U = A->P;  // the primitives are rebuilt by every reverse stage
   k_set_clock<<<1, 1, 0, h->stream>>>(h->d_ctrl, dt, 1);
   a.X = X;
   a.Y = nullptr;
@@ -1084,6 +1087,7 @@ int bx_adj_forward(bx_adj* A, const double* cons0, double* consT, int32_t frozen
     a.tiles = h->d_tiles;
     a.ncells_total = g.ng;
     a.nsrc = nsrc;
+    a.U = A->P;
     if (frozen) {
       k_set_clock<<<1, 1, 0, s>>>(h->d_ctrl, A->dts[k], 1);
     } else {

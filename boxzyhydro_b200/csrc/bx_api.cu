@@ -599,6 +599,9 @@ static int fused_launch(bx_handle* h) {
   a.tiles = h->d_tiles;
   a.ncells_total = h->g.ng;
   a.nsrc = h->nsrc;
+  // the velocity array is stale while the state lives in the planes (to_phase
+  // rebuilds it), so it holds the stage-0 velocity here
+  a.U = h->pa.u;
   const bool p2 = h->g.pow2 != 0, t3 = h->g.threed != 0;
   CK(launch_dt(h->d_ctrl, 1, h->stream));
   a.X = h->buf[X];

@@ -52,6 +52,7 @@ struct bx_batch {
   long long N = 0;  // cells in the pool (plane stride)
   long long max_ng = 0;
   double* buf[3] = {nullptr, nullptr, nullptr};
+  double* ubuf = nullptr;  // 3 planes: stage-0 velocity of every box
   int cur = 0;
   Geom* d_geom = nullptr;
   Ctrl* d_ctrl = nullptr;
@@ -190,6 +191,7 @@ int bx_batch_create(int32_t nbox, const bx_params* params, bx_batch** out) {
   BCKC(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
   b->own_stream = true;
   for (int k = 0; k < 3; ++k) BCKC(cudaMalloc(&b->buf[k], 5 * b->N * sizeof(double)));
+  BCKC(cudaMalloc(&b->ubuf, 3 * b->N * sizeof(double)));
   BCKC(cudaMalloc(&b->d_geom, nbox * sizeof(Geom)));
   BCKC(cudaMemcpy(b->d_geom, b->G.data(), nbox * sizeof(Geom), cudaMemcpyHostToDevice));
   BCKC(cudaMalloc(&b->d_ctrl, nbox * sizeof(Ctrl)));
@@ -264,6 +266,7 @@ int bx_batch_destroy(bx_batch* b) {
     cudaFree(s.sgn2);
   }
   for (int k = 0; k < 3; ++k) cudaFree(b->buf[k]);
+  cudaFree(b->ubuf);
   cudaFree(b->d_geom);
   cudaFree(b->d_ctrl);
   if (b->h_ctrl) cudaFreeHost(b->h_ctrl);
@@ -363,6 +366,7 @@ static int enqueue_steps(bx_batch* b, int nsteps) {
   a.tiles = b->d_tiles;
   a.ncells_total = b->N;
   a.nsrc = 0;  // per box
+  a.U = b->ubuf;
   int c = b->cur;
   b->step_x.assign(nsteps, 0);
   for (int k = 0; k < nsteps; ++k) {

@@ -116,6 +116,8 @@ struct StageArgs {
   const double* X;   // step input planes (C2 if nsrc==2, C3 if nsrc==1)
   const double* Y;   // stage-1 input: C1
   double* out;       // stage output planes (interior cells written)
+  double* U;         // 3 planes: stage 0 writes m/rho of the step input at its own
+                     // cells, stage 1 reads it as the stale velocity of its EOS
   Ctrl* ctrl;        // per box control blocks
   const Geom* geom;  // per box geometry (device)
   const Tile* tiles;

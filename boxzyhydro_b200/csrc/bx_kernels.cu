@@ -66,6 +66,23 @@ __device__ __forceinline__ Cons load_cons(const double* B, long long PS, const G
   return r;
 }
 
+// the step input's velocity m/rho at a cell, as stage 0 stored it for the
+// interior cells (ghost cells read their source cell, reflected components negated)
+__device__ __forceinline__ void load_u(const double* U, long long PS, const Geom& g, int x, int y,
+                                       int z, double& u1, double& u2, double& u3) {
+  bool fx = false, fy = false, fz = false;
+  const int xx = remap_axis(x, g.ax0, g.ax1, g.wall[0], g.wall[1], fx);
+  const int yy = remap_axis(y, g.ay0, g.ay1, g.wall[2], g.wall[3], fy);
+  const int zz = g.threed ? remap_axis(z, g.az0, g.az1, g.wall[4], g.wall[5], fz) : z;
+  const long long c = g.base + xx + (long long)yy * g.sy + (long long)zz * g.sz;
+  u1 = ldg(U + c);
+  u2 = ldg(U + PS + c);
+  u3 = ldg(U + 2 * PS + c);
+  if (fx) u1 = -u1;
+  if (fy) u2 = -u2;
+  if (fz) u3 = -u3;
+}
+
 __device__ __forceinline__ void apply_sources(Cons& c, int nsrc, double small_eps) {
   for (int k = 0; k < nsrc; ++k) c.E = source_energy(c.d, c.m1, c.m2, c.m3, c.E, small_eps);
 }
@@ -75,7 +92,8 @@ __device__ __forceinline__ void apply_sources(Cons& c, int nsrc, double small_ep
 //           state() with the velocity array of the previous step, which equals
 //           m/rho of the same momenta (source adds zero momentum).
 //  stage 1: cons = Y; u = m/rho of Y (velocity at main.f90:355); p from state()
-//           with the stage-0 velocity m0/rho0 (main.f90:353 uses the stale u).
+//           with the stage-0 velocity m0/rho0 (main.f90:353 uses the stale u),
+//           which stage 0 stored in U (the same quotient, so the same bits).
 template <int STAGE>
 __device__ __forceinline__ Prim load_prim(const StageArgs& a, const Geom& g, int x, int y, int z,
                                           unsigned& flags, int nsrc, bool need_c = true) {
@@ -91,13 +109,13 @@ __device__ __forceinline__ Prim load_prim(const StageArgs& a, const Geom& g, int
     q.e = recon_eps(q.d, c.E, q.u1, q.u2, q.u3, g.small_eps);
     q.p = q.e * g.gm1;
   } else {
-    const Cons c0 = load_cons(a.X, PS, g, x, y, z);
     const Cons c1 = load_cons(a.Y, PS, g, x, y, z);
+    double s1, s2, s3;
+    load_u(a.U, PS, g, x, y, z, s1, s2, s3);
     q.d = c1.d;
     q.u1 = c1.m1 / c1.d;
     q.u2 = c1.m2 / c1.d;
     q.u3 = c1.m3 / c1.d;
-    const double s1 = c0.m1 / c0.d, s2 = c0.m2 / c0.d, s3 = c0.m3 / c0.d;
     q.e = recon_eps(q.d, c1.E, q.u1, q.u2, q.u3, g.small_eps);
     q.p = eos_pressure(q.d, c1.E, s1, s2, s3, g.gm1, g.small_eps);
   }
@@ -251,6 +269,13 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         Pk = load_prim<STAGE>(a, g, gx, gy, z, flags, nsrc);
       }
       put_prim(SP, (ty + 2) * PW + (tx + 2), Pk);
+      if (STAGE == 0) {
+        // sources change only E, so this is m/rho of the step input
+        const long long o = g.base + gx + (long long)gy * g.sy + (long long)z * g.sz;
+        a.U[o] = Pk.u1;
+        a.U[PS + o] = Pk.u2;
+        a.U[2 * PS + o] = Pk.u3;
+      }
     }
     // halo cells go first to the threads without a column of their own
     for (int i = (tid + NT - TX * TY) % NT; i < nhalo; i += NT) {
