@@ -342,11 +342,11 @@ def adjoint_arm(args, rank, world, local):
     del st
     snaps = args.snapshots
     if snaps <= 0:
-        # engine: 7 state sets + 14 scratch planes + (snaps + 1) state sets;
+        # engine: 9 state sets + 14 scratch planes + (snaps + 1) state sets;
         # this arm, beside c0: gradient, direction, perturbed state, output and
         # one density plane (21 planes)
         free = torch.cuda.mem_get_info(dev)[0]
-        fixed = (7 * 5 + 14 + 5 + 21) * plane + (6 << 30)
+        fixed = (9 * 5 + 14 + 5 + 21) * plane + (6 << 30)
         snaps = int(max(1, min(args.steps, (free - fixed) // (5 * plane))))
     peak = [0]
 

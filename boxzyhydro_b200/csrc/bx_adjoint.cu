@@ -723,6 +723,14 @@ struct bx_adj {
   // so the backward skips its recomputation (nsteps state sets)
   double* c1pool = nullptr;
   bool c1_valid = false;
+  // stage-0 results left by the last step of recent advances, tagged with
+  // their step (-1: empty): the reverse of that step then skips its stage-0
+  // recompute.  Two entries, so an advance to state k can leave C1 of step k-1
+  // while the entry of step k, needed first, stays.
+  double* c1c[2] = {nullptr, nullptr};
+  long long c1tag[2] = {-1, -1};
+  long long c1_hits = 0;
+  long long rev_done = 0;  // last reversed step (steps are reversed downwards)
   // work planes
   double *W0 = nullptr, *W1 = nullptr, *W2 = nullptr;  // C0', C1, scratch state
   double* XT = nullptr;  // state after the last step of the forward run (C2_T)
@@ -762,9 +770,9 @@ static int amalloc(bx_adj* A, double** p, long long ndoubles) {
 }
 
 // one forward step from X into Y (fused stage kernels, dt frozen at dts[k]),
-// using W1 for the stage-0 result.  Returns the guard flags in *flags if given.
+// with the stage-0 result in c1out, or in W1 when c1out is null.
 static int fwd_step(bx_adj* A, const double* X, int nsrc, double dt, double* Y,
-                    bool stage0_only = false) {
+                    bool stage0_only = false, double* c1out = nullptr) {
   bx_handle* h = A->h;
   StageArgs a{};
   a.ctrl = h->d_ctrl;
@@ -776,10 +784,10 @@ static int fwd_step(bx_adj* A, const double* X, int nsrc, double dt, double* Y,
   k_set_clock<<<1, 1, 0, h->stream>>>(h->d_ctrl, dt, 1);
   a.X = X;
   a.Y = nullptr;
-  a.out = A->W1;
+  a.out = c1out ? c1out : A->W1;
   ACK(launch_stage(0, h->g.pow2 ? 1 : 0, h->g.threed != 0, a, h->ntiles, h->stream));
   if (stage0_only) return BX_OK;
-  a.Y = A->W1;
+  a.Y = a.out;
   a.out = Y;
   ACK(launch_stage(1, h->g.pow2 ? 1 : 0, h->g.threed != 0, a, h->ntiles, h->stream));
   return BX_OK;
@@ -862,9 +870,13 @@ static int rev_step(bx_adj* A, const double* X, long long k, double* lam) {
   const double* C1 = A->W1;
   if (A->c1pool && A->c1_valid) {
     C1 = A->c1pool + k * 5 * g.ng;
+  } else if (A->c1tag[0] == k || A->c1tag[1] == k) {
+    C1 = A->c1c[A->c1tag[0] == k ? 0 : 1];
+    A->c1_hits += 1;
   } else {
     if (int r = fwd_step(A, X, nsrc, dt, nullptr, true)) return r;  // W1 <- C1
   }
+  A->rev_done = k;
   // stage 1 reads lam/2; writes lamC1 (adjoint of C1) and lamA (of C0')
   if (int r = rev_stage(A, 1, C1, A->W0, lam, kHalf, dt, lam, A->lamC1, A->lamA, X, nsrc))
     return r;
@@ -918,7 +930,22 @@ static int advance(bx_adj* A, const double* src, long long from, long long to, d
   const double* cur = src;
   for (long long k = from; k < to; ++k) {
     double* out = ((to - k) % 2 == 1) ? dst : A->W2;
-    if (int r = fwd_step(A, cur, A->step_nsrc[k], A->dts[k], out)) return r;
+    double* c1out = nullptr;
+    if (k == to - 1 && !A->c1pool) {
+      // keep C1 of step to-1 (reversed soon after step `to` when no further
+      // split comes between them) in an entry that is free or already used;
+      // else in the one of the step reversed later, never in step `to`'s
+      auto dead = [&](long long t) { return t < 0 || t >= A->rev_done; };
+      int j;
+      if (A->c1tag[0] == to) j = 1;
+      else if (A->c1tag[1] == to) j = 0;
+      else if (dead(A->c1tag[0])) j = 0;
+      else if (dead(A->c1tag[1])) j = 1;
+      else j = A->c1tag[0] < A->c1tag[1] ? 0 : 1;
+      A->c1tag[j] = k;
+      c1out = A->c1c[j];
+    }
+    if (int r = fwd_step(A, cur, A->step_nsrc[k], A->dts[k], out, false, c1out)) return r;
     cur = out;
     A->fwd_steps_in_bwd += 1;
   }
@@ -966,7 +993,7 @@ int bx_adj_destroy(bx_adj* A) {
   if (A->h && A->h->stream) cudaStreamSynchronize(A->h->stream);
   for (double* p : A->pool) cudaFree(p);
   double* ps[] = {A->W0, A->W1, A->W2, A->XT, A->lamA, A->lamB, A->lamC1,
-                  A->P,  A->PA, A->d_dts};
+                  A->P,  A->PA, A->d_dts, A->c1c[0], A->c1c[1]};
   for (double* p : ps) cudaFree(p);
   cudaFree(A->c1pool);
   if (A->h) bx_destroy(A->h);
@@ -1005,7 +1032,8 @@ int bx_adj_create(const bx_params* params, int64_t nsteps, int32_t snapshots, bx
   A->pool.assign(A->snaps + 1, nullptr);
   for (int k = 0; k <= A->snaps; ++k)
     if ((rc = amalloc(A, &A->pool[k], 5 * n))) return fail(rc);
-  double** planes5[] = {&A->W0, &A->W1, &A->W2, &A->XT, &A->lamA, &A->lamB, &A->lamC1};
+  double** planes5[] = {&A->W0,   &A->W1,    &A->W2,    &A->XT,   &A->lamA,
+                        &A->lamB, &A->lamC1, &A->c1c[0], &A->c1c[1]};
   for (double** p : planes5)
     if ((rc = amalloc(A, p, 5 * n))) return fail(rc);
   if ((rc = amalloc(A, &A->P, 7 * n))) return fail(rc);
@@ -1152,6 +1180,9 @@ int bx_adj_backward(bx_adj* A, const double* lamT, double* lam0) {
   cudaEventCreate(&e1);
   ACK(cudaEventRecord(e0, s));
   A->fwd_steps_in_bwd = 0;
+  A->c1tag[0] = A->c1tag[1] = -1;
+  A->c1_hits = 0;
+  A->rev_done = A->nsteps;
   A->pool_free.clear();
   const bool chain = A->chain_valid;
   for (int k = A->snaps; k >= 1; --k)
