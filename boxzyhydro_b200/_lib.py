@@ -76,6 +76,7 @@ def lib():
         "bx_set_clock": (C.c_int, [H, C.c_double, C.c_double, C.c_int64]),
         "bx_get_clock": (C.c_int, [H, dp, dp, dp, i64p]),
         "bx_step": (C.c_int, [H, C.c_double, i32p]),
+        "bx_step_host": (C.c_int, [H, vp, vp, C.c_double, i32p]),
         "bx_run": (C.c_int, [H, C.c_double, C.c_int64, i64p]),
         "bx_write_celldump": (C.c_int, [H, C.c_char_p, vp]),
         "bx_read_celldump": (C.c_int, [H, C.c_char_p, vp, dp, i64p]),

@@ -177,6 +177,7 @@ static int create_handle(const bx_params* params, bx_handle** out, bool lean) {
   const int per_sm = std::max(1, stage_blocks_per_sm(1, h->g.pow2, h->g.threed));
   std::vector<Tile> tiles = make_tiles(h->g, 0, sms * per_sm);
   h->ntiles = (int)tiles.size();
+  h->h_tiles = tiles;
   CKC(dalloc((void**)&h->d_tiles, tiles.size() * sizeof(Tile)));
   CKC(cudaMemcpy(h->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
   CKC(dalloc((void**)&h->d_ctrl, sizeof(Ctrl)));
@@ -207,6 +208,9 @@ int bx_destroy(bx_handle* h) {
   cudaFree(h->pa.gtmp);
   cudaFree(h->pa.muc);
   cudaFree(h->d_eos);
+  for (cudaStream_t x : h->hs)
+    if (x) cudaStreamDestroy(x);
+  for (cudaEvent_t e : h->hev) cudaEventDestroy(e);
   cudaFree(h->d_dst);
   cudaFree(h->d_src1);
   cudaFree(h->d_src2);
@@ -635,6 +639,60 @@ static int enter_fused(bx_handle* h) {
   return pull_clock(h);
 }
 
+// the step on the per-phase kernels (reference data flow), then back to the
+// fused form when the step left a state it reproduces
+static int phase_path(bx_handle* h, int32_t* ran) {
+  if (int r = phase_step(h)) return r;
+  if (int r = pull_clock(h)) return r;
+  const unsigned f = h->clock.flags;
+  h->status |= f;
+  h->last_path = 0;
+  if (ran) *ran = 1;
+  h->clock.flags = 0;
+  if (int r = push_clock(h)) return r;
+  if (f & kFlagNonFinite) return set_err(h, BX_ERR_STATE, "non-finite state produced by the step");
+  if (h->eligible && !h->gforce_set && !(f & (kFlagVlimit | kFlagLowRho)))
+    return enter_fused(h);
+  return BX_OK;
+}
+
+// after the fused launches of a step from the clock `before`: commit it, or
+// redo it on the per-phase kernels when the limiter or the low-density branch
+// fired (the input planes are untouched)
+static int after_fused(bx_handle* h, const Ctrl& before, int32_t* ran, bool timed) {
+  if (int r = pull_clock(h)) return r;
+  const unsigned f = h->clock.flags;
+  if (f & kFlagNonFinite) {
+    h->status |= f;
+    return set_err(h, BX_ERR_STATE, "non-finite state produced by the step");
+  }
+  if (timed && h->prof) {
+    float t0 = 0.f, t1 = 0.f;
+    CK(cudaEventElapsedTime(&t0, h->ev[0], h->ev[1]));
+    CK(cudaEventElapsedTime(&t1, h->ev[1], h->ev[2]));
+    h->ms_stage[0] += t0;
+    h->ms_stage[1] += t1;
+    h->n_stage += 1;
+  }
+  if (!(f & (kFlagVlimit | kFlagLowRho))) {
+    h->cur = (h->cur + 2) % 3;
+    h->nsrc = 2;
+    h->clock.flags = 0;
+    if (int r = push_clock(h)) return r;
+    h->last_path = 1;
+    if (ran) *ran = 1;
+    return BX_OK;
+  }
+  // the limiter or the low-density branch fires in this step: redo it from
+  // its untouched input with the reference data flow
+  h->status |= f & (kFlagVlimit | kFlagLowRho);
+  h->clock = before;
+  h->clock.rate_bits = 0;
+  if (int r = push_clock(h)) return r;
+  if (int r = to_phase(h)) return r;
+  return phase_path(h, ran);
+}
+
 int bx_step(bx_handle* h, double endtime, int32_t* ran) {
   CHECK_H();
   if (ran) *ran = 0;
@@ -651,48 +709,176 @@ int bx_step(bx_handle* h, double endtime, int32_t* ran) {
   const Ctrl before = h->clock;
   if (h->mode == 1) {
     if (int r = fused_launch(h)) return r;
-    if (int r = pull_clock(h)) return r;
-    const unsigned f = h->clock.flags;
-    if (f & kFlagNonFinite) {
-      h->status |= f;
-      return set_err(h, BX_ERR_STATE, "non-finite state produced by the step");
+    return after_fused(h, before, ran, true);
+  }
+  return phase_path(h, ran);
+}
+
+// ---- one step with the state on the host, copies overlapped with the step.
+// Slabs: groups of consecutive tile z-chunks (the tiles are z-chunk major),
+// each with its cell range and the entries of the (igrid-ordered) ghost plan
+// in it; a slab takes the next chunk too while a ghost of it has its donor
+// beyond it, so every slab's ghosts can be filled once the slab is done.
+static int host_io_setup(bx_handle* h) {
+  if (!h->slabs.empty()) return BX_OK;
+  const Geom& g = h->g;
+  const long long n = g.ng;
+  struct Chunk {
+    int z0, z1, t0, nt;
+  };
+  std::vector<Chunk> ch;
+  for (int t = 0; t < (int)h->h_tiles.size(); ++t) {
+    const Tile& T = h->h_tiles[t];
+    if (ch.empty() || ch.back().z0 != T.z0) ch.push_back(Chunk{T.z0, T.z1, t, 0});
+    ch.back().nt += 1;
+  }
+  const std::vector<int32_t>& dst = h->T.dst;
+  const std::vector<int32_t>& src = h->T.src2;
+  auto first_ghost = [&](long long i) {
+    return (int)(std::lower_bound(dst.begin(), dst.end(), (int32_t)std::min<long long>(i, INT32_MAX)) -
+                 dst.begin());
+  };
+  size_t c = 0;
+  while (c < ch.size()) {
+    bx_handle::Slab sl{};
+    sl.t0 = ch[c].t0;
+    sl.i0 = h->slabs.empty() ? 0 : h->slabs.back().i1;
+    sl.g0 = first_ghost(sl.i0);
+    size_t e = c;
+    for (;;) {
+      const bool last = e + 1 == ch.size();
+      sl.i1 = last ? n : (long long)(g.az0 + ch[e].z1) * g.sz;
+      sl.g1 = first_ghost(sl.i1);
+      bool ok = true;
+      for (int k = sl.g0; k < sl.g1 && ok; ++k) ok = src[k] < sl.i1;
+      if (ok || last) break;
+      ++e;
     }
-    if (h->prof) {
-      float t0 = 0.f, t1 = 0.f;
-      CK(cudaEventElapsedTime(&t0, h->ev[0], h->ev[1]));
-      CK(cudaEventElapsedTime(&t1, h->ev[1], h->ev[2]));
-      h->ms_stage[0] += t0;
-      h->ms_stage[1] += t1;
-      h->n_stage += 1;
-    }
-    if (!(f & (kFlagVlimit | kFlagLowRho))) {
-      h->cur = (h->cur + 2) % 3;
-      h->nsrc = 2;
-      h->clock.flags = 0;
-      if (int r = push_clock(h)) return r;
-      h->last_path = 1;
-      if (ran) *ran = 1;
-      return BX_OK;
-    }
-    // the limiter or the low-density branch fires in this step: redo it from
-    // its untouched input with the reference data flow
-    h->status |= f & (kFlagVlimit | kFlagLowRho);
-    h->clock = before;
+    sl.nt = ch[e].t0 + ch[e].nt - sl.t0;
+    h->slabs.push_back(sl);
+    c = e + 1;
+  }
+  for (int k = 0; k < 3; ++k)
+    CK(cudaStreamCreateWithFlags(&h->hs[k], cudaStreamNonBlocking));
+  const size_t nev = 3 * h->slabs.size() + 3;
+  h->hev.assign(nev, nullptr);
+  for (size_t k = 0; k < nev; ++k) CK(cudaEventCreateWithFlags(&h->hev[k], cudaEventDisableTiming));
+  return BX_OK;
+}
+
+int bx_step_host(bx_handle* h, const double* cons_in, double* cons_out, double endtime,
+                 int32_t* ran) {
+  CHECK_H();
+  if (ran) *ran = 0;
+  if (!cons_in || !cons_out) return set_err(h, BX_ERR_ARG, "cons_in and cons_out are required");
+  if (!h->pa.cons) return set_err(h, BX_ERR_STATE, "the handle holds no state (lean handle)");
+  if (!h->eligible || h->gforce_set || h->g.tab) {
+    // not on the fused path: the three calls it stands for
+    if (int r = bx_upload_conserved(h, cons_in)) return r;
+    if (int r = bx_step(h, endtime, ran)) return r;
+    return bx_download(h, cons_out, nullptr, nullptr);
+  }
+  if (int r = host_io_setup(h)) return r;
+  const Geom& g = h->g;
+  const long long n = g.ng;
+  const int ns = (int)h->slabs.size();
+  cudaStream_t s = h->stream, xs = h->hs[0], cs = h->hs[1], s2 = h->hs[2];
+  cudaEvent_t* ev = h->hev.data();
+  cudaEvent_t ev_start = ev[0], ev_st0 = ev[1], ev_join = ev[2];
+  cudaEvent_t* ev_in = ev + 3;        // per slab: uploaded
+  cudaEvent_t* ev_st1 = ev + 3 + ns;  // per slab: stage 1 done
+  cudaEvent_t* ev_cv = ev + 3 + 2 * ns;  // per slab: converted
+  // the reference arrays are rebuilt from the planes whenever they are asked
+  // for, so their cons array serves as the AoS staging of both directions
+  double* aos = h->pa.cons;
+  double* X = h->buf[h->cur];
+  const size_t cell = 5 * sizeof(double);
+  // ---- upload: copies on xs, each slab transposed into the planes on s
+  CK(cudaEventRecord(ev_start, s));
+  CK(cudaStreamWaitEvent(xs, ev_start, 0));
+  for (int j = 0; j < ns; ++j) {
+    const bx_handle::Slab& sl = h->slabs[j];
+    CK(cudaMemcpyAsync(aos + 5 * sl.i0, cons_in + 5 * sl.i0, (sl.i1 - sl.i0) * cell,
+                       cudaMemcpyHostToDevice, xs));
+    CK(cudaEventRecord(ev_in[j], xs));
+    CK(cudaStreamWaitEvent(s, ev_in[j], 0));
+    CK(slab_in(aos, X, n, sl.i0, sl.i1, s));
+  }
+  h->launches += ns;
+  // the state must be one the fused stages reproduce (as bx_upload_conserved checks)
+  h->clock.flags = 0;
+  h->clock.rate_bits = 0;
+  if (int r = push_clock(h)) return r;
+  CK(box_check_clean(g, X, n, h->nghost, h->d_dst, h->d_src2, h->d_sgn2, h->d_ctrl, s));
+  CK(box_rate(g, X, n, h->d_ctrl, s));
+  h->launches += 3;
+  if (int r = pull_clock(h)) return r;
+  if (h->clock.flags & kFlagNotClean) {
+    // the reference data flow, from the uploaded cons
+    h->clock.flags = 0;
     h->clock.rate_bits = 0;
     if (int r = push_clock(h)) return r;
-    if (int r = to_phase(h)) return r;
+    CK(cudaMemcpyAsync(h->pa.cons, X, 5 * n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+    CK(prims_from_cons(g, h->pa, s));
+    h->launches += 1;
+    h->mode = 0;
+    if (int r = bx_adindx_fill(h)) return r;
+    if (int r = bx_step(h, endtime, ran)) return r;
+    return bx_download(h, cons_out, nullptr, nullptr);
   }
-  if (int r = phase_step(h)) return r;
-  if (int r = pull_clock(h)) return r;
-  const unsigned f = h->clock.flags;
-  h->status |= f;
-  h->last_path = 0;
-  if (ran) *ran = 1;
-  h->clock.flags = 0;
-  if (int r = push_clock(h)) return r;
-  if (f & kFlagNonFinite) return set_err(h, BX_ERR_STATE, "non-finite state produced by the step");
-  if (h->eligible && !h->gforce_set && !(f & (kFlagVlimit | kFlagLowRho)))
-    return enter_fused(h);
+  h->nsrc = 1;
+  h->mode = 1;
+  if (!(h->clock.time < endtime) || h->clock.step >= 1000000)
+    return bx_download(h, cons_out, nullptr, nullptr);
+  if (h->clock.endtime != endtime) {
+    h->clock.endtime = endtime;
+    if (int r = push_clock(h)) return r;
+  }
+  const Ctrl before = h->clock;
+  // ---- the step: stage 0 on s, stage 1 slab by slab on s and s2 in turn;
+  // each finished slab is converted on cs and copied back on xs
+  const int Yi = (h->cur + 1) % 3, Zi = (h->cur + 2) % 3;
+  const bool p2 = g.pow2 != 0, t3 = g.threed != 0;
+  StageArgs a{};
+  a.ctrl = h->d_ctrl;
+  a.geom = h->d_geom;
+  a.ncells_total = n;
+  a.nsrc = h->nsrc;
+  a.U = h->pa.u;
+  a.tiles = h->d_tiles;
+  CK(launch_dt(h->d_ctrl, 1, s));
+  a.X = X;
+  a.out = h->buf[Yi];
+  CK(launch_stage(0, p2, t3, a, h->ntiles, s));
+  CK(cudaEventRecord(ev_st0, s));
+  CK(cudaStreamWaitEvent(s2, ev_st0, 0));
+  a.Y = h->buf[Yi];
+  a.out = h->buf[Zi];
+  for (int j = 0; j < ns; ++j) {
+    const bx_handle::Slab& sl = h->slabs[j];
+    cudaStream_t sj = (j & 1) ? s2 : s;
+    StageArgs aj = a;
+    aj.tiles = h->d_tiles + sl.t0;
+    CK(launch_stage(1, p2, t3, aj, sl.nt, sj));
+    CK(cudaEventRecord(ev_st1[j], sj));
+    CK(cudaStreamWaitEvent(cs, ev_st1[j], 0));
+    CK(slab_out(g, h->buf[Zi], n, 2, aos, sl.i0, sl.i1, h->d_dst, h->d_src2, h->d_sgn2, sl.g0,
+                sl.g1, cs));
+    CK(cudaEventRecord(ev_cv[j], cs));
+    CK(cudaStreamWaitEvent(xs, ev_cv[j], 0));
+    CK(cudaMemcpyAsync(cons_out + 5 * sl.i0, aos + 5 * sl.i0, (sl.i1 - sl.i0) * cell,
+                       cudaMemcpyDeviceToHost, xs));
+  }
+  CK(cudaEventRecord(ev_join, s2));
+  CK(cudaStreamWaitEvent(s, ev_join, 0));
+  CK(launch_end(h->d_ctrl, 1, s));
+  h->launches += 3 + 3 * ns;
+  // the copies (and the conversions they wait for) finish before anything else
+  // may touch the staging or cons_out
+  CK(cudaStreamSynchronize(xs));
+  if (int r = after_fused(h, before, ran, false)) return r;
+  // a step redone on the per-phase kernels: its result replaces the copies
+  if (h->last_path == 0) return bx_download(h, cons_out, nullptr, nullptr);
   return BX_OK;
 }
 

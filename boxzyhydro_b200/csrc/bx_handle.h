@@ -3,6 +3,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <vector>
 
 #include "bx_internal.h"
 
@@ -37,6 +38,18 @@ struct bx_handle {
   long long n_stage = 0;
   long long launches = 0;  // kernels of this library launched on the handle's stream
   double* d_eos = nullptr;  // device copy of the tabulated EOS (H2STAT >= 0)
+  // bx_step_host: the tiles on the host, the z slabs of the cell range (groups
+  // of tile z-chunks) with their ghost ranges, and the streams and events that
+  // overlap the copies with the step (made on first use)
+  std::vector<bx::Tile> h_tiles;
+  struct Slab {
+    long long i0, i1;  // cells [i0, i1)
+    int g0, g1;        // entries [g0, g1) of the ghost plan
+    int t0, nt;        // tiles [t0, t0 + nt)
+  };
+  std::vector<Slab> slabs;
+  cudaStream_t hs[3] = {nullptr, nullptr, nullptr};  // copies, conversions, second stage-1
+  std::vector<cudaEvent_t> hev;
   std::string err;
 };
 

@@ -189,6 +189,14 @@ cudaError_t check_clean(const Geom& g, const PhaseArrays& a, int nghost, const i
 // AoS host layout <-> SoA device layout
 cudaError_t aos_to_soa(const double* aos, double* soa, long long n, int k, cudaStream_t s);
 cudaError_t prims_from_cons(const Geom& g, PhaseArrays& a, cudaStream_t s);
+// host-overlapped step: AoS slab [i0, i1) -> planes; planes -> AoS reference cons
+// of the slab (interior cells nsrc sources short, then the ghosts [g0, g1) of
+// the resolved plan, whose donors lie in this slab or an earlier one)
+cudaError_t slab_in(const double* aos, double* X, long long ps, long long i0, long long i1,
+                    cudaStream_t s);
+cudaError_t slab_out(const Geom& g, const double* X, long long ps, int nsrc, double* aos,
+                     long long i0, long long i1, const int32_t* dst, const int32_t* src2,
+                     const uint8_t* sgn2, int g0, int g1, cudaStream_t s);
 cudaError_t fill_const(double* a, long long n, double v, cudaStream_t s);
 cudaError_t soa_to_aos(const double* soa, double* aos, long long n, int k, cudaStream_t s);
 

@@ -1064,6 +1064,41 @@ __global__ void k_fill_resolved(int nghost, const int32_t* dst, const int32_t* s
   cons[3 * n + d] = (m & 4) ? -cons[3 * n + s] : cons[3 * n + s];
   cons[4 * n + d] = cons[4 * n + s];
 }
+// Host-overlapped step: z slabs of a cell range [i0, i1) between the reference's
+// AoS layout (5 doubles per cell, as on the host) and the fused planes X.
+__global__ void k_slab_in(const double* aos, double* X, long long ps, long long i0, long long i1) {
+  const long long i = i0 + blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= i1) return;
+  for (int q = 0; q < 5; ++q) X[q * ps + i] = aos[5 * i + q];
+}
+// the reference cons of the interior cells of the slab (as k_f2p_interior)
+__global__ void k_slab_out(Geom g, const double* X, long long ps, int nsrc, double* aos,
+                           long long i0, long long i1) {
+  const long long i = i0 + blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= i1) return;
+  const int x = (int)(i % g.nx), y = (int)((i / g.nx) % g.ny), z = (int)(i / g.sz);
+  if (is_ghost(g, x, y, z)) return;
+  Cons c{X[i], X[ps + i], X[2 * ps + i], X[3 * ps + i], X[4 * ps + i]};
+  apply_sources(c, nsrc - 1, g.small_eps);
+  aos[5 * i] = c.d;
+  aos[5 * i + 1] = c.m1;
+  aos[5 * i + 2] = c.m2;
+  aos[5 * i + 3] = c.m3;
+  aos[5 * i + 4] = c.E;
+}
+// the ghosts [g0, g1) of the resolved plan (as k_fill_resolved; donors already written)
+__global__ void k_slab_ghosts(const int32_t* dst, const int32_t* src, const uint8_t* sgn,
+                              double* aos, int g0, int g1) {
+  const int k = g0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= g1) return;
+  const long long s = src[k], d = dst[k];
+  const unsigned m = sgn[k];
+  aos[5 * d] = aos[5 * s];
+  aos[5 * d + 1] = (m & 1) ? -aos[5 * s + 1] : aos[5 * s + 1];
+  aos[5 * d + 2] = (m & 2) ? -aos[5 * s + 2] : aos[5 * s + 2];
+  aos[5 * d + 3] = (m & 4) ? -aos[5 * s + 3] : aos[5 * s + 3];
+  aos[5 * d + 4] = aos[5 * s + 4];
+}
 // velocity and pressure arrays of the reference after the last state()/velocity()
 __global__ void k_f2p_prims(Geom g, PhaseArrays a) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -1193,6 +1228,18 @@ cudaError_t fused_to_phase(const Geom& g, const double* X, int nsrc, PhaseArrays
 __global__ void k_fill_const(double* a, long long n, double v) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i < n) a[i] = v;
+}
+cudaError_t slab_in(const double* aos, double* X, long long ps, long long i0, long long i1,
+                    cudaStream_t s) {
+  if (i1 > i0) k_slab_in<<<nblk(i1 - i0), PB, 0, s>>>(aos, X, ps, i0, i1);
+  return cudaGetLastError();
+}
+cudaError_t slab_out(const Geom& g, const double* X, long long ps, int nsrc, double* aos,
+                     long long i0, long long i1, const int32_t* dst, const int32_t* src2,
+                     const uint8_t* sgn2, int g0, int g1, cudaStream_t s) {
+  if (i1 > i0) k_slab_out<<<nblk(i1 - i0), PB, 0, s>>>(g, X, ps, nsrc, aos, i0, i1);
+  if (g1 > g0) k_slab_ghosts<<<nblk(g1 - g0), PB, 0, s>>>(dst, src2, sgn2, aos, g0, g1);
+  return cudaGetLastError();
 }
 cudaError_t fill_const(double* a, long long n, double v, cudaStream_t s) {
   k_fill_const<<<nblk(n), PB, 0, s>>>(a, n, v);

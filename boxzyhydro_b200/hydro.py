@@ -185,6 +185,25 @@ class Hydro:
         self._c(lib().bx_step(self._h, float(endtime), C.byref(ran)))
         return bool(ran.value)
 
+    def step_host(self, cons_in, cons_out=None, endtime=1e300):
+        """One step of a state held on the host: upload_conserved(cons_in), step(),
+        download of cons into cons_out (cons_in itself when None), with the copies
+        overlapped with the step (bx_step_host).  Arrays (ngrid, 5) float64,
+        C-contiguous; page-locked memory lets the copies run asynchronously."""
+        if cons_out is None:
+            cons_out = cons_in
+        for a in (cons_in, cons_out):
+            if (not isinstance(a, np.ndarray) or a.dtype != np.float64 or a.shape != (self.ng, 5)
+                    or not a.flags.c_contiguous):
+                raise ValueError("cons arrays must be C-contiguous float64 of shape (ngrid, 5)")
+        if not cons_out.flags.writeable:
+            raise ValueError("cons_out must be writeable")
+        ran = C.c_int32()
+        self._c(lib().bx_step_host(self._h, cons_in.ctypes.data_as(C.c_void_p),
+                                   cons_out.ctypes.data_as(C.c_void_p), float(endtime),
+                                   C.byref(ran)))
+        return bool(ran.value)
+
     def run(self, endtime=1e300, nsteps=(1 << 62)):
         n = C.c_int64()
         self._c(lib().bx_run(self._h, float(endtime), int(nsteps), C.byref(n)))

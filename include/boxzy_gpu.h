@@ -113,6 +113,19 @@ int bx_get_clock(bx_handle *h, double *time, double *dt, double *dtold, int64_t 
  * *ran = 0 (ran may be NULL). */
 int bx_step(bx_handle *h, double endtime, int32_t *ran);
 
+/* One loop iteration (main.f90:212-545) on a state held on the host: the result
+ * of bx_upload_conserved(h, cons_in), bx_step(h, endtime, ran) and
+ * bx_download(h, cons_out, NULL, NULL), bit for bit, with the copies overlapped
+ * with the work: the upload goes in z slabs, each transposed as it lands, and the
+ * second flux stage runs slab by slab while the finished slabs are converted to
+ * the (5, ngrid) layout and copied back.  cons_in and cons_out may be the same
+ * array; pinned (page-locked) host memory lets the copies run asynchronously.
+ * States the fused path does not take (see bx_upload_conserved; forces, tables)
+ * run the three calls in sequence.  Uses the handle's reference cons array as
+ * staging; returns after the result is in cons_out. */
+int bx_step_host(bx_handle *h, const double *cons_in, double *cons_out, double endtime,
+                 int32_t *ran);
+
 /* Repeat bx_step until time >= endtime or nsteps steps ran. */
 int bx_run(bx_handle *h, double endtime, int64_t nsteps, int64_t *steps_taken);
 

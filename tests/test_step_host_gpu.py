@@ -1,0 +1,121 @@
+"""bx_step_host -- one main-loop iteration on a state held on the host, with the
+copies overlapped with the step -- against the three calls it stands for
+(bx_upload_conserved, bx_step, bx_download of cons) and against the oracle, bit
+for bit: several z slabs, reflective and outflow walls, a 2-D grid, a state the
+fused path rejects (dirty ghosts), steps the velocity limiter redoes, the end
+time, in place and into a second array, pageable and page-locked memory."""
+import numpy as np
+import pytest
+import torch
+
+import oracle as O
+from boxzyhydro_b200 import ic
+from boxzyhydro_b200.hydro import Hydro
+
+from .helpers import small_random_box
+
+pytestmark = pytest.mark.gpu
+
+
+_PINNED = []  # the tensors that own the page-locked buffers
+
+
+def pinned_copy(a):
+    t = torch.empty(a.shape, dtype=torch.float64, pin_memory=True)
+    _PINNED.append(t)
+    out = t.numpy()
+    out[:] = a
+    return out
+
+
+def three_calls(g, cons, endtime=1e300):
+    g.upload_conserved(cons)
+    ran = g.step(endtime)
+    return g.download()[0], ran
+
+
+def oracle_from(st, cons):
+    """The oracle at the state bx_upload_conserved makes of cons: u = m/rho, p
+    from state() with that u."""
+    o = O.Oracle(st.params)
+    gam = st.params.gammafix
+    u = cons[:, 1:4] / cons[:, 0:1]
+    ek = cons[:, 0] * 0.5 * (u[:, 0] * u[:, 0] + u[:, 1] * u[:, 1] + u[:, 2] * u[:, 2])
+    p = np.maximum(cons[:, 4] - ek, st.params.small_eps) * (gam - 1.0)
+    o.set_state(cons, u, p, np.full(len(cons), gam))
+    return o
+
+
+def run_pair(st, nsteps, pinned, in_place, endtime=1e300):
+    ga, gb = Hydro(st.params), Hydro(st.params)
+    c0 = np.ascontiguousarray(st.cons)
+    ca = pinned_copy(c0) if pinned else c0.copy()
+    cb = c0.copy()
+    out = ca if in_place else (pinned_copy(c0) if pinned else np.empty_like(c0))
+    o = oracle_from(st, c0)
+    src = ca
+    for k in range(nsteps):
+        ra = ga.step_host(src, out, endtime)
+        cb, rb = three_calls(gb, cb, endtime)
+        assert ra == rb, f"step {k + 1}: ran {ra} vs {rb}"
+        assert np.array_equal(out, cb), f"step {k + 1}: cons differs from the three calls " \
+            f"(max |d| {np.nanmax(np.abs(out - cb)):.3e}, {int((out != cb).sum())} values)"
+        ka, kb = ga.clock(), gb.clock()
+        for key in ("time", "dt", "dtold", "step"):
+            assert ka[key] == kb[key], f"step {k + 1}: clock {key} {ka[key]!r} vs {kb[key]!r}"
+        assert o.step(endtime) == ra
+        assert np.array_equal(out, o.get_state()[0]), f"step {k + 1}: cons differs from the oracle"
+        assert o.clock()["time"] == ka["time"]
+        if not in_place:
+            src[:] = out
+    return ga, gb
+
+
+def test_turbulent_box_many_slabs_pinned_in_place():
+    st = ic.turbulent_box(n=64, seed=5)
+    ga, _ = run_pair(st, 4, pinned=True, in_place=True)
+    assert ga.status()[1] == 1
+
+
+def test_walls_ragged_pageable_two_arrays():
+    st = small_random_box(nx=37, ny=21, nz=19, walls=(0, 1, 1, 0, 0, 1), seed=21)
+    ga, _ = run_pair(st, 4, pinned=False, in_place=False)
+    assert ga.status()[1] == 1
+
+
+def test_grid_off_the_fused_path():
+    """Reflective walls on all six sides of a 3-D grid: the fused path does not
+    take it, and the call runs the three calls in sequence."""
+    st = small_random_box(nx=13, ny=12, nz=10, walls=(1,) * 6, seed=2)
+    ga, _ = run_pair(st, 3, pinned=True, in_place=True)
+    assert ga.status()[1] == 0
+
+
+def test_two_dimensional_grid():
+    st = small_random_box(nx=40, ny=30, nz=4, walls=(0, 1, 1, 0, 0, 0), seed=22)
+    run_pair(st, 4, pinned=True, in_place=False)
+
+
+def test_dirty_ghosts_take_the_reference_flow():
+    """Ghost values that are not copies of their donors: the fused path does not
+    take the state, the step runs the per-phase kernels like the three calls."""
+    st = small_random_box(nx=20, ny=18, nz=16, walls=(0,) * 6, seed=23)
+    st.cons[0, 4] *= 1.5  # a corner ghost
+    ga, gb = run_pair(st, 3, pinned=True, in_place=True)
+    sa, sb = ga.status(), gb.status()
+    assert sa == sb
+
+
+def test_velocity_limiter_redo():
+    """|u| > vlimit: the fused step is redone on the per-phase kernels and the
+    copies already made are replaced."""
+    st = small_random_box(nx=16, ny=13, nz=9, walls=(0,) * 6, seed=8, amp=0.6, vlimit=0.55)
+    ga, gb = run_pair(st, 5, pinned=True, in_place=True)
+    sa, sb = ga.status(), gb.status()
+    assert sa[0] & 1 and sa == sb
+
+
+def test_end_time_reached():
+    st = ic.turbulent_box(n=32, seed=6)
+    ga, gb = run_pair(st, 2, pinned=True, in_place=False, endtime=0.0)
+    assert ga.clock()["step"] == 0
