@@ -38,18 +38,21 @@ struct bx_handle {
   long long n_stage = 0;
   long long launches = 0;  // kernels of this library launched on the handle's stream
   double* d_eos = nullptr;  // device copy of the tabulated EOS (H2STAT >= 0)
-  // bx_step_host: the tiles on the host, the z slabs of the cell range (groups
-  // of tile z-chunks) with their ghost ranges, and the streams and events that
-  // overlap the copies with the step (made on first use)
-  std::vector<bx::Tile> h_tiles;
+  // bx_step_host: its tiles (thin z-chunks), the z slabs of the cell range
+  // (groups of those chunks) with their ghost ranges, and the streams and
+  // events that overlap the copies with the step (made on first use)
+  bx::Tile* d_io_tiles = nullptr;
   struct Slab {
     long long i0, i1;  // cells [i0, i1)
     int g0, g1;        // entries [g0, g1) of the ghost plan
     int t0, nt;        // tiles [t0, t0 + nt)
+    int z0, z1;        // interior-relative z range of the tiles
+    int s0_after, s1_after;  // uploaded slab after which its stage 0 / stage 1 can run
   };
   std::vector<Slab> slabs;
-  cudaStream_t hs[3] = {nullptr, nullptr, nullptr};  // copies, conversions, second stage-1
-  std::vector<cudaEvent_t> hev;
+  // upload copies, download copies, conversions, second stage-1 stream
+  cudaStream_t hs[4] = {nullptr, nullptr, nullptr, nullptr};
+  std::vector<cudaEvent_t> hev;  // start, join, then per slab: in, stage 0, stage 1, converted
   std::string err;
 };
 

@@ -197,6 +197,9 @@ cudaError_t slab_in(const double* aos, double* X, long long ps, long long i0, lo
 cudaError_t slab_out(const Geom& g, const double* X, long long ps, int nsrc, double* aos,
                      long long i0, long long i1, const int32_t* dst, const int32_t* src2,
                      const uint8_t* sgn2, int g0, int g1, cudaStream_t s);
+// Courant rate (as box_rate) of the interior cells of [i0, i1), atomicMax into *bits
+cudaError_t slab_rate(const Geom& g, const double* X, long long ps, long long i0, long long i1,
+                      unsigned long long* bits, cudaStream_t s);
 cudaError_t fill_const(double* a, long long n, double v, cudaStream_t s);
 cudaError_t soa_to_aos(const double* soa, double* aos, long long n, int k, cudaStream_t s);
 

@@ -1320,6 +1320,36 @@ cudaError_t box_check_clean(const Geom& g, const double* X, long long ps, int ng
     k_box_check_ghosts<<<nblk(nghost), PB, 0, s>>>(nghost, dst, src2, sgn2, X, ps, ctrl);
   return cudaGetLastError();
 }
+// the same over the interior cells of [i0, i1), into *bits
+__global__ void k_slab_rate(Geom g, const double* X, long long ps, long long i0, long long i1,
+                            unsigned long long* bits) {
+  const long long i = i0 + blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  double r = 0.0;
+  if (i < i1) {
+    const int x = (int)(i % g.nx), y = (int)((i / g.nx) % g.ny), z = (int)(i / g.sz);
+    if (!is_ghost(g, x, y, z)) {
+      const double d = X[i];
+      const double u1 = X[ps + i] / d, u2 = X[2 * ps + i] / d, u3 = X[3 * ps + i] / d;
+      const double p = eos_pressure(d, X[4 * ps + i], u1, u2, u3, g.gm1, g.small_eps);
+      r = g.pow2 ? courant_rate<true>(d, p, g.gam, u1, u2, u3, g.dx, g.dy, g.dz, g.idx, g.idy, g.idz)
+                 : courant_rate<false>(d, p, g.gam, u1, u2, u3, g.dx, g.dy, g.dz, g.idx, g.idy, g.idz);
+    }
+  }
+  __shared__ double wm[PB / 32];
+  r = warp_max(r);
+  if ((threadIdx.x & 31) == 0) wm[threadIdx.x >> 5] = r;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double m = 0.0;
+    for (int k = 0; k < PB / 32; ++k) m = fmax(m, wm[k]);
+    atomicMax(bits, (unsigned long long)__double_as_longlong(m));
+  }
+}
+cudaError_t slab_rate(const Geom& g, const double* X, long long ps, long long i0, long long i1,
+                      unsigned long long* bits, cudaStream_t s) {
+  if (i1 > i0) k_slab_rate<<<nblk(i1 - i0), PB, 0, s>>>(g, X, ps, i0, i1, bits);
+  return cudaGetLastError();
+}
 cudaError_t box_rate(const Geom& g, const double* X, long long ps, Ctrl* ctrl, cudaStream_t s) {
   k_box_rate<<<nblk(g.ng), PB, 0, s>>>(g, X, ps, ctrl);
   return cudaGetLastError();

@@ -34,27 +34,32 @@ def three_calls(g, cons, endtime=1e300):
     return g.download()[0], ran
 
 
-def oracle_from(st, cons):
-    """The oracle at the state bx_upload_conserved makes of cons: u = m/rho, p
-    from state() with that u."""
-    o = O.Oracle(st.params)
-    gam = st.params.gammafix
+def oracle_set(o, params, cons):
+    """The oracle's arrays at the state bx_upload_conserved makes of cons:
+    u = m/rho, p from state() with that u (the clock is kept)."""
+    gam = params.gammafix
     u = cons[:, 1:4] / cons[:, 0:1]
     ek = cons[:, 0] * 0.5 * (u[:, 0] * u[:, 0] + u[:, 1] * u[:, 1] + u[:, 2] * u[:, 2])
-    p = np.maximum(cons[:, 4] - ek, st.params.small_eps) * (gam - 1.0)
+    p = np.maximum(cons[:, 4] - ek, params.small_eps) * (gam - 1.0)
     o.set_state(cons, u, p, np.full(len(cons), gam))
-    return o
 
 
-def run_pair(st, nsteps, pinned, in_place, endtime=1e300):
+def run_pair(st, nsteps, pinned, in_place, endtime=1e300, modify=None):
+    """Steps through bx_step_host (handle a), the three calls (handle b) and the
+    oracle from the same cons; `modify(k, cons)` changes the host state in place
+    before step k (the same change on all three)."""
     ga, gb = Hydro(st.params), Hydro(st.params)
     c0 = np.ascontiguousarray(st.cons)
     ca = pinned_copy(c0) if pinned else c0.copy()
     cb = c0.copy()
     out = ca if in_place else (pinned_copy(c0) if pinned else np.empty_like(c0))
-    o = oracle_from(st, c0)
+    o = O.Oracle(st.params)
+    oracle_set(o, st.params, c0)
     src = ca
     for k in range(nsteps):
+        if modify is not None and modify(k, src):
+            cb[:] = src
+            oracle_set(o, st.params, src)
         ra = ga.step_host(src, out, endtime)
         cb, rb = three_calls(gb, cb, endtime)
         assert ra == rb, f"step {k + 1}: ran {ra} vs {rb}"
@@ -113,6 +118,27 @@ def test_velocity_limiter_redo():
     ga, gb = run_pair(st, 5, pinned=True, in_place=True)
     sa, sb = ga.status(), gb.status()
     assert sa[0] & 1 and sa == sb
+
+
+def test_host_changes_the_state_between_steps():
+    """The step is started with dt from the rate the device holds for the state
+    it left; a host that changes the state between the calls gets the step of
+    the state it passed (a change of the maximum rate restarts the step, others
+    keep it)."""
+    st = ic.turbulent_box(n=48, seed=7)
+
+    def modify(k, c):
+        if k == 2:  # every momentum: the maximum rate changes
+            c[:, 1:4] *= 1.001
+            return True
+        if k == 4:  # one interior cell's energy, far from the maximum rate
+            i = (st.params.nx * st.params.ny) * 20 + st.params.nx * 20 + 20
+            c[i, 4] *= 1.0 + 1e-9
+            return True
+        return False
+
+    ga, _ = run_pair(st, 6, pinned=True, in_place=True, modify=modify)
+    assert ga.status()[1] == 1
 
 
 def test_end_time_reached():
