@@ -130,6 +130,108 @@ def cpu_sample(st, steps=3, threads=None):
     return cells * steps / dt, threads, dt
 
 
+def physics_arm(args, rank, world, local):
+    """The rows beyond the plain step on the turbulent box: angular-momentum
+    fluxing (fluxangmom, yoffset 0.25), the tabulated EOS (H2STAT >= 0 with
+    synthetic ideal-gas tables of the eos module's layout) and the gravity
+    coupling (a softened point-mass potential handed over from page-locked host
+    memory before every step, its upload and calc_gforce inside the timed
+    region).  All three run on the
+    per-phase kernels.  Device-timed steps and the oracle with the same physics
+    on a bounded sample of the host cores."""
+    import dataclasses
+
+    import numpy as np
+    import torch
+    from boxzyhydro_b200 import grid as G
+    from boxzyhydro_b200 import ic
+    from boxzyhydro_b200.eos_table import synthetic_table
+    from boxzyhydro_b200.hydro import Hydro
+
+    if rank != 0:
+        return 0
+    base = ic.turbulent_box(n=args.n, seed=args.seed)
+    hp0 = base.params
+    cells = hp0.n_active()
+    x, y, z = G.cell_centres(hp0.nx, hp0.ny, hp0.nz, hp0.dx, hp0.dy, hp0.dz)
+    phi = torch.empty(hp0.ngrid, dtype=torch.float64, pin_memory=True).numpy()
+    phi[:] = -0.1 / np.sqrt(x * x + y * y + z * z + 0.01)
+    tab = synthetic_table()
+    variants = {
+        "fluxang": dict(params=dataclasses.replace(hp0, fluxangmom=True, yoffset=0.25)),
+        "eostable": dict(params=dataclasses.replace(hp0, h2stat=1), table=tab),
+        "gravity": dict(params=hp0, phi=phi),
+    }
+    out = {}
+    stream = torch.cuda.Stream()
+    for name, v in variants.items():
+        hp = v["params"]
+        g = Hydro(hp)
+        g.set_stream(stream.cuda_stream)
+        g.upload(base.cons, base.u, base.p)
+        if "table" in v:
+            g.set_eos_table(v["table"])
+
+        def one():
+            if "phi" in v:
+                g.set_phi(v["phi"])
+            g.step()
+
+        for _ in range(args.warmup):
+            one()
+        g.profile(True)
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            one()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        prof = g.profile_read()
+        bits, path = g.status()
+        g.close()
+        rec = {"value": cells * args.steps / (ms * 1e-3), "unit": UNIT,
+               "ms_per_step": ms / args.steps, "steps": args.steps,
+               "path": "fused stage kernels" if path == 1 else "per-phase kernels",
+               "status_bits": bits, "gpu_launches": prof["launches"]}
+        if not args.no_cpu:
+            sys.path.insert(0, os.path.join(ROOT, "oracle"))
+            import oracle as O
+            threads = os.cpu_count()
+            O.set_threads(threads)
+            o = O.Oracle(hp, racy_ghosts=True)
+            if "table" in v:
+                o.set_eos_table(v["table"])
+            o.set_state(base.cons, base.u, base.p, base.adindx)
+
+            def cpu_one():
+                if "phi" in v:
+                    o.set_gforce(o.calc_gforce(v["phi"]))
+                o.step()
+
+            cpu_one()
+            t0 = time.perf_counter()
+            for _ in range(args.cpu_steps):
+                cpu_one()
+            secs = time.perf_counter() - t0
+            o.close()
+            rec["cpu_baseline"] = {
+                "value": cells * args.cpu_steps / secs, "unit": UNIT, "cores": threads,
+                "kind": "port", "sample": f"{args.cpu_steps} steps after one warm-up step "
+                                          f"({secs:.1f} s), oracle/bx_oracle.c, OpenMP"}
+        out[name] = rec
+    line = {"metric": METRIC, "unit": UNIT, "n_gpus": 1, "warmup": args.warmup,
+            "higher_is_better": True, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"turbulent box {args.n}^3 interior, gamma=5/3, CFL 0.4, "
+                                   "outflow walls, with each physics option in turn",
+                       "cells_per_step": cells},
+            "variants": out}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def max_over_ranks(ms, world, device=None):
     """The slowest rank's time (the timing rule for N > 1: every rank takes its
     device time between barriers, the job's time is the maximum)."""
@@ -451,7 +553,7 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=2, dest="cpu_steps")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
-    ap.add_argument("--workload", default="turb", choices=["turb", "batched", "adjoint"])
+    ap.add_argument("--workload", default="turb", choices=["turb", "batched", "adjoint", "physics"])
     ap.add_argument("--snapshots", type=int, default=15)
     ap.add_argument("--fd-dirs", type=int, default=16, dest="fd_dirs")
     ap.add_argument("--adj-ic", default="blob", choices=["blob", "turb"], dest="adj_ic")
@@ -471,6 +573,8 @@ def main():
         return batched_arm(args, rank, world, local)
     if args.workload == "adjoint":
         return adjoint_arm(args, rank, world, local)
+    if args.workload == "physics":
+        return physics_arm(args, rank, world, local)
 
     import numpy as np
     import torch

@@ -67,25 +67,7 @@ def step_both(o, g, nsteps, endtime=1e300, check_every=1):
 
 
 def synthetic_eos_table(neos=40, neos_rho=9, seed=0):
-    """Tables in the layout of the eos module (eos.f90:30-51) for the tabulated
-    state() path: log-spaced specific energies per density row, smooth gamma and
-    mu, and T = (gamma-1) eng mu / R so that p = rho T R / mu = (gamma-1) rho eng
-    at the table points.  Code densities covered: about 0.0017 to 17."""
-    from boxzyhydro_b200 import celldump as CD
-    rng = np.random.default_rng(seed)
-    u = CD.units()
-    D = float(u[CD.UNIT_NAMES.index("density")])
-    R = float(u[CD.UNIT_NAMES.index("rgas")])
-    log_low, drho = -9.0, 0.5
-    j = np.arange(1, neos_rho + 1)
-    i = np.arange(1, neos + 1)[:, None]
-    rho_table = 10.0 ** (log_low + (j - 1) * drho) / D
-    deng = 0.05 + 0.002 * j
-    e0 = 0.1 * (1.0 + 0.1 * j) * rng.uniform(0.9, 1.1, neos_rho)
-    eng = e0[None, :] * 10.0 ** ((i - 1) * deng[None, :])
-    gam = 1.35 + 0.25 * np.sin(0.2 * i + j[None, :])
-    muc = 2.3 - 0.5 * i / neos + 0.01 * j[None, :]
-    tk = (gam - 1.0) * eng * muc / R
-    return dict(neos=neos, neos_rho=neos_rho, log_rho_eos_low=log_low, drho_eos=drho,
-                density_unit=D, tk_bgrnd=1e-6, eng_table2=eng, gamma_table2=gam,
-                muc_table2=muc, tk_table2=tk, rho_table=rho_table, deng_eos_array=deng)
+    """Tables in the layout of the eos module for the tabulated state() path
+    (boxzyhydro_b200.eos_table.synthetic_table)."""
+    from boxzyhydro_b200.eos_table import synthetic_table
+    return synthetic_table(neos, neos_rho, seed)
