@@ -269,11 +269,27 @@ static int bx_adindx_fill(bx_handle* h) {
   return BX_OK;
 }
 
+// the reference arrays of the fused state (p as state() leaves it after a step
+// with a force, whose velocity array is the one of before source(1))
+static int fused_arrays(bx_handle* h) {
+  CK(fused_to_phase(h->g, h->buf[h->cur], h->nsrc, h->pa, h->nghost, h->d_dst, h->d_src2,
+                    h->d_sgn2, h->stream));
+  h->launches += 3;
+  if (h->p_saved) {
+    // no fused step since the planes took the reference arrays: their p stands
+    CK(cudaMemcpyAsync(h->pa.p, h->pa.cons_old + 3 * h->g.ng, h->g.ng * sizeof(double),
+                       cudaMemcpyDeviceToDevice, h->stream));
+  } else if (h->grav_step) {
+    CK(p_after_force(h->g, h->pa, h->pa.cons_old, h->nghost, h->d_dst, h->d_src2, h->stream));
+    h->launches += 2;
+  }
+  return BX_OK;
+}
+
 // make the reference arrays current (from the fused planes if needed)
 static int to_phase(bx_handle* h) {
   if (h->mode == 0) return BX_OK;
-  CK(fused_to_phase(h->g, h->buf[h->cur], h->nsrc, h->pa, h->nghost, h->d_dst, h->d_src2,
-                    h->d_sgn2, h->stream));
+  if (int r = fused_arrays(h)) return r;
   h->mode = 0;
   return BX_OK;
 }
@@ -304,7 +320,7 @@ int bx_upload(bx_handle* h, const double* cons, const double* u, const double* p
   h->mode = 0;
   // a state the fused stages reproduce exactly (as left by a previous step)
   // continues on them; anything else starts on the per-phase kernels
-  if (h->eligible && !h->gforce_set) {
+  if (h->eligible) {
     if (int r = pull_clock(h)) return r;
     h->clock.flags = 0;
     if (int r = push_clock(h)) return r;
@@ -335,7 +351,7 @@ int bx_upload_conserved(bx_handle* h, const double* cons) {
   CK(prims_from_cons(h->g, h->pa, s));
   h->launches += 2;
   h->mode = 0;
-  if (h->eligible && !h->gforce_set) {
+  if (h->eligible) {
     if (int r = pull_clock(h)) return r;
     h->clock.flags = 0;
     if (int r = push_clock(h)) return r;
@@ -355,9 +371,7 @@ int bx_download(bx_handle* h, double* cons, double* u, double* p) {
   const long long n = h->g.ng;
   cudaStream_t s = h->stream;
   if (h->mode == 1) {
-    CK(fused_to_phase(h->g, h->buf[h->cur], h->nsrc, h->pa, h->nghost, h->d_dst, h->d_src2,
-                      h->d_sgn2, s));
-    h->launches += 3;
+    if (int r = fused_arrays(h)) return r;
   }
   double* tmp = staging(h);
   if (cons) {
@@ -469,12 +483,13 @@ int bx_set_gforce(bx_handle* h, const double* gforce) {
   const long long n = h->g.ng;
   if (!gforce) {
     h->gforce_set = false;
+    CK(cudaStreamSynchronize(h->stream));
     cudaFree(h->pa.gforce);
     h->pa.gforce = nullptr;
     return BX_OK;
   }
   if (!h->pa.gforce) CK(dalloc((void**)&h->pa.gforce, 3 * n * sizeof(double)));
-  if (int r = to_phase(h)) return r;
+  // the staging planes hold no state in either form
   double* tmp = staging(h);
   CK(cudaMemcpyAsync(tmp, gforce, 3 * n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CK(aos_to_soa(tmp, h->pa.gforce, n, 3, h->stream));
@@ -525,7 +540,6 @@ int bx_set_phi(bx_handle* h, const double* phi) {
   if (!phi) return bx_set_gforce(h, nullptr);
   const long long n = h->g.ng;
   if (!h->pa.gforce) CK(dalloc((void**)&h->pa.gforce, 3 * n * sizeof(double)));
-  if (int r = to_phase(h)) return r;
   double* tmp = staging(h);
   CK(cudaMemcpyAsync(tmp, phi, n * sizeof(double), cudaMemcpyHostToDevice, h->stream));
   CK(phase_calc_gforce(h->g, tmp, h->pa.gforce, h->stream));
@@ -545,8 +559,7 @@ int bx_status(bx_handle* h, uint32_t* bits, int32_t* last_path) {
 int bx_device_cons(bx_handle* h, double** cons_soa, int64_t* ngrid) {
   CHECK_H();
   if (h->mode == 1)
-    CK(fused_to_phase(h->g, h->buf[h->cur], h->nsrc, h->pa, h->nghost, h->d_dst, h->d_src2,
-                      h->d_sgn2, h->stream));
+    if (int r = fused_arrays(h)) return r;
   CK(cudaStreamSynchronize(h->stream));
   if (cons_soa) *cons_soa = h->pa.cons;
   if (ngrid) *ngrid = h->g.ng;
@@ -605,8 +618,11 @@ static int fused_launch(bx_handle* h) {
   a.ncells_total = h->g.ng;
   a.nsrc = h->nsrc;
   // the velocity array is stale while the state lives in the planes (to_phase
-  // rebuilds it), so it holds the stage-0 velocity here
+  // rebuilds it), so it holds the stage-0 velocity here; cons_old likewise
+  // takes the velocity after flux(1) of a step with a force
   a.U = h->pa.u;
+  a.G = h->gforce_set ? h->pa.gforce : nullptr;
+  a.UC = h->pa.cons_old;
   const bool p2 = h->g.pow2 != 0, t3 = h->g.threed != 0;
   CK(launch_dt(h->d_ctrl, 1, h->stream));
   a.X = h->buf[X];
@@ -629,6 +645,11 @@ static int fused_launch(bx_handle* h) {
 // rate of the next step's state()/courant() is accumulated now.
 static int enter_fused(bx_handle* h) {
   if (int r = bx_adindx_fill(h)) return r;
+  // p of the reference arrays (after a step with a force, state() read a
+  // velocity that m/rho of the planes no longer gives) kept until the next step
+  CK(cudaMemcpyAsync(h->pa.cons_old + 3 * h->g.ng, h->pa.p, h->g.ng * sizeof(double),
+                     cudaMemcpyDeviceToDevice, h->stream));
+  h->p_saved = true;
   CK(cudaMemcpyAsync(h->buf[h->cur], h->pa.cons, 5 * h->g.ng * sizeof(double),
                      cudaMemcpyDeviceToDevice, h->stream));
   CK(phase_state(h->g, h->pa, h->d_ctrl, h->stream));
@@ -637,6 +658,7 @@ static int enter_fused(bx_handle* h) {
   h->launches += 2;
   h->nsrc = 1;
   h->mode = 1;
+  h->grav_step = false;
   return pull_clock(h);
 }
 
@@ -652,8 +674,7 @@ static int phase_path(bx_handle* h, int32_t* ran) {
   h->clock.flags = 0;
   if (int r = push_clock(h)) return r;
   if (f & kFlagNonFinite) return set_err(h, BX_ERR_STATE, "non-finite state produced by the step");
-  if (h->eligible && !h->gforce_set && !(f & (kFlagVlimit | kFlagLowRho)))
-    return enter_fused(h);
+  if (h->eligible && !(f & (kFlagVlimit | kFlagLowRho))) return enter_fused(h);
   return BX_OK;
 }
 
@@ -677,7 +698,10 @@ static int after_fused(bx_handle* h, const Ctrl& before, int32_t* ran, bool time
   }
   if (!(f & (kFlagVlimit | kFlagLowRho))) {
     h->cur = (h->cur + 2) % 3;
-    h->nsrc = 2;
+    // with a force the step's last source is applied in stage 1
+    h->grav_step = h->gforce_set;
+    h->p_saved = false;
+    h->nsrc = h->gforce_set ? 1 : 2;
     h->clock.flags = 0;
     if (int r = push_clock(h)) return r;
     h->last_path = 1;
@@ -699,9 +723,6 @@ int bx_step(bx_handle* h, double endtime, int32_t* ran) {
   if (ran) *ran = 0;
   if (h->g.tab && !h->pa.muc)
     return set_err(h, BX_ERR_STATE, "H2STAT >= 0: bx_set_eos_table must come first");
-  if (h->gforce_set && h->mode == 1) {
-    if (int r = to_phase(h)) return r;
-  }
   if (!(h->clock.time < endtime) || h->clock.step >= 1000000) return BX_OK;
   if (h->clock.endtime != endtime) {
     h->clock.endtime = endtime;
@@ -913,6 +934,8 @@ int bx_step_host(bx_handle* h, const double* cons_in, double* cons_out, double e
   const bool spec = runs && h->clock.rate_bits != 0;
   // the uploaded state is one step boundary of the reference: sources short by one
   h->nsrc = 1;
+  h->grav_step = false;
+  h->p_saved = false;
   h->clock.endtime = endtime;
   h->clock.flags = 0;
   h->clock.rate_bits0 = 0;
@@ -1008,6 +1031,8 @@ int bx_handle_adopt_fused(bx_handle* h, const double* planes, long long ps, int 
                        cudaMemcpyDeviceToDevice, h->stream));
   h->nsrc = nsrc;
   h->mode = 1;
+  h->grav_step = false;
+  h->p_saved = false;
   h->clock = clock;
   h->clock.flags = 0;
   h->clock.active = 0;

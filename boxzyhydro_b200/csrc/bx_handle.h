@@ -27,6 +27,12 @@ struct bx_handle {
   bx::Ctrl* h_ctrl = nullptr;  // pinned mirror
   bx::Ctrl clock{};            // host copy of the clock after the last completed call
   int mode = 0;            // 0 = reference arrays current, 1 = fused planes current
+  // the last fused step had a force: the planes hold the state after source(1)
+  // (nsrc 1) and pa.cons_old the velocity after flux(1) that state() reads
+  bool grav_step = false;
+  // the planes took the reference arrays and no fused step ran since: their p
+  // (kept in pa.cons_old's fourth plane) is the one to give back
+  bool p_saved = false;
   bool eligible = false;
   bool gforce_set = false;
   uint32_t status = 0;

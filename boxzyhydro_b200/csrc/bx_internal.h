@@ -118,6 +118,9 @@ struct StageArgs {
   double* out;       // stage output planes (interior cells written)
   double* U;         // 3 planes: stage 0 writes m/rho of the step input at its own
                      // cells, stage 1 reads it as the stale velocity of its EOS
+  const double* G;   // 3 planes of the gravitational acceleration, or null (no force)
+  double* UC;        // with G: stage 1 writes the velocity after flux(1) of its
+                     // own cells (the velocity state() reads at the step's end)
   Ctrl* ctrl;        // per box control blocks
   const Geom* geom;  // per box geometry (device)
   const Tile* tiles;
@@ -189,6 +192,10 @@ cudaError_t check_clean(const Geom& g, const PhaseArrays& a, int nghost, const i
 // AoS host layout <-> SoA device layout
 cudaError_t aos_to_soa(const double* aos, double* soa, long long n, int k, cudaStream_t s);
 cudaError_t prims_from_cons(const Geom& g, PhaseArrays& a, cudaStream_t s);
+// after fused_to_phase of a step with a force: the pressure from the cons and
+// the velocity after flux(1) (uc, 3 planes of interior cells), ghosts as donors
+cudaError_t p_after_force(const Geom& g, PhaseArrays& a, const double* uc, int nghost,
+                          const int32_t* dst, const int32_t* src2, cudaStream_t s);
 // host-overlapped step: AoS slab [i0, i1) -> planes; planes -> AoS reference cons
 // of the slab (interior cells nsrc sources short, then the ghosts [g0, g1) of
 // the resolved plan, whose donors lie in this slab or an earlier one)

@@ -83,6 +83,26 @@ __device__ __forceinline__ void load_u(const double* U, long long PS, const Geom
   if (fz) u3 = -u3;
 }
 
+// the gravitational acceleration at a cell: the donor's for a ghost coordinate,
+// reflected components negated like the momenta (the source update is exact
+// under reflecting m and g together)
+__device__ __forceinline__ void load_g(const double* G, long long PS, const Geom& g, int x, int y,
+                                       int z, double& g1, double& g2, double& g3) {
+  load_u(G, PS, g, x, y, z, g1, g2, g3);
+}
+
+// source(0) with gravity on conserved values c (source.f90:161-182 with dt/2):
+// the velocity array it reads is m/rho before the kick (the last velocity() ran
+// on these momenta); returns that velocity in (v1, v2, v3) for state()
+__device__ __forceinline__ void gravity_source0(Cons& c, double g1, double g2, double g3,
+                                                double dth, double small_eps, double& v1,
+                                                double& v2, double& v3) {
+  v1 = c.m1 / c.d;
+  v2 = c.m2 / c.d;
+  v3 = c.m3 / c.d;
+  source_gravity(c.d, c.m1, c.m2, c.m3, c.E, g1, g2, g3, v1, v2, v3, dth, small_eps);
+}
+
 __device__ __forceinline__ void apply_sources(Cons& c, int nsrc, double small_eps) {
   for (int k = 0; k < nsrc; ++k) c.E = source_energy(c.d, c.m1, c.m2, c.m3, c.E, small_eps);
 }
@@ -94,12 +114,29 @@ __device__ __forceinline__ void apply_sources(Cons& c, int nsrc, double small_ep
 //  stage 1: cons = Y; u = m/rho of Y (velocity at main.f90:355); p from state()
 //           with the stage-0 velocity m0/rho0 (main.f90:353 uses the stale u),
 //           which stage 0 stored in U (the same quotient, so the same bits).
-template <int STAGE>
+//  GRAV (a gravitational force this step): stage 0 takes the nsrc-1 force-free
+//           sources still pending, then source(0) with the force, which kicks
+//           the momenta; state() then reads the velocity array of before the
+//           kick (main.f90:318-319 call state() before velocity()).
+template <int STAGE, bool GRAV = false>
 __device__ __forceinline__ Prim load_prim(const StageArgs& a, const Geom& g, int x, int y, int z,
-                                          unsigned& flags, int nsrc, bool need_c = true) {
+                                          unsigned& flags, int nsrc, double dth,
+                                          bool need_c = true) {
   const long long PS = a.ncells_total;
   Prim q;
-  if (STAGE == 0) {
+  if (STAGE == 0 && GRAV) {
+    Cons c = load_cons(a.X, PS, g, x, y, z);
+    double g1, g2, g3, v1, v2, v3;
+    load_g(a.G, PS, g, x, y, z, g1, g2, g3);
+    apply_sources(c, nsrc - 1, g.small_eps);
+    gravity_source0(c, g1, g2, g3, dth, g.small_eps, v1, v2, v3);
+    q.d = c.d;
+    q.u1 = c.m1 / c.d;
+    q.u2 = c.m2 / c.d;
+    q.u3 = c.m3 / c.d;
+    q.e = recon_eps(q.d, c.E, q.u1, q.u2, q.u3, g.small_eps);
+    q.p = eos_pressure(q.d, c.E, v1, v2, v3, g.gm1, g.small_eps);
+  } else if (STAGE == 0) {
     Cons c = load_cons(a.X, PS, g, x, y, z);
     apply_sources(c, nsrc, g.small_eps);
     q.d = c.d;
@@ -204,7 +241,7 @@ __device__ __forceinline__ double warp_max(double v) {
 // ------------------------------------------------------------------ stage kernel
 // One tile of one stage.  FULL: the tile is a whole TX x TY block of interior
 // columns, so its extents are compile-time constants.
-template <int STAGE, bool POW2, bool THREED, bool FULL>
+template <int STAGE, bool POW2, bool THREED, bool FULL, bool GRAV>
 __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, const Geom& g,
                                            Ctrl* C, double* sm, double* red_rate,
                                            unsigned* red_flags) {
@@ -215,6 +252,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
   double* FY = sm + 5 * NFX;          // [5][TY+1][TX] y face fluxes
   double* ZS = SY + 12 * NSY;         // [16][NT]: Fzm 0-4, Fzp 5-9, plus state 10-15
   const double dt = C->dt;
+  const double dth = dt * kHalf;  // the sources' half step (main.f90:282,471)
   const int nsrc = a.nsrc > 0 ? a.nsrc : C->nsrc;
 
   const int tid = threadIdx.x;
@@ -239,10 +277,10 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
 
   const int z0 = g.az0 + t.z0, z1 = g.az0 + t.z1;
   if (THREED && own) {
-    const Prim Pm2 = load_prim<STAGE>(a, g, gx, gy, z0 - 2, flags, nsrc);
-    const Prim Pm1 = load_prim<STAGE>(a, g, gx, gy, z0 - 1, flags, nsrc);
-    Pk = load_prim<STAGE>(a, g, gx, gy, z0, flags, nsrc);
-    Pk1 = load_prim<STAGE>(a, g, gx, gy, z0 + 1, flags, nsrc);
+    const Prim Pm2 = load_prim<STAGE, GRAV>(a, g, gx, gy, z0 - 2, flags, nsrc, dth);
+    const Prim Pm1 = load_prim<STAGE, GRAV>(a, g, gx, gy, z0 - 1, flags, nsrc, dth);
+    Pk = load_prim<STAGE, GRAV>(a, g, gx, gy, z0, flags, nsrc, dth);
+    Pk1 = load_prim<STAGE, GRAV>(a, g, gx, gy, z0 + 1, flags, nsrc, dth);
     FaceState mm, pm, m0;
     if (z0 - 1 < g.az0) {
       ghost_states(Pm1, mm, pm);
@@ -264,9 +302,9 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
     FaceState mz1, pz1;
     if (own) {
       if (THREED) {
-        P2 = load_prim<STAGE>(a, g, gx, gy, z + 2, flags, nsrc);
+        P2 = load_prim<STAGE, GRAV>(a, g, gx, gy, z + 2, flags, nsrc, dth);
       } else {
-        Pk = load_prim<STAGE>(a, g, gx, gy, z, flags, nsrc);
+        Pk = load_prim<STAGE, GRAV>(a, g, gx, gy, z, flags, nsrc, dth);
       }
       put_prim(SP, (ty + 2) * PW + (tx + 2), Pk);
       if (STAGE == 0) {
@@ -294,7 +332,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
       const int fx = bx0 + cx, fy = by0 + cy;
       const bool near = cx >= -1 && cx <= w && cy >= -1 && cy <= h;
       const bool inner = fx >= g.ax0 && fx < g.ax1 && fy >= g.ay0 && fy < g.ay1;
-      const Prim q = load_prim<STAGE>(a, g, fx, fy, z, flags, nsrc, near && inner);
+      const Prim q = load_prim<STAGE, GRAV>(a, g, fx, fy, z, flags, nsrc, dth, near && inner);
       put_prim(SP, (cy + 2) * PW + (cx + 2), q);
     }
     if (THREED && own) {
@@ -385,7 +423,15 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         ft[q] = POW2 ? -sum * dt * g.ivol : cdiv(-sum * dt, g.vol, g.ivol);
       }
       Cons c0 = load_cons(a.X, PS, g, gx, gy, z);
-      apply_sources(c0, nsrc, g.small_eps);
+      double go1 = 0.0, go2 = 0.0, go3 = 0.0;  // the own cell's acceleration
+      if (GRAV) {
+        load_g(a.G, PS, g, gx, gy, z, go1, go2, go3);
+        double v1, v2, v3;
+        apply_sources(c0, nsrc - 1, g.small_eps);
+        gravity_source0(c0, go1, go2, go3, dth, g.small_eps, v1, v2, v3);
+      } else {
+        apply_sources(c0, nsrc, g.small_eps);
+      }
       double n[5];
       if (STAGE == 0) {
         n[0] = c0.d + ft[0];
@@ -411,13 +457,36 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         if (n[0] < kLowRho) flags |= kFlagLowRho;
         if (fabs(u1) > g.vlimit || fabs(u2) > g.vlimit || fabs(u3) > g.vlimit)
           flags |= kFlagVlimit;
-        // source(1) energy, then the Courant rate of the next step (courant.f90:173-175)
-        const double E3 = source_energy(n[0], n[1], n[2], n[3], n[4], g.small_eps);
-        const double pA = eos_pressure(n[0], E3, u1, u2, u3, g.gm1, g.small_eps);
-        const double r0 = courant_rate<POW2>(n[0], pA, g.gam, u1, u2, u3, g.dx, g.dy, g.dz,
-                                             g.idx, g.idy, g.idz);
-        rate = fmax(rate, r0);
-        if (!(r0 >= 0.0)) flags |= kFlagNonFinite;
+        if (GRAV) {
+          // source(1) with the force (main.f90:471): the planes take its result,
+          // the velocity it read goes to UC for state() at the step's end
+          // (main.f90:513-514), and the Courant rate of the next step is taken
+          // with the velocity after it (main.f90:515)
+          const long long o = g.base + gx + (long long)gy * g.sy + (long long)z * g.sz;
+          a.UC[o] = u1;
+          a.UC[PS + o] = u2;
+          a.UC[2 * PS + o] = u3;
+          source_gravity(n[0], n[1], n[2], n[3], n[4], go1, go2, go3, u1, u2, u3, dth,
+                         g.small_eps);
+          const double w1 = n[1] / n[0], w2 = n[2] / n[0], w3 = n[3] / n[0];
+          if (fabs(w1) > g.vlimit || fabs(w2) > g.vlimit || fabs(w3) > g.vlimit)
+            flags |= kFlagVlimit;
+          if (!(isfinite(n[1]) && isfinite(n[2]) && isfinite(n[3]) && isfinite(n[4])))
+            flags |= kFlagNonFinite;
+          const double pA = eos_pressure(n[0], n[4], w1, w2, w3, g.gm1, g.small_eps);
+          const double r0 = courant_rate<POW2>(n[0], pA, g.gam, w1, w2, w3, g.dx, g.dy, g.dz,
+                                               g.idx, g.idy, g.idz);
+          rate = fmax(rate, r0);
+          if (!(r0 >= 0.0)) flags |= kFlagNonFinite;
+        } else {
+          // source(1) energy, then the Courant rate of the next step (courant.f90:173-175)
+          const double E3 = source_energy(n[0], n[1], n[2], n[3], n[4], g.small_eps);
+          const double pA = eos_pressure(n[0], E3, u1, u2, u3, g.gm1, g.small_eps);
+          const double r0 = courant_rate<POW2>(n[0], pA, g.gam, u1, u2, u3, g.dx, g.dy, g.dz,
+                                               g.idx, g.idy, g.idz);
+          rate = fmax(rate, r0);
+          if (!(r0 >= 0.0)) flags |= kFlagNonFinite;
+        }
       }
       const long long o = g.base + gx + (long long)gy * g.sy + (long long)z * g.sz;
 #pragma unroll
@@ -455,7 +524,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
 // PM: 1 = every box of the launch has power-of-two spacings (divisions by the
 // cell sizes are multiplications by exact reciprocals), 0 = otherwise (cdiv,
 // exact for any spacing)
-template <int STAGE, int PM, bool THREED>
+template <int STAGE, int PM, bool THREED, bool GRAV = false>
 __global__ void __launch_bounds__(NT, 65536 / (NT * 128)) k_stage(StageArgs a) {
   extern __shared__ double sm[];
   __shared__ Geom sg;
@@ -469,39 +538,47 @@ __global__ void __launch_bounds__(NT, 65536 / (NT * 128)) k_stage(StageArgs a) {
   const bool full = (t.x0 + TX <= sg.ax1 - sg.ax0) && (t.y0 + TY <= sg.ay1 - sg.ay0);
   if (PM == 1) {
     if (full)
-      stage_tile<STAGE, true, THREED, true>(a, t, sg, C, sm, red_rate, red_flags);
+      stage_tile<STAGE, true, THREED, true, GRAV>(a, t, sg, C, sm, red_rate, red_flags);
     else
-      stage_tile<STAGE, true, THREED, false>(a, t, sg, C, sm, red_rate, red_flags);
+      stage_tile<STAGE, true, THREED, false, GRAV>(a, t, sg, C, sm, red_rate, red_flags);
   } else {
     if (full)
-      stage_tile<STAGE, false, THREED, true>(a, t, sg, C, sm, red_rate, red_flags);
+      stage_tile<STAGE, false, THREED, true, GRAV>(a, t, sg, C, sm, red_rate, red_flags);
     else
-      stage_tile<STAGE, false, THREED, false>(a, t, sg, C, sm, red_rate, red_flags);
+      stage_tile<STAGE, false, THREED, false, GRAV>(a, t, sg, C, sm, red_rate, red_flags);
   }
 }
 
-template <int STAGE, int PM, bool THREED>
+template <int STAGE, int PM, bool THREED, bool GRAV>
 static cudaError_t launch_stage_t(const StageArgs& a, int ntiles, cudaStream_t s) {
   const size_t smem = SMEM_DOUBLES * sizeof(double);
   static bool attr_set = false;
   if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(k_stage<STAGE, PM, THREED>,
+    cudaError_t e = cudaFuncSetAttribute(k_stage<STAGE, PM, THREED, GRAV>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     attr_set = true;
   }
   if (ntiles <= 0) return cudaSuccess;
-  k_stage<STAGE, PM, THREED><<<ntiles, NT, smem, s>>>(a);
+  k_stage<STAGE, PM, THREED, GRAV><<<ntiles, NT, smem, s>>>(a);
   return cudaGetLastError();
 }
 
+template <int STAGE, bool GRAV>
+static cudaError_t launch_stage_g(int pm, bool threed, const StageArgs& a, int ntiles,
+                                  cudaStream_t s) {
+  if (pm == 1) return threed ? launch_stage_t<STAGE, 1, true, GRAV>(a, ntiles, s)
+                             : launch_stage_t<STAGE, 1, false, GRAV>(a, ntiles, s);
+  return threed ? launch_stage_t<STAGE, 0, true, GRAV>(a, ntiles, s)
+                : launch_stage_t<STAGE, 0, false, GRAV>(a, ntiles, s);
+}
+
+// a.G set: the step has a gravitational force (instances with the force terms)
 template <int STAGE>
 static cudaError_t launch_stage_s(int pm, bool threed, const StageArgs& a, int ntiles,
                                   cudaStream_t s) {
-  if (pm == 1) return threed ? launch_stage_t<STAGE, 1, true>(a, ntiles, s)
-                             : launch_stage_t<STAGE, 1, false>(a, ntiles, s);
-  return threed ? launch_stage_t<STAGE, 0, true>(a, ntiles, s)
-                : launch_stage_t<STAGE, 0, false>(a, ntiles, s);
+  return a.G ? launch_stage_g<STAGE, true>(pm, threed, a, ntiles, s)
+             : launch_stage_g<STAGE, false>(pm, threed, a, ntiles, s);
 }
 
 // pm: 1 every box has power-of-two spacings, 0 otherwise
@@ -1064,6 +1141,23 @@ __global__ void k_fill_resolved(int nghost, const int32_t* dst, const int32_t* s
   cons[3 * n + d] = (m & 4) ? -cons[3 * n + s] : cons[3 * n + s];
   cons[4 * n + d] = cons[4 * n + s];
 }
+// the pressure state() leaves at the end of a step with a force (main.f90:513):
+// from the cons after source(1) and the velocity array of before it (UC, the
+// velocity after flux(1)), a ghost's as its donor's (|u| is the same)
+__global__ void k_p_from_uc(Geom g, PhaseArrays a, const double* uc) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= g.ng) return;
+  const int x = (int)(i % g.nx), y = (int)((i / g.nx) % g.ny), z = (int)(i / g.sz);
+  if (is_ghost(g, x, y, z)) return;
+  const long long n = g.ng;
+  a.p[i] = eos_pressure(a.cons[i], a.cons[4 * n + i], uc[i], uc[n + i], uc[2 * n + i], g.gm1,
+                        g.small_eps);
+}
+__global__ void k_p_ghosts(int nghost, const int32_t* dst, const int32_t* src, double* p) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < nghost) p[dst[k]] = p[src[k]];
+}
+
 // Host-overlapped step: z slabs of a cell range [i0, i1) between the reference's
 // AoS layout (5 doubles per cell, as on the host) and the fused planes X.
 __global__ void k_slab_in(const double* aos, double* X, long long ps, long long i0, long long i1) {
@@ -1228,6 +1322,12 @@ cudaError_t fused_to_phase(const Geom& g, const double* X, int nsrc, PhaseArrays
 __global__ void k_fill_const(double* a, long long n, double v) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i < n) a[i] = v;
+}
+cudaError_t p_after_force(const Geom& g, PhaseArrays& a, const double* uc, int nghost,
+                          const int32_t* dst, const int32_t* src2, cudaStream_t s) {
+  k_p_from_uc<<<nblk(g.ng), PB, 0, s>>>(g, a, uc);
+  if (nghost > 0) k_p_ghosts<<<nblk(nghost), PB, 0, s>>>(nghost, dst, src2, a.p);
+  return cudaGetLastError();
 }
 cudaError_t slab_in(const double* aos, double* X, long long ps, long long i0, long long i1,
                     cudaStream_t s) {
