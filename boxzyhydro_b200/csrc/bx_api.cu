@@ -850,7 +850,12 @@ static int host_io_enqueue(bx_handle* h, const double* cons_in, double* cons_out
   a.ncells_total = n;
   a.nsrc = h->nsrc;
   a.U = h->pa.u;
+  a.G = h->gforce_set ? h->pa.gforce : nullptr;
+  a.UC = h->pa.cons_old;
   a.X = X;
+  // the reference cons after the step: stage 1 applied source(1) itself when
+  // the step has a force, else it is one force-free source short
+  const int nsrc_out = h->gforce_set ? 1 : 2;
   int st1 = 0;  // stage-1 launches so far (alternating streams)
   for (int k = 0; k < ns; ++k) {
     const bx_handle::Slab& sk = h->slabs[k];
@@ -886,8 +891,8 @@ static int host_io_enqueue(bx_handle* h, const double* cons_in, double* cons_out
       CK(launch_stage(1, p2, t3, aj, sl.nt, sj));
       CK(cudaEventRecord(ev_st1[j], sj));
       CK(cudaStreamWaitEvent(cs, ev_st1[j], 0));
-      CK(slab_out(g, h->buf[Zi], n, 2, aos, sl.i0, sl.i1, h->d_dst, h->d_src2, h->d_sgn2, sl.g0,
-                  sl.g1, cs));
+      CK(slab_out(g, h->buf[Zi], n, nsrc_out, aos, sl.i0, sl.i1, h->d_dst, h->d_src2, h->d_sgn2,
+                  sl.g0, sl.g1, cs));
       CK(cudaEventRecord(ev_cv[j], cs));
       CK(cudaStreamWaitEvent(down, ev_cv[j], 0));
       CK(cudaMemcpyAsync(cons_out + 5 * sl.i0, aos + 5 * sl.i0, (sl.i1 - sl.i0) * cell,
@@ -919,7 +924,7 @@ int bx_step_host(bx_handle* h, const double* cons_in, double* cons_out, double e
   if (ran) *ran = 0;
   if (!cons_in || !cons_out) return set_err(h, BX_ERR_ARG, "cons_in and cons_out are required");
   if (!h->pa.cons) return set_err(h, BX_ERR_STATE, "the handle holds no state (lean handle)");
-  if (!h->eligible || h->gforce_set || h->g.tab) {
+  if (!h->eligible || h->g.tab) {
     // not on the fused path: the three calls it stands for
     if (int r = bx_upload_conserved(h, cons_in)) return r;
     if (int r = bx_step(h, endtime, ran)) return r;

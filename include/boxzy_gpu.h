@@ -17,10 +17,10 @@
  *    arrays directly (assumed-size dummies of a bind(c) interface).
  *  - Calls on one handle are single-threaded (outside OpenMP parallel regions or
  *    under !$OMP MASTER).  Each handle owns one CUDA stream unless one is given.
- *  - Grids with the fixed-gamma EOS (H2STAT=-1), Cartesian fluxing and a zero
- *    or no gravitational force step on the fused stage kernels; the tabulated
- *    EOS (H2STAT>=0, bx_set_eos_table), angular-momentum fluxing
- *    (fluxangmom=1) and a force (bx_set_gforce, bx_set_phi) step on the
+ *  - Grids with the fixed-gamma EOS (H2STAT=-1) and Cartesian fluxing step on
+ *    the fused stage kernels, with or without a gravitational force
+ *    (bx_set_gforce, bx_set_phi); the tabulated EOS (H2STAT>=0,
+ *    bx_set_eos_table) and angular-momentum fluxing (fluxangmom=1) step on the
  *    per-phase kernels, with the same results as the reference's subroutines.
  */
 #ifndef BOXZY_GPU_H
@@ -91,12 +91,14 @@ int bx_set_stream(bx_handle *h, void *cuda_stream);
 int bx_upload(bx_handle *h, const double *cons, const double *u, const double *p);
 
 /* Upload a state at a step boundary from the conserved variables alone: u is set
- * to m/rho (the loop body ends with state() and velocity(), main.f90:513-515;
- * with no force the last source() left m unchanged) and p to the
- * pressure state() gives with it, which is what the reference holds there when
- * no cell lies below rho = 1e-4 (the low-density branch of state.f90:50-55 keeps
- * a p that cons does not determine: use bx_upload for such states).  Moves 40
- * bytes per cell instead of 72.  Fixed-gamma grids only. */
+ * to m/rho (the loop body ends with state() and velocity(), main.f90:513-515)
+ * and p to the pressure state() gives with it, which is what the reference
+ * holds there when no force acted and no cell lies below rho = 1e-4 (the
+ * low-density branch of state.f90:50-55 keeps a p that cons does not
+ * determine: use bx_upload for such states; after a step with a force the
+ * reference's p used the velocity of before source(1) -- the next step
+ * recomputes p before reading it either way).  Moves 40 bytes per cell instead
+ * of 72.  Fixed-gamma grids only. */
 int bx_upload_conserved(bx_handle *h, const double *cons);
 
 /* Copy the state arrays out (what write_files.f90:55-63 writes after state()).
@@ -120,8 +122,9 @@ int bx_step(bx_handle *h, double endtime, int32_t *ran);
  * second flux stage runs slab by slab while the finished slabs are converted to
  * the (5, ngrid) layout and copied back.  cons_in and cons_out may be the same
  * array; pinned (page-locked) host memory lets the copies run asynchronously.
- * States the fused path does not take (see bx_upload_conserved; forces, tables)
- * run the three calls in sequence.  Uses the handle's reference cons array as
+ * A force set with bx_set_phi or bx_set_gforce applies to the step.  States the
+ * fused path does not take (see bx_upload_conserved; tabulated EOS) run the
+ * three calls in sequence.  Uses the handle's reference cons array as
  * staging; returns after the result is in cons_out. */
 int bx_step_host(bx_handle *h, const double *cons_in, double *cons_out, double endtime,
                  int32_t *ran);
@@ -186,7 +189,8 @@ int bx_set_gforce(bx_handle *h, const double *gforce);
  * under USEPOTENTIAL): phi(ngrid) from the host's solver, turned into gforce on the
  * device by calc_gforce (utils.f90:549-571, central differences on interior cells).
  * Call it whenever the solver updates phi (each step); NULL removes the force.
- * Steps with a force run the per-phase kernels. */
+ * Both sources of the next step apply the force; grids the fused path takes run
+ * it in the stage kernels. */
 int bx_set_phi(bx_handle *h, const double *phi);
 
 /* Status bits accumulated since the last call (BX_STATUS_*) and the path the

@@ -9,6 +9,7 @@ import pytest
 import torch
 
 import oracle as O
+from boxzyhydro_b200 import grid as G
 from boxzyhydro_b200 import ic
 from boxzyhydro_b200.hydro import Hydro
 
@@ -44,10 +45,11 @@ def oracle_set(o, params, cons):
     o.set_state(cons, u, p, np.full(len(cons), gam))
 
 
-def run_pair(st, nsteps, pinned, in_place, endtime=1e300, modify=None):
+def run_pair(st, nsteps, pinned, in_place, endtime=1e300, modify=None, phi=None):
     """Steps through bx_step_host (handle a), the three calls (handle b) and the
     oracle from the same cons; `modify(k, cons)` changes the host state in place
-    before step k (the same change on all three)."""
+    before step k (the same change on all three); `phi(k)` gives the potential
+    of step k (or None: no force)."""
     ga, gb = Hydro(st.params), Hydro(st.params)
     c0 = np.ascontiguousarray(st.cons)
     ca = pinned_copy(c0) if pinned else c0.copy()
@@ -60,6 +62,11 @@ def run_pair(st, nsteps, pinned, in_place, endtime=1e300, modify=None):
         if modify is not None and modify(k, src):
             cb[:] = src
             oracle_set(o, st.params, src)
+        if phi is not None:
+            ph = phi(k)
+            ga.set_phi(ph)
+            gb.set_phi(ph)
+            o.set_gforce(None if ph is None else o.calc_gforce(ph))
         ra = ga.step_host(src, out, endtime)
         cb, rb = three_calls(gb, cb, endtime)
         assert ra == rb, f"step {k + 1}: ran {ra} vs {rb}"
@@ -138,6 +145,22 @@ def test_host_changes_the_state_between_steps():
         return False
 
     ga, _ = run_pair(st, 6, pinned=True, in_place=True, modify=modify)
+    assert ga.status()[1] == 1
+
+
+def test_potential_from_the_host():
+    """A potential from the host's solver before every step (a point mass that
+    moves, off for one step): the force terms of the stage kernels."""
+    st = ic.turbulent_box(n=48, seed=9)
+    hp = st.params
+    x, y, z = G.cell_centres(hp.nx, hp.ny, hp.nz, hp.dx, hp.dy, hp.dz)
+
+    def phi(k):
+        if k == 3:
+            return None
+        return -0.05 / np.sqrt((x - 0.02 * k) ** 2 + y * y + z * z + 0.02)
+
+    ga, _ = run_pair(st, 6, pinned=True, in_place=True, phi=phi)
     assert ga.status()[1] == 1
 
 
