@@ -258,7 +258,7 @@ static int push_clock(bx_handle* h) {
 
 static int ensure_states(bx_handle* h) {
   if (!h->pa.states)
-    CK(dalloc((void**)&h->pa.states, (h->g.ang ? 54 : 42) * h->g.ng * sizeof(double)));
+    CK(dalloc((void**)&h->pa.states, (h->g.ang ? 54 : 57) * h->g.ng * sizeof(double)));
   return BX_OK;
 }
 

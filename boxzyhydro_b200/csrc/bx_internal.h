@@ -150,7 +150,8 @@ struct PhaseArrays {
   double* p;        // ng
   double* adindx;   // ng
   double* gforce;   // 3*ng or null (zero force)
-  double* states;   // 42*ng scratch for flux
+  double* states;   // flux scratch: 42*ng face states, then 15*ng face fluxes
+                    // (fixed frame); 54*ng face states with fluxangmom
   double* gtmp;     // 5*nghost scratch for the ghost fill
   double* muc;      // ng (H2STAT >= 0: muc_array of state(); else null)
   EosDev eos;       // valid when muc is set

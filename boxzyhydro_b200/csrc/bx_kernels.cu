@@ -1075,8 +1075,17 @@ __global__ void k_phase_update(Geom g, PhaseArrays a, Ctrl* ctrl, int avg) {
     const long long st[3] = {1, g.sy, g.threed ? g.sz : 0};
     double fm[3][5], fp[3][5];
     for (int dir = 0; dir < 3; ++dir) {
-      phase_face<ANG>(a.states, n, dir, i - st[dir], i, cx, cy, cr, fm[dir]);
-      phase_face<ANG>(a.states, n, dir, i, i + st[dir], cx, cy, cr, fp[dir]);
+      if (ANG) {
+        // the pressure terms depend on the updated cell: both faces here
+        phase_face<ANG>(a.states, n, dir, i - st[dir], i, cx, cy, cr, fm[dir]);
+        phase_face<ANG>(a.states, n, dir, i, i + st[dir], cx, cy, cr, fp[dir]);
+      } else {
+        const double* F = a.states + 42 * n;  // k_phase_faces
+        for (int k = 0; k < 5; ++k) {
+          fm[dir][k] = F[(dir * 5 + k) * n + i - st[dir]];
+          fp[dir][k] = F[(dir * 5 + k) * n + i];
+        }
+      }
     }
     for (int k = 0; k < 5; ++k)
       ft[k] = -(g.ayz * (fp[0][k] - fm[0][k]) + g.axz * (fp[1][k] - fm[1][k]) +
@@ -1106,6 +1115,22 @@ __global__ void k_phase_update(Geom g, PhaseArrays a, Ctrl* ctrl, int avg) {
     if (!isfinite(v[k])) bad = true;
   }
   if (bad) atomicOr(&ctrl->flags, (unsigned)kFlagNonFinite);
+}
+
+// HLL flux of every face once (fixed frame): F[dir][i] = flux through the face
+// between cells i and i + stride(dir), from the face states; without z ghosts
+// (nz < 6) the z "face" is the cell with itself, as the update reads it
+__global__ void k_phase_faces(Geom g, PhaseArrays a, double* F) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= g.ng) return;
+  const long long n = g.ng;
+  const long long st[3] = {1, g.sy, g.threed ? g.sz : 0};
+  for (int dir = 0; dir < 3; ++dir) {
+    if (i + st[dir] >= n) continue;
+    double f[5];
+    phase_face<false>(a.states, n, dir, i, i + st[dir], 0.0, 0.0, 0.0, f);
+    for (int k = 0; k < 5; ++k) F[(dir * 5 + k) * n + i] = f[k];
+  }
 }
 
 __global__ void k_copy5(const double* src, double* dst, long long n) {
@@ -1302,6 +1327,7 @@ cudaError_t phase_flux(const Geom& g, PhaseArrays& a, Ctrl* ctrl, int avg, cudaS
     k_phase_update<true><<<nblk(g.ng), PB, 0, s>>>(g, a, ctrl, avg);
   } else {
     k_phase_states<false><<<nblk(g.ng), PB, 0, s>>>(g, a, ctrl);
+    k_phase_faces<<<nblk(g.ng), PB, 0, s>>>(g, a, a.states + 42 * g.ng);
     k_phase_update<false><<<nblk(g.ng), PB, 0, s>>>(g, a, ctrl, avg);
   }
   return cudaGetLastError();
