@@ -208,6 +208,8 @@ int bx_destroy(bx_handle* h) {
   cudaFree(h->pa.gtmp);
   cudaFree(h->pa.muc);
   cudaFree(h->d_eos);
+  for (cudaGraphExec_t x : h->run_graph)
+    if (x) cudaGraphExecDestroy(x);
   for (cudaStream_t x : h->hs)
     if (x) cudaStreamDestroy(x);
   for (cudaEvent_t e : h->hev) cudaEventDestroy(e);
@@ -1071,11 +1073,107 @@ int bx_ghost_plan(const bx_params* params, int64_t* nghost, int32_t* dst, int32_
   return BX_OK;
 }
 
+// Up to kRunChunk steps on the fused form without a host round trip per step:
+// the batched path's clock kernels save the clock at each step's start; a step
+// whose guard fires (limiter, low density, non-finite) restores it and
+// deactivates the rest of the run, its input planes untouched, and so does
+// the end time.  *taken = steps committed; *tripped = a step is to be redone.
+static constexpr int kRunChunk = 32;
+static int fused_run(bx_handle* h, double endtime, int64_t nsteps, int64_t* taken,
+                     bool* tripped) {
+  *taken = 0;
+  *tripped = false;
+  const Geom& g = h->g;
+  cudaStream_t s = h->stream;
+  const int K = (int)std::min<int64_t>(nsteps, kRunChunk);
+  h->clock.endtime = endtime;
+  h->clock.flags = 0;
+  h->clock.tripped = 0;
+  h->clock.run_step = 0;
+  if (int r = push_clock(h)) return r;
+  const long long step0 = h->clock.step;
+  const int cur0 = h->cur;
+  StageArgs a{};
+  a.ctrl = h->d_ctrl;
+  a.geom = h->d_geom;
+  a.tiles = h->d_tiles;
+  a.ncells_total = g.ng;
+  a.U = h->pa.u;
+  a.G = h->gforce_set ? h->pa.gforce : nullptr;
+  a.UC = h->pa.cons_old;
+  const bool p2 = g.pow2 != 0, t3 = g.threed != 0;
+  auto enqueue = [&]() -> cudaError_t {
+    int cur = cur0;
+    for (int k = 0; k < K; ++k) {
+      cudaError_t e = launch_dt_batch(h->d_ctrl, 1, s);
+      a.nsrc = k == 0 ? h->nsrc : (h->gforce_set ? 1 : 2);
+      a.X = h->buf[cur];
+      a.Y = nullptr;
+      a.out = h->buf[(cur + 1) % 3];
+      if (e == cudaSuccess) e = launch_stage(0, p2, t3, a, h->ntiles, s);
+      a.Y = h->buf[(cur + 1) % 3];
+      a.out = h->buf[(cur + 2) % 3];
+      if (e == cudaSuccess) e = launch_stage(1, p2, t3, a, h->ntiles, s);
+      if (e == cudaSuccess) e = launch_end_batch(h->d_ctrl, 1, s);
+      if (e != cudaSuccess) return e;
+      cur = (cur + 2) % 3;
+    }
+    return cudaSuccess;
+  };
+  if (K == kRunChunk && !h->gforce_set) {
+    // whole chunks replay a CUDA graph per (input plane set, pending sources):
+    // the launches of a chunk cost less than the work of a small grid
+    const int key = cur0 + 3 * (h->nsrc - 1);
+    if (!h->run_graph[key]) {
+      cudaGraph_t graph = nullptr;
+      CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeRelaxed));
+      const cudaError_t e = enqueue();
+      const cudaError_t e2 = cudaStreamEndCapture(s, &graph);
+      CK(e);
+      CK(e2);
+      const cudaError_t e3 = cudaGraphInstantiate(&h->run_graph[key], graph, 0);
+      cudaGraphDestroy(graph);
+      CK(e3);
+    }
+    CK(cudaGraphLaunch(h->run_graph[key], s));
+  } else {
+    CK(enqueue());
+  }
+  h->launches += 4 * K;
+  if (int r = pull_clock(h)) return r;
+  const long long m = h->clock.step - step0;
+  *taken = m;
+  *tripped = h->clock.tripped != 0;
+  if (m > 0) {
+    h->cur = (int)((cur0 + 2 * m) % 3);
+    h->nsrc = h->gforce_set ? 1 : 2;
+    h->grav_step = h->gforce_set;
+    h->p_saved = false;
+    h->last_path = 1;
+  }
+  h->clock.flags = 0;
+  h->clock.tripped = 0;
+  h->clock.active = 0;
+  return push_clock(h);
+}
+
 int bx_run(bx_handle* h, double endtime, int64_t nsteps, int64_t* steps_taken) {
   CHECK_H();
   int64_t n = 0;
   int rc = BX_OK;
   while (n < nsteps) {
+    if (h->mode == 1 && !h->prof) {
+      int64_t m = 0;
+      bool tripped = false;
+      rc = fused_run(h, endtime, nsteps - n, &m, &tripped);
+      if (rc != BX_OK) break;
+      n += m;
+      if (!tripped) {
+        if (m < std::min<int64_t>(nsteps - n + m, kRunChunk)) break;  // end time or step cap
+        continue;
+      }
+      // the tripped step: bx_step takes it again (on the per-phase kernels)
+    }
     int32_t ran = 0;
     rc = bx_step(h, endtime, &ran);
     if (rc != BX_OK || !ran) break;

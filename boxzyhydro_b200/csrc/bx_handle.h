@@ -59,6 +59,9 @@ struct bx_handle {
   // upload copies, download copies, conversions, second stage-1 stream
   cudaStream_t hs[4] = {nullptr, nullptr, nullptr, nullptr};
   std::vector<cudaEvent_t> hev;  // start, join, then per slab: in, stage 0, stage 1, converted
+  // bx_run: CUDA graphs of a whole chunk of force-free steps, per input plane
+  // set (3) and pending sources (1 or 2)
+  cudaGraphExec_t run_graph[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   std::string err;
 };
 
