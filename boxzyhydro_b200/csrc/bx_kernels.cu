@@ -949,6 +949,8 @@ __global__ void k_phase_states(Geom g, PhaseArrays a, Ctrl* ctrl) {
   const double d0 = c[i];
   const double sound = sqrt(a.p[i] * a.adindx[i] / d0);
   const double eps0 = recon_eps(d0, c[4 * n + i], u[i], u[n + i], u[2 * n + i], g.small_eps);
+  // unrolled: the per-direction constants stay in registers, not on the stack
+#pragma unroll
   for (int dir = 0; dir < 3; ++dir) {
     const long long im = ghost ? i : i - st[dir], ip = ghost ? i : i + st[dir];
     const long long idx3[3] = {im, i, ip};
@@ -978,6 +980,7 @@ __global__ void k_phase_states(Geom g, PhaseArrays a, Ctrl* ctrl) {
       q[7] = c[n + i];
       q[NQ - 1] = c[2 * n + i];
     }
+#pragma unroll
     for (int k = 0; k < NQ; ++k) {
       const double mi = q[k] + kHalf * (-1.0 - lm) * sl[k];
       const double pl = q[k] + kHalf * (1.0 - lp) * sl[k];
