@@ -326,6 +326,7 @@ def batched_arm(args, rank, world, local):
     total_ms = 0.0
     launches = 0
     checked, maxdiff, solo = 0, 0.0, 0
+    tuned = []
     check_every = max(1, args.nbox // args.check_boxes)
     t_wall0 = time.perf_counter()
     for ci, chunk in enumerate(chunks):
@@ -336,6 +337,10 @@ def batched_arm(args, rank, world, local):
             b.upload(i, ic.riemann_box_cons(s["side"], s["axis"], s["left"], s["right"],
                                             s["gamma"]))
         b.run(args.warmup)
+        if not args.no_autotune:
+            zc, tms = b.autotune(reps=2)
+            tuned.append({"tile_depth": "whole box" if zc >= 1 << 30 else
+                          ("default rule" if zc == 0 else zc), "trial_ms_per_step": tms})
         b.run(args.steps)
         inf = b.info()
         total_ms += inf["last_run_ms"]
@@ -398,6 +403,7 @@ def batched_arm(args, rank, world, local):
                              "ms_per_box_run_by_side": per_size_ms,
                              "sample_per_side": args.loop_sample},
         "speedup_vs_loop": value / loop_value,
+        "autotune": tuned or None,
         "parity": {"boxes_checked": checked, "max_rel_diff_cons": maxdiff,
                    "boxes_on_own_handle": solo},
         "gpu_launches": launches,
@@ -560,6 +566,7 @@ def main():
     ap.add_argument("--keep-stage0", action="store_true", dest="keep_stage0")
     ap.add_argument("--nbox", type=int, default=4096)
     ap.add_argument("--check-boxes", type=int, default=16, dest="check_boxes")
+    ap.add_argument("--no-autotune", action="store_true", dest="no_autotune")
     ap.add_argument("--loop-sample", type=int, default=8, dest="loop_sample")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)

@@ -109,6 +109,7 @@ def lib():
         "bx_batch_set_clock": (C.c_int, [H, C.c_int32, C.c_double, C.c_double, C.c_int64]),
         "bx_batch_get_clock": (C.c_int, [H, C.c_int32, dp, dp, dp, i64p]),
         "bx_batch_run": (C.c_int, [H, C.c_int64, C.c_double, C.c_int32]),
+        "bx_batch_autotune": (C.c_int, [H, C.c_int32, i32p, dp]),
         "bx_batch_download": (C.c_int, [H, C.c_int32, vp, vp, vp]),
         "bx_batch_info": (C.c_int, [H, dp, i64p, i32p, i64p]),
         "bx_batch_last_error": (C.c_char_p, [H]),

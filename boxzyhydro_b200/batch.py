@@ -67,6 +67,15 @@ class Batch:
     def run(self, nsteps, endtime=1e300, graph=True):
         self._c(lib().bx_batch_run(self._h, int(nsteps), float(endtime), 1 if graph else 0))
 
+    def autotune(self, reps=2):
+        """Pick the ensemble's tile depth by timing trial steps from the current
+        states (left unchanged): returns (depth, ms per step); depth 0 is the
+        default rule, >= 2**30 whole box depths."""
+        zc = C.c_int32()
+        ms = C.c_double()
+        self._c(lib().bx_batch_autotune(self._h, int(reps), C.byref(zc), C.byref(ms)))
+        return zc.value, ms.value
+
     def download(self, box):
         n = self.params[box].ngrid
         c = np.empty((n, 5))

@@ -59,6 +59,7 @@ struct bx_batch {
   Ctrl* h_ctrl = nullptr;  // pinned, nbox
   Tile* d_tiles = nullptr;
   int ntiles = 0;
+  int zc = 0;  // tile depth policy of the tile list (set_tiles)
   bool pow2 = true, threed = true;
   int pm = 1;  // 1: all boxes have power-of-two spacings; 0: otherwise (cdiv, exact for any)
   PhaseArrays scratch{};  // reference arrays of the largest box (downloads)
@@ -110,6 +111,60 @@ extern "C" {
 int bx_batch_destroy(bx_batch* b);
 
 const char* bx_batch_last_error(bx_batch* b) { return b ? b->err.c_str() : g_batch_err.c_str(); }
+
+// Tiles of every box, longest first.  zc: the z extent of a column tile
+// (interior planes; capped at each box's depth), or 0 for the default rule: a
+// tile marches through the whole box depth when the ensemble has enough
+// columns to fill the GPU many times over (no z warm-up repeated per chunk),
+// else depths are cut into chunks of 32 planes.
+static std::vector<Tile> batch_tiles(const bx_batch* b, int zc_req) {
+  int dev = 0, sms = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  long long ncol = 0;
+  for (int i = 0; i < b->nbox; ++i) {
+    const Geom& g = b->G[i];
+    ncol += (long long)((g.ax1 - g.ax0 + TX - 1) / TX) * ((g.ay1 - g.ay0 + TY - 1) / TY);
+  }
+  const bool whole = ncol >= 16ll * sms * std::max(1, stage_blocks_per_sm(1, b->pm, b->threed));
+  std::vector<std::pair<long long, Tile>> tl;
+  for (int i = 0; i < b->nbox; ++i) {
+    const Geom& g = b->G[i];
+    const int NAx = g.ax1 - g.ax0, NAy = g.ay1 - g.ay0, NAz = g.az1 - g.az0;
+    int zc = 1;
+    if (g.threed) zc = zc_req > 0 ? std::min(NAz, zc_req) : (whole ? NAz : std::min(NAz, 32));
+    for (int z = 0; z < NAz; z += zc)
+      for (int y = 0; y < NAy; y += TY)
+        for (int x = 0; x < NAx; x += TX) {
+          const int z1 = std::min(NAz, z + zc);
+          const long long work = (long long)(z1 - z + (g.threed ? 1 : 0)) *
+                                 std::min(TX, NAx - x) * std::min(TY, NAy - y);
+          tl.push_back({work, Tile{i, x, y, z, z1}});
+        }
+  }
+  std::stable_sort(tl.begin(), tl.end(),
+                   [](const auto& a, const auto& c) { return a.first > c.first; });
+  std::vector<Tile> tiles(tl.size());
+  for (size_t k = 0; k < tl.size(); ++k) tiles[k] = tl[k].second;
+  return tiles;
+}
+
+// (re)build the device tile list; a captured run graph holds the old one
+static int set_tiles(bx_batch* b, int zc_req) {
+  const std::vector<Tile> tiles = batch_tiles(b, zc_req);
+  if (b->graph) {
+    cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+    b->graph_steps = -1;
+  }
+  cudaFree(b->d_tiles);
+  b->d_tiles = nullptr;
+  b->ntiles = (int)tiles.size();
+  BCK(cudaMalloc(&b->d_tiles, tiles.size() * sizeof(Tile)));
+  BCK(cudaMemcpy(b->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+  b->zc = zc_req;
+  return BX_OK;
+}
 
 int bx_batch_create(int32_t nbox, const bx_params* params, bx_batch** out) {
   if (nbox <= 0 || !params || !out) return berr(nullptr, BX_ERR_ARG, "bad arguments");
@@ -204,40 +259,7 @@ int bx_batch_create(int32_t nbox, const bx_params* params, bx_batch** out) {
     b->h_ctrl[i].nsrc = 1;
   }
   BCKC(cudaMemcpy(b->d_ctrl, b->h_ctrl, nbox * sizeof(Ctrl), cudaMemcpyHostToDevice));
-  // tiles of every box, longest first.  A column tile marches through the whole
-  // box depth when the ensemble has enough columns to fill the GPU many times
-  // over (no z warm-up repeated per chunk); otherwise depths are cut into
-  // chunks of 32 planes.
-  int dev = 0, sms = 148;
-  cudaGetDevice(&dev);
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  long long ncol = 0;
-  for (int i = 0; i < nbox; ++i) {
-    const Geom& g = b->G[i];
-    ncol += (long long)((g.ax1 - g.ax0 + TX - 1) / TX) * ((g.ay1 - g.ay0 + TY - 1) / TY);
-  }
-  const bool whole = ncol >= 16ll * sms * std::max(1, stage_blocks_per_sm(1, b->pm, b->threed));
-  std::vector<std::pair<long long, Tile>> tl;
-  for (int i = 0; i < nbox; ++i) {
-    const Geom& g = b->G[i];
-    const int NAx = g.ax1 - g.ax0, NAy = g.ay1 - g.ay0, NAz = g.az1 - g.az0;
-    const int zc = g.threed ? (whole ? NAz : std::min(NAz, 32)) : 1;
-    for (int z = 0; z < NAz; z += zc)
-      for (int y = 0; y < NAy; y += TY)
-        for (int x = 0; x < NAx; x += TX) {
-          const int z1 = std::min(NAz, z + zc);
-          const long long work = (long long)(z1 - z + (g.threed ? 1 : 0)) *
-                                 std::min(TX, NAx - x) * std::min(TY, NAy - y);
-          tl.push_back({work, Tile{i, x, y, z, z1}});
-        }
-  }
-  std::stable_sort(tl.begin(), tl.end(),
-                   [](const auto& a, const auto& c) { return a.first > c.first; });
-  std::vector<Tile> tiles(tl.size());
-  for (size_t k = 0; k < tl.size(); ++k) tiles[k] = tl[k].second;
-  b->ntiles = (int)tiles.size();
-  BCKC(cudaMalloc(&b->d_tiles, tiles.size() * sizeof(Tile)));
-  BCKC(cudaMemcpy(b->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
+  if (int r = set_tiles(b, 0)) return fail(r);
   // reference arrays for downloads, sized for the largest box
   const long long m = b->max_ng;
   BCKC(cudaMalloc(&b->scratch.cons, 5 * m * sizeof(double)));
@@ -468,6 +490,54 @@ int bx_batch_run(bx_batch* b, int64_t nsteps, double endtime, int32_t use_graph)
         return berr(b, r, bx_last_error(b->solo[i]));
     }
   }
+  return BX_OK;
+}
+
+// The tile shape of the ensemble picked by measurement: each candidate tile
+// depth (the default rule, whole box depths, and 64, 32, 16 and 8 planes) runs
+// `reps` trial steps from the boxes' current states -- the step reads the
+// input plane set and writes the other two, and the clocks are put back after
+// every trial, so the ensemble is left as it was -- and the fastest stays.
+// The tile's x-y extent is the stage kernel's (32 x 8) and the halo depth is
+// the stencil's (two cells), so depth is what remains to tune.
+int bx_batch_autotune(bx_batch* b, int32_t reps, int32_t* zc_out, double* ms_out) {
+  if (!b || reps < 1) return berr(b, BX_ERR_ARG, "bad arguments");
+  if (int r = pull_ctrl(b)) return r;
+  const std::vector<Ctrl> saved(b->h_ctrl, b->h_ctrl + b->nbox);
+  const int cand[] = {0, -1, 64, 32, 16, 8};
+  int best = 0;
+  double best_ms = 1e300;
+  for (int zc : cand) {
+    // whole depths: a chunk no box exceeds
+    const int zreq = zc < 0 ? (1 << 30) : zc;
+    if (int r = set_tiles(b, zreq)) return r;
+    double ms_min = 1e300;
+    for (int r = 0; r < reps; ++r) {
+      for (int i = 0; i < b->nbox; ++i) {
+        b->h_ctrl[i] = saved[i];
+        b->h_ctrl[i].endtime = 1e300;
+        b->h_ctrl[i].flags = 0;
+        b->h_ctrl[i].run_step = 0;
+      }
+      if (int rc = push_ctrl(b)) return rc;
+      BCK(cudaEventRecord(b->ev0, b->stream));
+      if (int rc = enqueue_steps(b, 1)) return rc;
+      BCK(cudaEventRecord(b->ev1, b->stream));
+      BCK(cudaEventSynchronize(b->ev1));
+      float ms = 0.f;
+      BCK(cudaEventElapsedTime(&ms, b->ev0, b->ev1));
+      ms_min = std::min(ms_min, (double)ms);
+    }
+    if (ms_min < best_ms) {
+      best_ms = ms_min;
+      best = zreq;
+    }
+  }
+  if (int r = set_tiles(b, best)) return r;
+  std::copy(saved.begin(), saved.end(), b->h_ctrl);
+  if (int r = push_ctrl(b)) return r;
+  if (zc_out) *zc_out = best;
+  if (ms_out) *ms_out = best_ms;
   return BX_OK;
 }
 

@@ -238,6 +238,13 @@ int bx_batch_get_clock(bx_batch *b, int32_t box, double *time, double *dt, doubl
                        int64_t *step);
 /* nsteps iterations of every box's main loop (boxes at endtime stop). */
 int bx_batch_run(bx_batch *b, int64_t nsteps, double endtime, int32_t use_graph);
+/* Tile shape of the ensemble picked by measurement: every candidate tile depth
+ * (the default rule, whole box depths, 64, 32, 16, 8 planes) runs reps trial steps
+ * from the boxes' current states, which the trials leave unchanged (inputs are
+ * not overwritten; clocks are restored), and the fastest is kept for the following
+ * runs.  *zc = the chosen depth (0 = default rule, >= 2^30 = whole depths), *ms =
+ * its trial step time.  Results do not depend on the tiling. */
+int bx_batch_autotune(bx_batch *b, int32_t reps, int32_t *zc, double *ms);
 int bx_batch_download(bx_batch *b, int32_t box, double *cons, double *u, double *p);
 /* device time of the last run (ms), kernels it launched, boxes running on their own
  * handles, cells in the pool */

@@ -65,6 +65,34 @@ def test_batch_box_leaving_the_fused_path():
     b.close()
 
 
+def test_autotune_leaves_the_ensemble_as_it_was():
+    """The tile-depth autotuner times trial steps from the current states; the
+    boxes then continue exactly as if it had not run, with the tiling it chose,
+    and so does a box already on its own handle."""
+    boxes = ensemble(10, seed=12, sides=(8, 12, 20, 26))
+    boxes[3].params.vlimit = 0.6
+    boxes[3].params.validate()
+    b = Batch([st.params for st in boxes])
+    for i, st in enumerate(boxes):
+        b.upload(i, st.cons)
+    b.run(3)
+    solo = b.info()["solo_boxes"]
+    zc, ms = b.autotune(reps=2)
+    assert ms > 0 and (zc in (0, 8, 16, 32, 64) or zc >= 1 << 30)
+    assert b.info()["solo_boxes"] == solo
+    for i in range(len(boxes)):
+        assert b.clock(i)["step"] == 3
+    b.run(5)
+    for i, st in enumerate(boxes):
+        (c0, u0, p0), clk0 = alone(st, 8)
+        c1, u1, p1 = b.download(i)
+        assert np.array_equal(c0, c1) and np.array_equal(u0, u1) and np.array_equal(p0, p1), i
+        clk1 = b.clock(i)
+        for k in ("time", "dt", "dtold", "step"):
+            assert clk0[k] == clk1[k], (i, k)
+    b.close()
+
+
 def test_batch_rejects_state_it_cannot_start_from():
     st = ic.sod_x(n_active=16, ny=8, nz=8)
     st.params.no_outflow_xl = st.params.no_outflow_xr = False
