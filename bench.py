@@ -15,7 +15,8 @@ steps, barrier and synchronize on both sides, max over ranks.  Under torchrun
 every rank advances its own replica of the box (the step has no exchange; the
 reference runs on one node's shared memory), so value = ranks x cells x K / t.
 The JSON line also carries the end-to-end figure through the C ABI with host
-arrays (upload of cons/u/p from pinned memory, step, download every step), the
+arrays (bx_step_host: cons from pinned memory in, one step, cons back, every
+step; the three separate calls and the full cons/u/p arrays beside it), the
 HBM roofline of the dominant stage kernel, the FP64 roofline, nvidia-smi clocks
 sampled during the timed region and the oracle timed on the host cores.
 
