@@ -350,10 +350,14 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
     }
     __syncthreads();
 
-    // ---- B: x and y face states of the plane
-    for (int i = tid; i < nxs + nys; i += NT) {
+    // ---- B: x and y face states of the plane.  The y items start at a warp
+    // boundary, so no warp runs both the x and the y code (the x items end in
+    // idle lanes instead)
+    const int nxs_w = (nxs + 31) & ~31;
+    for (int i = tid; i < nxs_w + nys; i += NT) {
       FaceState mi, pl;
-      if (i < nxs) {
+      if (i < nxs_w) {
+        if (i >= nxs) continue;
         const int cy = i / (w + 2), cx = i % (w + 2) - 1;
         const int c = (cy + 2) * PW + (cx + 2);
         const Prim q = get_prim(SP, c);
@@ -368,7 +372,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         put_fs(SX, NSX, o, mi);
         put_fs(SX + 6 * NSX, NSX, o, pl);
       } else {
-        const int k = i - nxs;
+        const int k = i - nxs_w;
         const int cy = k / w - 1, cx = k % w;
         const int c = (cy + 2) * PW + (cx + 2);
         const Prim q = get_prim(SP, c);
@@ -386,10 +390,13 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
     }
     __syncthreads();
 
-    // ---- C: x and y face fluxes (face f lies between cells f-1 and f)
-    for (int i = tid; i < nxf + nyf; i += NT) {
+    // ---- C: x and y face fluxes (face f lies between cells f-1 and f); the y
+    // faces start at a warp boundary as in B
+    const int nxf_w = (nxf + 31) & ~31;
+    for (int i = tid; i < nxf_w + nyf; i += NT) {
       double F[5];
-      if (i < nxf) {
+      if (i < nxf_w) {
+        if (i >= nxf) continue;
         const int cy = i / (w + 1), f = i % (w + 1);
         const int base = cy * (TX + 2);
         const FaceState L = get_fs(SX + 6 * NSX, NSX, base + f);  // plus state of cell f-1
@@ -399,7 +406,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
 #pragma unroll
         for (int q = 0; q < 5; ++q) FX[q * NFX + o] = F[q];
       } else {
-        const int k = i - nxf;
+        const int k = i - nxf_w;
         const int f = k / w, cx = k % w;
         const FaceState L = get_fs(SY + 6 * NSY, NSY, f * TX + cx);
         const FaceState R = get_fs(SY, NSY, (f + 1) * TX + cx);
