@@ -451,13 +451,22 @@ def adjoint_arm(args, rank, world, local):
     c0 = torch.tensor(np.ascontiguousarray(st.cons.T), device=dev)
     del st
     snaps = args.snapshots
+    # stage-0 cache entries: 8 beside a given snapshot count; when the snapshots
+    # fill HBM, about a third of the free state sets (a schedule simulation of
+    # 400 steps in 17 sets: 11 snapshots + 6 entries recompute least)
+    entries = args.stage0_cache if args.stage0_cache > 0 else 8
+    if args.keep_stage0:
+        entries = 2
     if snaps <= 0:
-        # engine: 9 state sets + 14 scratch planes + (snaps + 1) state sets;
-        # this arm, beside c0: gradient, direction, perturbed state, output and
-        # one density plane (21 planes)
+        # engine: 7 state sets + 14 scratch planes + cache entries + (snaps + 1)
+        # state sets; this arm, beside c0: gradient, direction, perturbed state,
+        # output and one density plane (21 planes)
         free = torch.cuda.mem_get_info(dev)[0]
-        fixed = (9 * 5 + 14 + 5 + 21) * plane + (6 << 30)
-        snaps = int(max(1, min(args.steps, (free - fixed) // (5 * plane))))
+        fixed = (7 * 5 + 14 + 5 + 21) * plane + (6 << 30)
+        sets = int(max(3, (free - fixed) // (5 * plane)))
+        if args.stage0_cache <= 0 and not args.keep_stage0:
+            entries = max(2, min(8, round(0.35 * sets)))
+        snaps = int(max(1, min(args.steps, sets - entries)))
     peak = [0]
 
     def used():
@@ -465,6 +474,7 @@ def adjoint_arm(args, rank, world, local):
         peak[0] = max(peak[0], t - f)
 
     eng = AdjointEngine(hp, args.steps, snaps)
+    eng.stage0_cache(entries)
     if args.keep_stage0:
         eng.keep_stage0(True)
     stream = torch.cuda.Stream()
@@ -529,7 +539,8 @@ def adjoint_arm(args, rank, world, local):
         "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"discrete adjoint, {n}^3 interior, gamma=5/3, {ic_name}, "
                                f"{args.steps} steps, loss 0.5||rho(T)-rho_target||^2",
-                   "snapshots": snaps, "keep_stage0": bool(args.keep_stage0)},
+                   "snapshots": snaps, "keep_stage0": bool(args.keep_stage0),
+                   "stage0_cache_entries": entries},
         "ms_forward": stats_fwd["ms_forward"], "ms_backward": stt["ms_backward"],
         "forward_cell_updates_per_s": hp.n_active() * args.steps / (stats_fwd["ms_forward"] * 1e-3),
         "recomputed_steps": stt["recomputed_steps"],
@@ -565,6 +576,7 @@ def main():
     ap.add_argument("--fd-dirs", type=int, default=16, dest="fd_dirs")
     ap.add_argument("--adj-ic", default="blob", choices=["blob", "turb"], dest="adj_ic")
     ap.add_argument("--keep-stage0", action="store_true", dest="keep_stage0")
+    ap.add_argument("--stage0-cache", type=int, default=0, dest="stage0_cache")
     ap.add_argument("--nbox", type=int, default=4096)
     ap.add_argument("--check-boxes", type=int, default=16, dest="check_boxes")
     ap.add_argument("--no-autotune", action="store_true", dest="no_autotune")

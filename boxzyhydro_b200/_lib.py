@@ -117,6 +117,7 @@ def lib():
         "bx_adj_destroy": (C.c_int, [H]),
         "bx_adj_set_stream": (C.c_int, [H, vp]),
         "bx_adj_keep_stage0": (C.c_int, [H, C.c_int32]),
+        "bx_adj_stage0_cache": (C.c_int, [H, C.c_int32]),
         "bx_adj_forward": (C.c_int, [H, vp, vp, C.c_int32]),
         "bx_adj_backward": (C.c_int, [H, vp, vp]),
         "bx_adj_stats": (C.c_int, [H, dp, dp, i64p, i64p]),

@@ -50,6 +50,10 @@ class AdjointEngine:
         speed: the backward then skips recomputing stage 0)."""
         self._c(lib().bx_adj_keep_stage0(self._h, 1 if enable else 0))
 
+    def stage0_cache(self, entries):
+        """Entries of the backward pass's cache of stage-0 results (>= 2)."""
+        self._c(lib().bx_adj_stage0_cache(self._h, int(entries)))
+
     def set_stream(self, ptr):
         self._c(lib().bx_adj_set_stream(self._h, C.c_void_p(ptr) if ptr else None))
 

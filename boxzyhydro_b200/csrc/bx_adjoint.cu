@@ -725,10 +725,11 @@ struct bx_adj {
   bool c1_valid = false;
   // stage-0 results left by the last step of recent advances, tagged with
   // their step (-1: empty): the reverse of that step then skips its stage-0
-  // recompute.  Two entries, so an advance to state k can leave C1 of step k-1
-  // while the entry of step k, needed first, stays.
-  double* c1c[2] = {nullptr, nullptr};
-  long long c1tag[2] = {-1, -1};
+  // recompute.  At least two entries, so an advance to state k can leave C1 of
+  // step k-1 while the entry of step k, needed first, stays
+  // (bx_adj_stage0_cache sets the count).
+  std::vector<double*> c1c;
+  std::vector<long long> c1tag;
   long long c1_hits = 0;
   long long rev_done = 0;  // last reversed step (steps are reversed downwards)
   // work planes
@@ -870,8 +871,8 @@ static int rev_step(bx_adj* A, const double* X, long long k, double* lam) {
   const double* C1 = A->W1;
   if (A->c1pool && A->c1_valid) {
     C1 = A->c1pool + k * 5 * g.ng;
-  } else if (A->c1tag[0] == k || A->c1tag[1] == k) {
-    C1 = A->c1c[A->c1tag[0] == k ? 0 : 1];
+  } else if (std::find(A->c1tag.begin(), A->c1tag.end(), k) != A->c1tag.end()) {
+    C1 = A->c1c[std::find(A->c1tag.begin(), A->c1tag.end(), k) - A->c1tag.begin()];
     A->c1_hits += 1;
   } else {
     if (int r = fwd_step(A, X, nsrc, dt, nullptr, true)) return r;  // W1 <- C1
@@ -931,17 +932,21 @@ static int advance(bx_adj* A, const double* src, long long from, long long to, d
   for (long long k = from; k < to; ++k) {
     double* out = ((to - k) % 2 == 1) ? dst : A->W2;
     double* c1out = nullptr;
-    if (k == to - 1 && !A->c1pool) {
+    if (k == to - 1 && !A->c1pool && !A->c1c.empty()) {
       // keep C1 of step to-1 (reversed soon after step `to` when no further
       // split comes between them) in an entry that is free or already used;
-      // else in the one of the step reversed later, never in step `to`'s
+      // else in the one of the step reversed last, never in step `to`'s
       auto dead = [&](long long t) { return t < 0 || t >= A->rev_done; };
-      int j;
-      if (A->c1tag[0] == to) j = 1;
-      else if (A->c1tag[1] == to) j = 0;
-      else if (dead(A->c1tag[0])) j = 0;
-      else if (dead(A->c1tag[1])) j = 1;
-      else j = A->c1tag[0] < A->c1tag[1] ? 0 : 1;
+      int j = -1;
+      for (int e = 0; e < (int)A->c1tag.size() && j < 0; ++e)
+        if (A->c1tag[e] != to && dead(A->c1tag[e])) j = e;
+      for (int e = 0; e < (int)A->c1tag.size() && j < 0; ++e)
+        if (A->c1tag[e] != to) j = e;
+      if (j < 0) j = 0;
+      for (int e = 0; e < (int)A->c1tag.size(); ++e)
+        if (A->c1tag[e] != to && !dead(A->c1tag[e]) && A->c1tag[e] < A->c1tag[j] &&
+            !dead(A->c1tag[j]))
+          j = e;
       A->c1tag[j] = k;
       c1out = A->c1c[j];
     }
@@ -993,8 +998,9 @@ int bx_adj_destroy(bx_adj* A) {
   if (A->h && A->h->stream) cudaStreamSynchronize(A->h->stream);
   for (double* p : A->pool) cudaFree(p);
   double* ps[] = {A->W0, A->W1, A->W2, A->XT, A->lamA, A->lamB, A->lamC1,
-                  A->P,  A->PA, A->d_dts, A->c1c[0], A->c1c[1]};
+                  A->P,  A->PA, A->d_dts};
   for (double* p : ps) cudaFree(p);
+  for (double* p : A->c1c) cudaFree(p);
   cudaFree(A->c1pool);
   if (A->h) bx_destroy(A->h);
   delete A;
@@ -1032,10 +1038,13 @@ int bx_adj_create(const bx_params* params, int64_t nsteps, int32_t snapshots, bx
   A->pool.assign(A->snaps + 1, nullptr);
   for (int k = 0; k <= A->snaps; ++k)
     if ((rc = amalloc(A, &A->pool[k], 5 * n))) return fail(rc);
-  double** planes5[] = {&A->W0,   &A->W1,    &A->W2,    &A->XT,   &A->lamA,
-                        &A->lamB, &A->lamC1, &A->c1c[0], &A->c1c[1]};
+  double** planes5[] = {&A->W0, &A->W1, &A->W2, &A->XT, &A->lamA, &A->lamB, &A->lamC1};
   for (double** p : planes5)
     if ((rc = amalloc(A, p, 5 * n))) return fail(rc);
+  A->c1c.assign(2, nullptr);
+  A->c1tag.assign(2, -1);
+  for (double*& p : A->c1c)
+    if ((rc = amalloc(A, &p, 5 * n))) return fail(rc);
   if ((rc = amalloc(A, &A->P, 7 * n))) return fail(rc);
   if ((rc = amalloc(A, &A->PA, 7 * n))) return fail(rc);
   if ((rc = amalloc(A, &A->d_dts, nsteps))) return fail(rc);
@@ -1073,6 +1082,29 @@ int bx_adj_keep_stage0(bx_adj* A, int32_t enable) {
     A->bytes -= (size_t)A->nsteps * 5 * A->ng * sizeof(double);
   }
   A->c1_valid = false;  // filled by the next unfrozen forward run
+  return BX_OK;
+}
+
+int bx_adj_stage0_cache(bx_adj* A, int32_t entries) {
+  if (!A || entries < 2) return aerr(A, BX_ERR_ARG, "the stage-0 cache needs at least 2 entries");
+  const long long n5 = 5 * A->ng;
+  if (A->h && A->h->stream) cudaStreamSynchronize(A->h->stream);
+  while ((int)A->c1c.size() > entries) {
+    cudaFree(A->c1c.back());
+    A->c1c.pop_back();
+    A->bytes -= n5 * sizeof(double);
+  }
+  while ((int)A->c1c.size() < entries) {
+    double* p = nullptr;
+    if (cudaMalloc(&p, n5 * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      A->c1tag.assign(A->c1c.size(), -1);
+      return aerr(A, BX_ERR_NOMEM, "no room for the stage-0 cache entries");
+    }
+    A->c1c.push_back(p);
+    A->bytes += n5 * sizeof(double);
+  }
+  A->c1tag.assign(A->c1c.size(), -1);
   return BX_OK;
 }
 
@@ -1180,7 +1212,7 @@ int bx_adj_backward(bx_adj* A, const double* lamT, double* lam0) {
   cudaEventCreate(&e1);
   ACK(cudaEventRecord(e0, s));
   A->fwd_steps_in_bwd = 0;
-  A->c1tag[0] = A->c1tag[1] = -1;
+  std::fill(A->c1tag.begin(), A->c1tag.end(), -1);
   A->c1_hits = 0;
   A->rev_done = A->nsteps;
   A->pool_free.clear();

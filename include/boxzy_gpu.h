@@ -267,6 +267,11 @@ int bx_adj_set_stream(bx_adj *a, void *cuda_stream);
  * (nsteps x 5 x ngrid doubles more), and backward passes use them instead of
  * recomputing stage 0 of each step; BX_ERR_NOMEM if they do not fit. */
 int bx_adj_keep_stage0(bx_adj *a, int32_t enable);
+/* Entries (>= 2, default 2; 5 x ngrid doubles each) of the cache of stage-0
+ * results the backward pass keeps from the last step of each recompute advance,
+ * so the reverse of that step skips its stage-0 recompute; more entries keep
+ * results for longer.  BX_ERR_NOMEM if they do not fit. */
+int bx_adj_stage0_cache(bx_adj *a, int32_t entries);
 /* frozen=0: dt by the CFL rule (main.f90:266-281) and recorded; frozen=1: the recorded
  * dt sequence (for finite differences).  BX_ERR_STATE if a guard fired. */
 int bx_adj_forward(bx_adj *a, const double *cons0, double *consT, int32_t frozen);

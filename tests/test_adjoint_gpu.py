@@ -156,6 +156,22 @@ def test_kept_stage0_results_give_the_same_gradient():
     eng.close()
 
 
+def test_stage0_cache_sizes_give_the_same_gradient():
+    """The backward pass's cache of stage-0 results changes what is recomputed,
+    not the gradient: 2, 3 and 8 entries, a backward repeated after a resize."""
+    st, eng = setup(nsteps=24, snaps=3)
+    hp = st.params
+    fwd(eng, st.cons, frozen=False)
+    rng = np.random.default_rng(6)
+    lamT = rand_dir(hp, rng, np.ones(5))
+    ref = bwd(eng, lamT)
+    for entries in (3, 8, 2):
+        eng.stage0_cache(entries)
+        fwd(eng, st.cons, frozen=False)
+        assert np.array_equal(bwd(eng, lamT), ref), entries
+    eng.close()
+
+
 def test_torch_autograd_function():
     torch = _torch()
     st, eng = setup()
