@@ -298,6 +298,13 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
 
   for (int z = (THREED ? z0 : g.az0 + t.z0); z < (THREED ? z1 : g.az0 + t.z1); ++z) {
     // ---- A: primitives of plane z (own from the pipeline, halo computed here)
+    if (STAGE == 1 && own) {
+      // the update at the end of this plane reads the step input of the own
+      // cell, which nothing in this stage loaded before: start it towards L2
+      const double* c = a.X + g.base + gx + (long long)gy * g.sy + (long long)z * g.sz;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) asm volatile("prefetch.global.L2 [%0];" ::"l"(c + q * PS));
+    }
     Prim P2;
     FaceState mz1, pz1;
     if (own) {
