@@ -304,6 +304,14 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
       const double* c = a.X + g.base + gx + (long long)gy * g.sy + (long long)z * g.sz;
 #pragma unroll
       for (int q = 0; q < 5; ++q) asm volatile("prefetch.global.L2 [%0];" ::"l"(c + q * PS));
+      if (THREED && z + 3 < g.az1) {
+        // the own column's loads of the next plane iteration
+        const long long o3 = g.base + gx + (long long)gy * g.sy + (long long)(z + 3) * g.sz;
+#pragma unroll
+        for (int q = 0; q < 5; ++q) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.Y + o3 + q * PS));
+#pragma unroll
+        for (int q = 0; q < 3; ++q) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.U + o3 + q * PS));
+      }
     }
     Prim P2;
     FaceState mz1, pz1;
