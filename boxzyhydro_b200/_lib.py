@@ -122,6 +122,7 @@ def lib():
         "bx_adj_backward": (C.c_int, [H, vp, vp]),
         "bx_adj_stats": (C.c_int, [H, dp, dp, i64p, i64p]),
         "bx_adj_dts": (C.c_int, [H, dp]),
+        "bx_adj_plan": (C.c_int, [C.c_int64, C.c_int32, i64p, i64p, i32p]),
         "bx_adj_last_error": (C.c_char_p, [H]),
     }
     for name, (res, args) in sig.items():

@@ -77,6 +77,22 @@ class AdjointEngine:
         return out
 
 
+def plan(nsteps: int, snapshots: int) -> dict:
+    """The checkpoint schedule of an nsteps run with `snapshots` plane sets,
+    computed on the host (no device): forward steps recomputed by the first
+    backward after a forward (`recomputed_first`, what `stats()` reports) and by
+    a further backward of the same run (`recomputed_again`), and the snapshots
+    the forward run stores on its way (`chain_snapshots`)."""
+    first, again = C.c_int64(), C.c_int64()
+    chain = C.c_int32()
+    rc = lib().bx_adj_plan(int(nsteps), int(snapshots), C.byref(first), C.byref(again),
+                           C.byref(chain))
+    if rc:
+        raise BoxzyError(rc, lib().bx_adj_last_error(None).decode())
+    return dict(recomputed_first=first.value, recomputed_again=again.value,
+                chain_snapshots=chain.value)
+
+
 def _torch():
     import torch
     return torch

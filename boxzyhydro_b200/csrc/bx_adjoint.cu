@@ -651,8 +651,8 @@ __global__ void k_record_dt(const Ctrl* c, double* dts, long long k) { dts[k] = 
 // The snapshots of the first chain of splits are stored by the forward run
 // itself, so their advances cost nothing:
 //   F(l, s) = min_m  F(l-m, s-1) + C(m, s),   F(l, 0) = C(l, 0).
-// Solved by dynamic programming when l^2 s is small enough; otherwise the split
-// follows the binomial rule (largest right part reversible with r repetitions).
+// Solved by dynamic programming when l^2 s is small enough; otherwise by the
+// closed-form split rules of split_of, which reach the same optimum.
 struct Schedule {
   long long L = 0;
   int S = 0;
@@ -898,25 +898,87 @@ static void give_slot(bx_adj* A, double* p) {
     if (A->pool[k] == p) A->pool_free.push_back((int)k);
 }
 
+// binomial coefficient (n over k), saturating at 2^50 (far above any step count)
 static long long binom(long long n, long long k) {
   if (k < 0 || k > n) return 0;
+  k = std::min(k, n - k);
+  const long long cap = 1ll << 50;
   long long r = 1;
   for (long long i = 1; i <= k; ++i) {
-    r = r * (n - k + i) / i;
-    if (r > (1ll << 50)) return 1ll << 50;
+    // r = (n-k+i over i) after this line: the division is exact
+    const __int128 v = (__int128)r * (n - k + i) / i;
+    if (v > cap) return cap;
+    r = (long long)v;
   }
   return r;
 }
 
-static long long binom(long long n, long long k);
+// beta(c, r) = (c + r over c): the most steps c checkpoints reverse with r
+// repetitions (Griewank 1992, "Achieving logarithmic growth of temporal and
+// spatial complexity in reverse automatic differentiation"); 0 for r < 0
+static long long beta(long long c, long long r) { return r < 0 ? 0 : binom(c + r, c); }
 
+// First split m (1 <= m < l) of reversing l steps with s >= 1 free slots.
+// Beyond the dynamic programme's table the split follows closed-form rules with
+// the same optimum.  C (repeated reversal): with c = s + 1 checkpoints (the held
+// state and the free slots) and r the smallest repetition number with
+// beta(c, r) >= l, C(l, s) = r l - beta(c + 1, r - 1), and a split is optimal when
+//   max(beta(c, r-2), l - beta(c-1, r)) <= m <= min(beta(c, r-1), l - beta(c-1, r-1)).
+// F (the chain the forward run stores): the chain spreads l steps over segments
+// reversed with s, s-1, ..., 0 free slots, each costing C, which is convex in the
+// segment length with slope r.  A segment with k slots holds up to beta(k+1, lam)
+// steps at marginal cost <= lam, all of them together beta(s+1, lam+1) - 1; with
+// the smallest lam that holds l, the first segment takes
+//   m = max(beta(s+1, lam-1), l - beta(s, lam+1) + 1).
 static long long split_of(const Schedule& sc, bool chain, long long l, int s) {
   if (sc.dp && l <= sc.L && s <= sc.S) return chain ? sc.mf[sc.at(l, s)] : sc.mc[sc.at(l, s)];
-  long long r = 1;
-  while (binom(s + r, s) < l) ++r;
-  long long l2 = std::min(binom(s - 1 + r, s - 1), l - 1);
-  if (l2 < 1) l2 = 1;
-  return l - l2;
+  if (s >= l - 1) return 1;
+  long long m;
+  if (chain) {
+    long long lam = 0;
+    while (beta(s + 1, lam + 1) - 1 < l) ++lam;
+    m = std::max(beta(s + 1, lam - 1), l - beta(s, lam + 1) + 1);
+  } else {
+    const long long c = s + 1;
+    long long r = 0;
+    while (beta(c, r) < l) ++r;
+    m = std::max(beta(c, r - 2), l - beta(c - 1, r));
+  }
+  return std::min(std::max(m, 1ll), l - 1);
+}
+
+// the chain of snapshots the unfrozen forward run stores: the step index of each
+// split of the first chain of the recursion
+static std::vector<long long> chain_of(const Schedule& sc, long long nsteps, int snaps) {
+  std::vector<long long> chain;
+  long long a = 0, l = nsteps;
+  for (int sl = snaps; l > 1 && sl > 0; --sl) {
+    const long long m = split_of(sc, true, l, sl);
+    a += m;
+    l -= m;
+    chain.push_back(a);
+  }
+  return chain;
+}
+
+// Recomputed steps of reverse_range over l steps, counted on the host: the same
+// walk with the free-slot and chain counters in place of the plane sets.
+static long long plan_range(const Schedule& sc, long long l, bool chain, int& free_slots,
+                            int& chain_left) {
+  if (l <= 1) return 0;
+  const int s = free_slots + (chain ? chain_left : 0);
+  if (s == 0) return l * (l - 1) / 2;
+  const long long m = split_of(sc, chain, l, s);
+  long long n = 0;
+  if (chain) {
+    chain_left -= 1;
+  } else {
+    free_slots -= 1;
+    n += m;
+  }
+  n += plan_range(sc, l - m, chain, free_slots, chain_left);
+  free_slots += 1;
+  return n + plan_range(sc, m, false, free_slots, chain_left);
 }
 
 // state of step `to` from the state of step `from` (held in src) into dst,
@@ -1050,18 +1112,8 @@ int bx_adj_create(const bx_params* params, int64_t nsteps, int32_t snapshots, bx
   if ((rc = amalloc(A, &A->d_dts, nsteps))) return fail(rc);
   build_schedule(A->sched, nsteps, A->snaps);
   A->chain_slot_of.assign(nsteps + 1, -1);
-  {
-    long long a = 0, l = nsteps;
-    int sl = A->snaps;
-    while (l > 1 && sl > 0) {
-      const long long m = split_of(A->sched, true, l, sl);
-      a += m;
-      l -= m;
-      A->chain_slot_of[a] = 1 + (int)A->chain.size();
-      A->chain.push_back(a);
-      --sl;
-    }
-  }
+  A->chain = chain_of(A->sched, nsteps, A->snaps);
+  for (size_t j = 0; j < A->chain.size(); ++j) A->chain_slot_of[A->chain[j]] = 1 + (int)j;
   *out = A;
   return BX_OK;
 }
@@ -1245,6 +1297,24 @@ int bx_adj_stats(bx_adj* A, double* ms_forward, double* ms_backward, int64_t* re
   if (ms_backward) *ms_backward = A->ms_bwd;
   if (recomputed_steps) *recomputed_steps = A->fwd_steps_in_bwd;
   if (device_bytes) *device_bytes = (int64_t)A->bytes;
+  return BX_OK;
+}
+
+int bx_adj_plan(int64_t nsteps, int32_t snapshots, int64_t* recomputed_first,
+                int64_t* recomputed_again, int32_t* chain_snapshots) {
+  if (nsteps <= 0 || snapshots < 1) return aerr(nullptr, BX_ERR_ARG, "bad arguments");
+  const int snaps = (int)std::min<long long>(snapshots, nsteps);
+  Schedule sc;
+  build_schedule(sc, nsteps, snaps);
+  const std::vector<long long> chain = chain_of(sc, nsteps, snaps);
+  int free_slots = snaps - (int)chain.size(), chain_left = (int)chain.size();
+  if (recomputed_first)
+    *recomputed_first = plan_range(sc, nsteps, true, free_slots, chain_left);
+  free_slots = snaps;
+  chain_left = 0;
+  if (recomputed_again)
+    *recomputed_again = plan_range(sc, nsteps, false, free_slots, chain_left);
+  if (chain_snapshots) *chain_snapshots = (int32_t)chain.size();
   return BX_OK;
 }
 

@@ -279,6 +279,14 @@ int bx_adj_forward(bx_adj *a, const double *cons0, double *consT, int32_t frozen
 int bx_adj_backward(bx_adj *a, const double *lamT, double *lam0);
 int bx_adj_stats(bx_adj *a, double *ms_forward, double *ms_backward, int64_t *recomputed_steps,
                  int64_t *device_bytes);
+/* Host only (no device, no handle): the checkpoint schedule of an nsteps run with
+ * `snapshots` plane sets, for choosing the snapshot count before allocating.
+ * recomputed_first: forward steps the first bx_adj_backward after an unfrozen
+ * forward recomputes (bx_adj_stats' recomputed_steps); recomputed_again: those of a
+ * further backward of the same run; chain_snapshots: snapshots the forward run
+ * stores on its way.  Any output may be NULL. */
+int bx_adj_plan(int64_t nsteps, int32_t snapshots, int64_t *recomputed_first,
+                int64_t *recomputed_again, int32_t *chain_snapshots);
 int bx_adj_dts(bx_adj *a, double *dts);
 const char *bx_adj_last_error(bx_adj *a);
 

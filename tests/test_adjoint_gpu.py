@@ -7,7 +7,7 @@ import pytest
 import oracle as O
 import tangent as TLM
 from boxzyhydro_b200 import grid as G
-from boxzyhydro_b200.adjoint import AdjointEngine, AdjointRun
+from boxzyhydro_b200.adjoint import AdjointEngine, AdjointRun, plan
 from tests.helpers import small_random_box
 
 pytestmark = pytest.mark.gpu
@@ -129,6 +129,7 @@ def test_checkpoint_schedules_agree():
     lamT = rand_dir(hp, rng, np.ones(5))
     ref = bwd(eng1, lamT)
     s1 = eng1.stats()
+    assert s1["recomputed_steps"] == plan(6, 1)["recomputed_first"]
     eng1.close()
     for snaps in (2, 3, 6):
         eng = AdjointEngine(hp, 6, snaps)
@@ -137,6 +138,8 @@ def test_checkpoint_schedules_agree():
         assert np.array_equal(got, ref), snaps
         st_ = eng.stats()
         assert st_["recomputed_steps"] <= s1["recomputed_steps"]
+        # the host's plan of the schedule is the walk the engine took
+        assert st_["recomputed_steps"] == plan(6, snaps)["recomputed_first"], snaps
         eng.close()
 
 
