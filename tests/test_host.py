@@ -141,3 +141,82 @@ def test_units_and_muc_match_oracle():
     assert rgas_code_units() == O.rgas_code_units()
     assert muc_from_abundances() == O.muc()
     assert abs(muc_from_abundances() - 1.0 / 0.4325) < 1e-15
+
+
+# C types of the headers -> (kind, size) of the value passed
+_C_SCALARS = {"int": ("i", 4), "int32_t": ("i", 4), "int64_t": ("i", 8), "uint32_t": ("u", 4),
+              "uint8_t": ("u", 1), "unsigned long long": ("u", 8), "double": ("f", 8),
+              "char": ("i", 1), "void": ("v", 0)}
+_C_STRUCTS = {"bx_params": 136, "bx_eos_table": None}  # sizes checked elsewhere
+_C_OPAQUE = ("bx_handle", "bx_batch", "bx_adj")
+
+
+def header_prototypes():
+    """(name, return type, [(base type, pointer depth)]) of every prototype."""
+    out = []
+    for hdr in ("boxzy_gpu.h", "boxzy_diag.h"):
+        text = open(os.path.join(ROOT, "include", hdr)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        text = re.sub(r"^\s*#.*$", "", text, flags=re.M)
+        for m in re.finditer(r"([\w\s]+?)\s*(\**)\s*(bx_\w+)\s*\(([^)]*)\)\s*;", text):
+            ret = (" ".join(m.group(1).replace("const", " ").split()), len(m.group(2)))
+            params = []
+            for p in m.group(4).split(","):
+                p = " ".join(p.replace("const", " ").split())
+                if p in ("", "void"):
+                    continue
+                depth = p.count("*")
+                toks = p.replace("*", " ").split()
+                params.append((" ".join(toks[:-1]), depth))
+            out.append((m.group(3), ret, params))
+    return out
+
+
+def _ctype_matches(c_type, ct):
+    base, depth = c_type
+    if depth == 0:
+        kind, size = _C_SCALARS[base]
+        if kind == "f":
+            return ct in (ctypes.c_double,)
+        return (ct is not None and issubclass(ct, ctypes._SimpleCData) and ct not in
+                (ctypes.c_double, ctypes.c_float, ctypes.c_void_p, ctypes.c_char_p) and
+                ctypes.sizeof(ct) == size)
+    if base in _C_OPAQUE and depth == 1:
+        return ct is ctypes.c_void_p
+    if ct is ctypes.c_void_p:
+        return True  # any pointer may be passed as an address
+    if base == "char" and depth == 1:
+        return ct is ctypes.c_char_p
+    if not (isinstance(ct, type) and issubclass(ct, ctypes._Pointer)):
+        return False
+    inner = ct._type_
+    if depth > 1 or base in _C_OPAQUE:
+        return inner is ctypes.c_void_p if depth == 2 or base in _C_OPAQUE else False
+    if base in _C_STRUCTS:
+        return inner.__name__.lower().replace("_", "") == base.replace("_", "")
+    return _ctype_matches((base, 0), inner)
+
+
+def test_ctypes_signatures_match_the_header():
+    """Every prototype of include/*.h has argtypes and restype in the Python layer
+    whose widths and kinds match the C declaration (an int32/int64 slip would
+    pass garbage through the ABI without an error)."""
+    L = _lib.lib()
+    protos = header_prototypes()
+    assert len(protos) == len(header_functions())
+    bad = []
+    for name, ret, params in protos:
+        f = getattr(L, name)
+        if f.argtypes is None:
+            bad.append(f"{name}: no argtypes")
+            continue
+        if len(f.argtypes) != len(params):
+            bad.append(f"{name}: {len(f.argtypes)} argtypes for {len(params)} parameters")
+            continue
+        for k, (p, ct) in enumerate(zip(params, f.argtypes)):
+            if not _ctype_matches(p, ct):
+                bad.append(f"{name} arg {k}: C {p} vs ctypes {ct}")
+        want_ret = ctypes.c_char_p if ret == ("char", 1) else ctypes.c_int
+        if f.restype is not want_ret:
+            bad.append(f"{name}: restype {f.restype} for C {ret}")
+    assert not bad, bad
