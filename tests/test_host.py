@@ -220,3 +220,142 @@ def test_ctypes_signatures_match_the_header():
         if f.restype is not want_ret:
             bad.append(f"{name}: restype {f.restype} for C {ret}")
     assert not bad, bad
+
+
+def _split_top(s):
+    """Split on commas outside parentheses."""
+    out, depth, cur = [], 0, ""
+    for ch in s:
+        depth += ch == "("
+        depth -= ch == ")"
+        if ch == "," and depth == 0:
+            out.append(cur.strip())
+            cur = ""
+        else:
+            cur += ch
+    if cur.strip():
+        out.append(cur.strip())
+    return out
+
+
+def _fortran_blocks():
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    return re.findall(r"```fortran\n(.*?)```", text, flags=re.S)
+
+
+def fortran_module():
+    mod = [b for b in _fortran_blocks() if b.startswith("module boxzy_gpu")]
+    assert len(mod) == 1
+    src = re.sub(r"!.*", "", mod[0])
+    return re.sub(r"&\s*\n\s*", " ", src)
+
+
+def _fortran_decls(body):
+    decls = {}
+    for stmt in re.split(r"[;\n]", body):
+        stmt = stmt.strip()
+        if "::" not in stmt:
+            continue
+        left, names = stmt.split("::")
+        parts = _split_top(left)
+        spec, attrs = parts[0].replace(" ", ""), [a.replace(" ", "") for a in parts[1:]]
+        for n in _split_top(names):
+            m = re.match(r"(\w+)\s*(\((.*)\))?", n)
+            decls[m.group(1)] = (spec, "value" in attrs, m.group(3))
+    return decls
+
+
+def _header_structs():
+    out = {}
+    for hdr in ("boxzy_gpu.h",):
+        text = open(os.path.join(ROOT, "include", hdr)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"typedef struct (\w+) \{(.*?)\} \1;", text, flags=re.S):
+            fields = []
+            for decl in m.group(2).split(";"):
+                decl = " ".join(decl.replace("const", " ").split())
+                if not decl:
+                    continue
+                base = decl.split()[0]
+                for n in decl[len(base):].split(","):
+                    n = n.strip()
+                    ptr = n.startswith("*")
+                    mm = re.match(r"\*?\s*(\w+)(\[(\d+)\])?", n)
+                    kind = ("ptr", 8) if ptr else (_C_SCALARS[base][0], _C_SCALARS[base][1])
+                    fields += [(mm.group(1), kind)] * int(mm.group(3) or 1)
+            out[m.group(1)] = fields
+    return out
+
+
+_F_KINDS = {"real(c_double)": ("f", 8), "integer(c_int64_t)": ("i", 8),
+            "integer(c_int32_t)": ("i", 4), "integer(c_int)": ("i", 4), "type(c_ptr)": ("ptr", 8)}
+
+
+def _fortran_matches(decl, c_param):
+    spec, value, dims = decl
+    base, depth = c_param
+    if spec == "type(c_ptr)":
+        return depth >= 1 if value else depth == 2
+    if spec.startswith("type("):  # a bind(c) derived type, passed by reference
+        return not value and depth == 1 and base == spec[5:-1]
+    if spec == "character(kind=c_char)":
+        return base == "char" and depth == 1 and dims == "*"
+    kind, size = _F_KINDS[spec]
+    if value != (depth == 0) or (value and dims):
+        return False
+    ck, cs = _C_SCALARS[base]
+    return cs == size and (ck == kind or (kind == "i" and ck == "u"))
+
+
+def test_fortran_interfaces_match_the_header():
+    """The ISO_C_BINDING module of the integration guide (what a maintainer adds
+    to the reference) against include/boxzy_gpu.h: every interface binds an
+    exported C name with the right argument count, kinds, widths and passing
+    (value or reference), its bind(c) types lay out the C structs field by field,
+    and every bx_ call of the guide's Fortran snippets has an interface."""
+    src = fortran_module()
+    protos = {n: (r, p) for n, r, p in header_prototypes()}
+    bad, fnames = [], set()
+    funcs = re.finditer(r"(integer\(c_int\)|type\(c_ptr\))\s+function\s+(\w+)\s*\(([^)]*)\)\s*"
+                        r"bind\(c,\s*name=\"(\w+)\"\)(.*?)end function", src, flags=re.S)
+    for m in funcs:
+        res, fname, args, cname, body = m.groups()
+        fnames.add(fname)
+        if cname not in protos:
+            bad.append(f"{fname}: {cname} is not declared in the header")
+            continue
+        ret, params = protos[cname]
+        want = ("int", 0) if res == "integer(c_int)" else None
+        if (want and ret != want) or (not want and ret[1] == 0):
+            bad.append(f"{fname}: result {res} for C {ret}")
+        names = [a.strip() for a in args.split(",") if a.strip()]
+        if len(names) != len(params):
+            bad.append(f"{fname}: {len(names)} dummies for {len(params)} C parameters")
+            continue
+        decls = _fortran_decls(body)
+        for k, (n, p) in enumerate(zip(names, params)):
+            if n not in decls or not _fortran_matches(decls[n], p):
+                bad.append(f"{fname} dummy {k} ({n}): {decls.get(n)} vs C {p}")
+    assert len(fnames) >= 25, sorted(fnames)
+    # bind(c) derived types against the C structs
+    structs = _header_structs()
+    for m in re.finditer(r"type, bind\(c\) :: (\w+)(.*?)end type", src, flags=re.S):
+        name, body = m.groups()
+        fields = []
+        for stmt in body.strip().split("\n"):
+            left, names = stmt.split("::")
+            for n in _split_top(names):
+                mm = re.match(r"(\w+)(\((\d+)\))?", n)
+                fields += [(mm.group(1), _F_KINDS[left.strip()])] * int(mm.group(3) or 1)
+        if fields != structs.get(name):
+            bad.append(f"type {name}: {fields} vs C {structs.get(name)}")
+    # calls in the guide's Fortran snippets
+    called = set()
+    for b in _fortran_blocks():
+        if b.startswith("module boxzy_gpu"):
+            continue
+        called |= set(re.findall(r"\b(bx_\w+)\s*\(", re.sub(r"!.*", "", b)))
+    types = {"bx_params", "bx_eos_table"}
+    missing = sorted(called - fnames - types - {"bx_message"})
+    assert not missing, missing
+    assert not bad, bad
