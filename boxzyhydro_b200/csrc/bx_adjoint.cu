@@ -749,6 +749,21 @@ struct bx_adj {
 
 static std::string g_adj_err;
 
+// two timing events, destroyed when the scope ends (on the error returns too)
+struct EventPair {
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  EventPair() {
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+  }
+  ~EventPair() {
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+  }
+  EventPair(const EventPair&) = delete;
+  EventPair& operator=(const EventPair&) = delete;
+};
+
 #define ACK(expr)                                                     \
   do {                                                                \
     cudaError_t e_ = (expr);                                          \
@@ -1176,10 +1191,8 @@ int bx_adj_forward(bx_adj* A, const double* cons0, double* consT, int32_t frozen
   const Geom& g = h->g;
   cudaStream_t s = h->stream;
   const long long n5 = 5 * g.ng;
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  ACK(cudaEventRecord(e0, s));
+  EventPair ev;
+  ACK(cudaEventRecord(ev.e0, s));
   // the unfrozen run keeps its initial state and the chain snapshots for the
   // backward pass; frozen runs start from lamB and store nothing
   double* X0 = frozen ? A->lamB : A->pool[0];
@@ -1221,12 +1234,10 @@ int bx_adj_forward(bx_adj* A, const double* cons0, double* consT, int32_t frozen
     nsrc = 2;
     cur = out;
   }
-  ACK(cudaEventRecord(e1, s));
-  ACK(cudaEventSynchronize(e1));
+  ACK(cudaEventRecord(ev.e1, s));
+  ACK(cudaEventSynchronize(ev.e1));
   float ms = 0.f;
-  cudaEventElapsedTime(&ms, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  cudaEventElapsedTime(&ms, ev.e0, ev.e1);
   if (!frozen) {
     A->ms_fwd = ms;
     ACK(cudaMemcpy(A->dts.data(), A->d_dts, A->nsteps * sizeof(double), cudaMemcpyDeviceToHost));
@@ -1259,10 +1270,8 @@ int bx_adj_backward(bx_adj* A, const double* lamT, double* lam0) {
   const Geom& g = h->g;
   cudaStream_t s = h->stream;
   const long long n5 = 5 * g.ng;
-  cudaEvent_t e0, e1;
-  cudaEventCreate(&e0);
-  cudaEventCreate(&e1);
-  ACK(cudaEventRecord(e0, s));
+  EventPair ev;
+  ACK(cudaEventRecord(ev.e0, s));
   A->fwd_steps_in_bwd = 0;
   std::fill(A->c1tag.begin(), A->c1tag.end(), -1);
   A->c1_hits = 0;
@@ -1280,12 +1289,10 @@ int bx_adj_backward(bx_adj* A, const double* lamT, double* lam0) {
   // without a new forward rebuilds them
   A->chain_valid = false;
   if (int r = reverse_range(A, A->pool[0], 0, A->nsteps, lam, chain)) return r;
-  ACK(cudaEventRecord(e1, s));
-  ACK(cudaEventSynchronize(e1));
+  ACK(cudaEventRecord(ev.e1, s));
+  ACK(cudaEventSynchronize(ev.e1));
   float ms = 0.f;
-  cudaEventElapsedTime(&ms, e0, e1);
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  cudaEventElapsedTime(&ms, ev.e0, ev.e1);
   A->ms_bwd = ms;
   return BX_OK;
 }
