@@ -671,46 +671,67 @@ static void flux_hll(const double fl[5], const double fr[5], const double ul[5],
   for (int i = 0; i < 5; ++i) fhll[i] = (ap * fl[i] + am * fr[i] - ap * am * (ur[i] - ul[i])) / (ap + am);
 }
 
+/* flux.f90:513-573: the HLL flux of one face from its left and right
+ * reconstructed states, each (rho, u1, u2, u3, p, eps, gamma); idir 0..2 */
+static void face_flux(const double L[7], const double R[7], int idir, double fhll[5]) {
+  double dl = L[0], pl = L[4], el = L[5], gl = L[6];
+  double vxl = L[1], vyl = L[2], vzl = L[3];
+  double sl[5], sr[5], fl[5], fr[5];
+  sl[0] = dl;
+  sl[1] = dl * vxl;
+  sl[2] = dl * vyl;
+  sl[3] = dl * vzl;
+  sl[4] = el + HALF * dl * (vxl * vxl + vyl * vyl + vzl * vzl);
+  double dr = R[0], pr = R[4], er = R[5], gr = R[6];
+  double vxr = R[1], vyr = R[2], vzr = R[3];
+  sr[0] = dr;
+  sr[1] = dr * vxr;
+  sr[2] = dr * vyr;
+  sr[3] = dr * vzr;
+  sr[4] = er + HALF * dr * (vxr * vxr + vyr * vyr + vzr * vzr);
+  for (int k = 0; k < 5; ++k) { fl[k] = ZERO; fr[k] = ZERO; }
+  double vr, vl;
+  if (idir == 0) { vr = vxr; vl = vxl; fl[1] = pl; fr[1] = pr; }
+  else if (idir == 1) { vr = vyr; vl = vyl; fl[2] = pl; fr[2] = pr; }
+  else { vr = vzr; vl = vzl; fl[3] = pl; fr[3] = pr; }
+  fl[0] = sl[0] * vl;
+  fl[1] = fl[1] + sl[1] * vl;
+  fl[2] = fl[2] + sl[2] * vl;
+  fl[3] = fl[3] + sl[3] * vl;
+  fl[4] = (sl[4] + pl) * vl;
+  fr[0] = sr[0] * vr;
+  fr[1] = fr[1] + sr[1] * vr;
+  fr[2] = fr[2] + sr[2] * vr;
+  fr[3] = fr[3] + sr[3] * vr;
+  fr[4] = (sr[4] + pr) * vr;
+  flux_hll(fl, fr, sl, sr, gl, gr, dl, dr, pl, pr, vl, vr, fhll);
+}
+
 /* flux.f90:487-573; isten = (minus, centre, plus), idir 0..2; fhll[2][5] */
 static void get_fluxes(const ox_sim *s, const int64_t isten[3], int idir, double fhll[2][5]) {
   for (int m_or_p = 0; m_or_p <= 1; ++m_or_p) {
     const int64_t a = isten[m_or_p], b = isten[1 + m_or_p];
-    double dl = s->st_d_p[3 * a + idir], pl = s->st_p_p[3 * a + idir];
-    double el = s->st_e_p[3 * a + idir], gl = s->st_g_p[3 * a + idir];
-    double vxl = s->st_u_p[9 * a + 3 * idir + 0], vyl = s->st_u_p[9 * a + 3 * idir + 1],
-           vzl = s->st_u_p[9 * a + 3 * idir + 2];
-    double sl[5], sr[5], fl[5], fr[5];
-    sl[0] = dl;
-    sl[1] = dl * vxl;
-    sl[2] = dl * vyl;
-    sl[3] = dl * vzl;
-    sl[4] = el + HALF * dl * (vxl * vxl + vyl * vyl + vzl * vzl);
-    double dr = s->st_d_m[3 * b + idir], pr = s->st_p_m[3 * b + idir];
-    double er = s->st_e_m[3 * b + idir], gr = s->st_g_m[3 * b + idir];
-    double vxr = s->st_u_m[9 * b + 3 * idir + 0], vyr = s->st_u_m[9 * b + 3 * idir + 1],
-           vzr = s->st_u_m[9 * b + 3 * idir + 2];
-    sr[0] = dr;
-    sr[1] = dr * vxr;
-    sr[2] = dr * vyr;
-    sr[3] = dr * vzr;
-    sr[4] = er + HALF * dr * (vxr * vxr + vyr * vyr + vzr * vzr);
-    for (int k = 0; k < 5; ++k) { fl[k] = ZERO; fr[k] = ZERO; }
-    double vr, vl;
-    if (idir == 0) { vr = vxr; vl = vxl; fl[1] = pl; fr[1] = pr; }
-    else if (idir == 1) { vr = vyr; vl = vyl; fl[2] = pl; fr[2] = pr; }
-    else { vr = vzr; vl = vzl; fl[3] = pl; fr[3] = pr; }
-    fl[0] = sl[0] * vl;
-    fl[1] = fl[1] + sl[1] * vl;
-    fl[2] = fl[2] + sl[2] * vl;
-    fl[3] = fl[3] + sl[3] * vl;
-    fl[4] = (sl[4] + pl) * vl;
-    fr[0] = sr[0] * vr;
-    fr[1] = fr[1] + sr[1] * vr;
-    fr[2] = fr[2] + sr[2] * vr;
-    fr[3] = fr[3] + sr[3] * vr;
-    fr[4] = (sr[4] + pr) * vr;
-    flux_hll(fl, fr, sl, sr, gl, gr, dl, dr, pl, pr, vl, vr, fhll[m_or_p]);
+    /* left: the plus state of cell a, right: the minus state of cell b */
+    const double L[7] = {s->st_d_p[3 * a + idir], s->st_u_p[9 * a + 3 * idir + 0],
+                         s->st_u_p[9 * a + 3 * idir + 1], s->st_u_p[9 * a + 3 * idir + 2],
+                         s->st_p_p[3 * a + idir], s->st_e_p[3 * a + idir],
+                         s->st_g_p[3 * a + idir]};
+    const double R[7] = {s->st_d_m[3 * b + idir], s->st_u_m[9 * b + 3 * idir + 0],
+                         s->st_u_m[9 * b + 3 * idir + 1], s->st_u_m[9 * b + 3 * idir + 2],
+                         s->st_p_m[3 * b + idir], s->st_e_m[3 * b + idir],
+                         s->st_g_m[3 * b + idir]};
+    face_flux(L, R, idir, fhll[m_or_p]);
   }
+}
+
+/* Known-answer probes of the building blocks above, for the oracle's own tests. */
+double ox_kat_genminmod(double x1, double x2, double x3) { return genminmod(x1, x2, x3); }
+double ox_kat_slope(double c0, double c1, double c2) { return slope(c0, c1, c2); }
+void ox_kat_muscl(double q, double lm, double lp, double sl, double *minus, double *plus) {
+  interface_muscl(q, lm, lp, sl, minus, plus);
+}
+void ox_kat_face_flux(const double *left7, const double *right7, int idir, double *f5) {
+  face_flux(left7, right7, idir, f5);
 }
 
 /* flux.f90:6-235 (anchors, flux.f90:134-184 and 592-601, need boundary>2 cells,

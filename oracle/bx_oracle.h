@@ -99,6 +99,15 @@ void ox_set_threads(int n);
 double ox_rgas_code_units(void);   /* units.f90:10-17 */
 double ox_muc(double xabun, double yabun, double zabun, double mu_z); /* eos.f90:144 */
 
+/* Known-answer probes (tests only): genminmod (utils.f90:696-707), slope with
+ * theta = SLOPE_THETA (utils.f90:738-741), interface_muscl (flux.f90:299-308) and
+ * the HLL flux of one face (flux.f90:513-590) from left/right reconstructed
+ * states (rho, u1, u2, u3, p, eps, gamma). */
+double ox_kat_genminmod(double x1, double x2, double x3);
+double ox_kat_slope(double c0, double c1, double c2);
+void ox_kat_muscl(double q, double lm, double lp, double sl, double *minus, double *plus);
+void ox_kat_face_flux(const double *left7, const double *right7, int idir, double *f5);
+
 #ifdef __cplusplus
 }
 #endif

@@ -79,6 +79,11 @@ def lib():
         L.ox_get_muc.argtypes = [P, C.c_void_p]
         L.ox_muc.restype = C.c_double
         L.ox_muc.argtypes = [C.c_double] * 4
+        for fn in ("ox_kat_genminmod", "ox_kat_slope"):
+            getattr(L, fn).restype = C.c_double
+            getattr(L, fn).argtypes = [C.c_double] * 3
+        L.ox_kat_muscl.argtypes = [C.c_double] * 4 + [dp, dp]
+        L.ox_kat_face_flux.argtypes = [C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
         _lib = L
     return _lib
 
@@ -267,3 +272,29 @@ def rgas_code_units():
 
 def muc(xabun=0.73, yabun=0.27, zabun=0.0, mu_z=16.78):
     return lib().ox_muc(xabun, yabun, zabun, mu_z)
+
+
+# known-answer probes of the restatement's building blocks (its own tests)
+def kat_genminmod(x1, x2, x3):
+    return lib().ox_kat_genminmod(float(x1), float(x2), float(x3))
+
+
+def kat_slope(c0, c1, c2):
+    return lib().ox_kat_slope(float(c0), float(c1), float(c2))
+
+
+def kat_muscl(q, lm, lp, sl):
+    """(minus, plus) face states of interface_muscl."""
+    m, p = C.c_double(), C.c_double()
+    lib().ox_kat_muscl(float(q), float(lm), float(lp), float(sl), C.byref(m), C.byref(p))
+    return m.value, p.value
+
+
+def kat_face_flux(left, right, idir):
+    """HLL flux (5,) of one face; left/right = (rho, u1, u2, u3, p, eps, gamma)."""
+    L = np.ascontiguousarray(left, dtype=np.float64)
+    R = np.ascontiguousarray(right, dtype=np.float64)
+    assert L.shape == (7,) and R.shape == (7,) and idir in (0, 1, 2)
+    f = np.empty(5)
+    lib().ox_kat_face_flux(_ptr(L), _ptr(R), int(idir), _ptr(f))
+    return f
