@@ -113,8 +113,20 @@ class ClockSampler:
         return out
 
 
-def cpu_sample(st, steps=3, threads=None):
-    """The oracle (reference algorithm, OpenMP) on `steps` steps of the state."""
+def timed_steps(step, min_steps, seconds, max_steps=200):
+    """Run step() at least min_steps times and until `seconds` of host time have
+    passed (at most max_steps): a bounded sample.  Returns (steps, seconds)."""
+    n = 0
+    t0 = time.perf_counter()
+    while n < min_steps or (n < max_steps and time.perf_counter() - t0 < seconds):
+        step()
+        n += 1
+    return n, time.perf_counter() - t0
+
+
+def cpu_sample(st, steps=2, seconds=10.0, threads=None):
+    """The oracle (reference algorithm, OpenMP) on at least `steps` steps and
+    `seconds` of host time of the state, after one warm-up step."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     threads = threads or os.cpu_count()
@@ -122,13 +134,10 @@ def cpu_sample(st, steps=3, threads=None):
     o = O.Oracle(st.params, racy_ghosts=True)
     o.set_state(st.cons, st.u, st.p, st.adindx)
     o.step()  # warm-up (first touch of every array)
-    t0 = time.perf_counter()
-    for _ in range(steps):
-        o.step()
-    dt = time.perf_counter() - t0
+    n, dt = timed_steps(o.step, steps, seconds)
     o.close()
     cells = st.params.n_active()
-    return cells * steps / dt, threads, dt
+    return cells * n / dt, threads, dt, n
 
 
 def physics_arm(args, rank, world, local):
@@ -213,14 +222,11 @@ def physics_arm(args, rank, world, local):
                 o.step()
 
             cpu_one()
-            t0 = time.perf_counter()
-            for _ in range(args.cpu_steps):
-                cpu_one()
-            secs = time.perf_counter() - t0
+            n, secs = timed_steps(cpu_one, args.cpu_steps, args.cpu_seconds)
             o.close()
             rec["cpu_baseline"] = {
-                "value": cells * args.cpu_steps / secs, "unit": UNIT, "cores": threads,
-                "kind": "port", "sample": f"{args.cpu_steps} steps after one warm-up step "
+                "value": cells * n / secs, "unit": UNIT, "cores": threads,
+                "kind": "port", "sample": f"{n} steps after one warm-up step "
                                           f"({secs:.1f} s), oracle/bx_oracle.c, OpenMP"}
         out[name] = rec
     line = {"metric": METRIC, "unit": UNIT, "n_gpus": 1, "warmup": args.warmup,
@@ -568,7 +574,10 @@ def main():
     ap.add_argument("--ref-n", type=int, default=128, dest="ref_n")
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--e2e-steps", type=int, default=10, dest="e2e_steps")
-    ap.add_argument("--cpu-steps", type=int, default=2, dest="cpu_steps")
+    ap.add_argument("--cpu-steps", type=int, default=2, dest="cpu_steps",
+                    help="least steps of the CPU baseline sample")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0, dest="cpu_seconds",
+                    help="least host seconds of the CPU baseline sample (at most 200 steps)")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--workload", default="turb", choices=["turb", "batched", "adjoint", "physics"])
@@ -766,9 +775,9 @@ def main():
     # ---- CPU baseline (rank 0, one GPU only)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        v, thr, secs = cpu_sample(st, steps=args.cpu_steps)
+        v, thr, secs, n = cpu_sample(st, steps=args.cpu_steps, seconds=args.cpu_seconds)
         cpu = {"value": v, "unit": UNIT, "cores": thr, "kind": "port",
-               "sample": f"{args.cpu_steps} steps of the same {args.n}^3 workload after one "
+               "sample": f"{n} steps of the same {args.n}^3 workload after one "
                          f"warm-up step ({secs:.1f} s), oracle/bx_oracle.c (C restatement of "
                          "the reference loop), OpenMP on all host threads"}
 
