@@ -1056,6 +1056,9 @@ int bx_ghost_plan(const bx_params* params, int64_t* nghost, int32_t* dst, int32_
   if (!params || !nghost) return set_err(nullptr, BX_ERR_ARG, "null argument");
   const bx_params& P = *params;
   if (P.nx < 5 || P.ny < 5 || P.nz < 1) return set_err(nullptr, BX_ERR_ARG, "grid too small");
+  // the plan holds int32 cell indices
+  if ((long long)P.nx * P.ny * P.nz >= (1ll << 31))
+    return set_err(nullptr, BX_ERR_ARG, "grid exceeds 2^31 cells");
   GhostTable T;
   build_ghost_tables(P, T);
   const size_t n = T.dst.size();

@@ -1,6 +1,8 @@
 """Host-side logic that needs no GPU: the C ABI library loads and exports every
-symbol of include/boxzy_gpu.h, its ghost-fill plans reproduce the oracle's
-set_ghost_cells sweeps exactly, namelist parsing, and grid geometry."""
+symbol of include/boxzy_gpu.h, the ctypes layer and the Fortran interface module
+of the integration guide bind those prototypes with matching argument types, its
+ghost-fill plans reproduce the oracle's set_ghost_cells sweeps exactly (and grids
+beyond int32 cell indices are refused), namelist parsing, and grid geometry."""
 import ctypes
 import os
 import re
@@ -359,3 +361,12 @@ def test_fortran_interfaces_match_the_header():
     missing = sorted(called - fnames - types - {"bx_message"})
     assert not missing, missing
     assert not bad, bad
+
+
+def test_ghost_plan_rejects_grids_beyond_int32_indices():
+    """The plan stores int32 cell indices: 1300^3 cells (> 2^31) is refused before
+    any table is built, like bx_create refuses it."""
+    hp = HydroParams(nx=1300, ny=1300, nz=1300, dx=0.1, dy=0.1, dz=0.1, h2stat=-1,
+                     gammafix=1.4)
+    with pytest.raises(_lib.BoxzyError, match="2\\^31"):
+        ghost_plan(hp)
