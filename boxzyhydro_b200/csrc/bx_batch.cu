@@ -179,6 +179,7 @@ int bx_batch_create(int32_t nbox, const bx_params* params, bx_batch** out) {
   for (int i = 0; i < nbox; ++i) {
     const bx_params& P = b->P[i];
     if (P.h2stat != -1 || P.fluxangmom || P.nx < 5 || P.ny < 5 || P.nz < 1 ||
+        (long long)P.nx * P.ny * P.nz >= (1ll << 31) ||  // int32 cell indices of the plans
         !(P.dx >= 1e-40 && P.dx <= 1e40 && P.dy >= 1e-40 && P.dy <= 1e40 && P.dz >= 1e-40 &&
           P.dz <= 1e40 && P.gammafix > 1.0 && P.cfl > 0)) {
       bx_batch_destroy(b);

@@ -370,3 +370,15 @@ def test_ghost_plan_rejects_grids_beyond_int32_indices():
                      gammafix=1.4)
     with pytest.raises(_lib.BoxzyError, match="2\\^31"):
         ghost_plan(hp)
+
+
+def test_batch_refuses_a_box_beyond_int32_indices():
+    """Each box's ghost plan holds int32 cell indices: a 1300^3 box is refused
+    while the parameters are checked, before any device work."""
+    from boxzyhydro_b200.batch import Batch
+    hp = HydroParams(nx=1300, ny=1300, nz=1300, dx=0.1, dy=0.1, dz=0.1, h2stat=-1,
+                     gammafix=1.4, no_outflow_xl=False, no_outflow_xr=False,
+                     no_outflow_yl=False, no_outflow_yr=False, no_outflow_zl=False,
+                     no_outflow_zr=False)
+    with pytest.raises(_lib.BoxzyError, match="box 0"):
+        Batch([hp])
