@@ -7,7 +7,8 @@ states (a reflective wall: no mass or energy through it) and against a numpy
 restatement of the Harten-Lax-van Leer formula with Davis's wave-speed bounds;
 the conservative form of the update (interior faces cancel; totals change by
 the flux through the boundary faces, whose ghost states have no slope), and
-mass kept to round-off where the walls see no normal velocity."""
+mass kept to round-off where the walls see no normal velocity; the tabulated
+EOS on ideal-gas tables reproducing the fixed-gamma state."""
 import numpy as np
 import pytest
 
@@ -236,3 +237,55 @@ def test_mass_kept_where_walls_see_no_normal_velocity():
         assert abs(c1[inner, v].sum() - m0) <= 1e-14 * abs(m0), v
     assert not np.array_equal(c1[inner], c0[inner])
     o.close()
+
+
+def test_tabulated_state_of_an_ideal_gas_table_is_the_fixed_gamma_state():
+    """Tables of an ideal gas (gamma and mu constant, T = (gamma-1) eng mu / R at
+    every entry): get_gamma2's interpolation in energy and between density rows
+    is linear in a linear function, so the tabulated state() (state.f90:60-79,
+    eos.f90:653-699) gives the fixed-gamma pressure (state.f90:49-59) to
+    rounding, and gamma and mu exactly; energies beyond the table are clamped."""
+    import dataclasses
+    from boxzyhydro_b200.eos_table import synthetic_table
+    st = small_random_box(nx=12, ny=11, nz=10, walls=(0,) * 6, seed=7)
+    hp = st.params
+    gam, mu = 5.0 / 3.0, 2.3
+    tab = synthetic_table()
+    eng = tab["eng_table2"]
+    tab["gamma_table2"] = np.full_like(eng, gam)
+    tab["muc_table2"] = np.full_like(eng, mu)
+    tab["tk_table2"] = (gam - 1.0) * eng * mu / hp.rgas
+    rng = np.random.default_rng(12)
+    ng = hp.ngrid
+    rho = np.exp(rng.uniform(np.log(0.01), np.log(10.0), ng))  # across the density rows
+    u = rng.uniform(-1, 1, (ng, 3))
+    e_spec = np.exp(rng.uniform(np.log(0.3), np.log(5.0), ng))  # inside every row's range
+    cons = np.empty((ng, 5))
+    cons[:, 0] = rho
+    cons[:, 1:4] = rho[:, None] * u
+    cons[:, 4] = rho * e_spec + 0.5 * rho * (u * u).sum(axis=1)
+    res = {}
+    for h2stat in (-1, 0):
+        hq = dataclasses.replace(hp, h2stat=h2stat, gammafix=gam)
+        o = O.Oracle(hq)
+        if h2stat >= 0:
+            o.set_eos_table(tab)
+        o.set_state(cons, u, np.ones(ng), np.full(ng, gam))
+        o.state()
+        res[h2stat] = o.get_state()[2:], o.muc_array()
+        o.close()
+    (p_fix, g_fix), _ = res[-1]
+    (p_tab, g_tab), mu_tab = res[0]
+    assert np.allclose(p_tab, p_fix, rtol=1e-13, atol=0)
+    assert np.all(g_tab == gam) and np.all(mu_tab == mu)
+    # an energy above every row's table is clamped to the row's last entry
+    hq = dataclasses.replace(hp, h2stat=0, gammafix=gam)
+    o = O.Oracle(hq)
+    o.set_eos_table(tab)
+    hot = cons.copy()
+    hot[:, 4] = rho * 1e4 + 0.5 * rho * (u * u).sum(axis=1)
+    o.set_state(hot, u, np.ones(ng), np.full(ng, gam))
+    o.state()
+    p_hot = o.get_state()[2]
+    o.close()
+    assert np.all(p_hot < (gam - 1.0) * rho * eng.max() * (1 + 1e-12))
