@@ -110,8 +110,8 @@ static int create_handle(const bx_params* params, bx_handle** out, bool lean) {
   const bx_params& P = *params;
   if (P.h2stat < -1)
     return set_err(nullptr, BX_ERR_ARG, "H2STAT must be -1 (fixed gamma) or >= 0 (tables)");
-  if (P.nx < 5 || P.ny < 5 || P.nz < 1 || (P.nz >= 6 && P.nz < 5))
-    return set_err(nullptr, BX_ERR_ARG, "grid too small: need nx,ny>=5");
+  if (P.nx < 5 || P.ny < 5 || P.nz < 1)
+    return set_err(nullptr, BX_ERR_ARG, "grid too small: need nx,ny>=5, nz>=1");
   if ((long long)P.nx * P.ny * P.nz >= (1ll << 31))
     return set_err(nullptr, BX_ERR_ARG, "grid exceeds 2^31 cells");
   if (!(P.dx > 0 && P.dy > 0 && P.dz > 0 && P.gammafix > 1.0 && P.cfl > 0))

@@ -382,3 +382,24 @@ def test_batch_refuses_a_box_beyond_int32_indices():
                      no_outflow_zr=False)
     with pytest.raises(_lib.BoxzyError, match="box 0"):
         Batch([hp])
+
+
+@pytest.mark.parametrize("field,value,msg", [
+    ("nx", 4, "too small"), ("ny", 3, "too small"), ("nz", 0, "too small"),
+    ("h2stat", -2, "H2STAT"), ("dx", 0.0, ">0"), ("dy", float("nan"), ">0"),
+    ("gammafix", 1.0, "gammafix"), ("cfl", 0.0, ">0"), ("dz", 1e-50, "1e-40"),
+    ("nx", 1300, "2\\^31")])
+def test_create_refuses_invalid_parameters(field, value, msg):
+    """bx_create checks its parameters before any device work, so a refusal
+    needs no GPU: status BX_ERR_ARG and the message of bx_last_error(NULL)."""
+    hp = HydroParams(nx=12, ny=10, nz=8, dx=0.1, dy=0.1, dz=0.1, h2stat=-1, gammafix=1.4)
+    p = _lib.make_params(hp)
+    if field == "nx" and value == 1300:
+        p.nx = p.ny = p.nz = 1300
+    else:
+        setattr(p, field, value)
+    h = ctypes.c_void_p()
+    L = _lib.lib()
+    assert L.bx_create(ctypes.byref(p), ctypes.byref(h)) == 1  # BX_ERR_ARG
+    assert not h.value
+    assert re.search(msg, L.bx_last_error(None).decode())
