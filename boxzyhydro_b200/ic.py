@@ -110,12 +110,18 @@ def _kmag(shape):
 
 
 def _solenoidal(rng, shape, slope=-2.0):
-    """Divergence-free Gaussian vector field, P(k) ~ k^slope, components (vx,vy,vz)."""
+    """Divergence-free Gaussian vector field, P(k) ~ k^slope, components (vx,vy,vz).
+    The Nyquist planes of an even grid (a wavenumber component of n/2) carry no
+    field: a real field's mode there has no spectral derivative, so the
+    projection cannot make it divergence-free."""
     kz, ky, kx = _kvec(shape)
     k2 = kx * kx + ky * ky + kz * kz
     k2[0, 0, 0] = 1.0
     amp = np.where(k2 > 0, np.sqrt(k2) ** (slope / 2.0), 0.0)
     amp[0, 0, 0] = 0.0
+    for kc, n in ((kz, shape[0]), (ky, shape[1]), (kx, shape[2])):
+        if n % 2 == 0:
+            amp[np.abs(kc) == n // 2] = 0.0
     comps = [np.fft.rfftn(rng.standard_normal(shape)) * amp for _ in range(3)]
     vx, vy, vz = comps
     div = (kx * vx + ky * vy + kz * vz) / k2
