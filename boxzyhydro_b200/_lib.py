@@ -123,6 +123,8 @@ def lib():
         "bx_adj_stats": (C.c_int, [H, dp, dp, i64p, i64p]),
         "bx_adj_dts": (C.c_int, [H, dp]),
         "bx_adj_plan": (C.c_int, [C.c_int64, C.c_int32, i64p, i64p, i32p]),
+        "bx_adj_device_bytes": (C.c_int, [C.POINTER(BxParams), C.c_int64, C.c_int32, C.c_int32,
+                                          C.c_int32, i64p]),
         "bx_adj_last_error": (C.c_char_p, [H]),
     }
     for name, (res, args) in sig.items():

@@ -93,6 +93,19 @@ def plan(nsteps: int, snapshots: int) -> dict:
                 chain_snapshots=chain.value)
 
 
+def device_bytes(params: HydroParams, nsteps: int, snapshots: int, stage0_cache: int = 2,
+                 keep_stage0: bool = False) -> int:
+    """Device bytes of an engine for this grid (what `stats()` reports), computed
+    on the host, to size a run to the device before allocating."""
+    out = C.c_int64()
+    p = make_params(params)
+    rc = lib().bx_adj_device_bytes(C.byref(p), int(nsteps), int(snapshots), int(stage0_cache),
+                                   1 if keep_stage0 else 0, C.byref(out))
+    if rc:
+        raise BoxzyError(rc, lib().bx_adj_last_error(None).decode())
+    return out.value
+
+
 def _torch():
     import torch
     return torch

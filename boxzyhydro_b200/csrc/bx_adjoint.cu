@@ -1325,6 +1325,24 @@ int bx_adj_plan(int64_t nsteps, int32_t snapshots, int64_t* recomputed_first,
   return BX_OK;
 }
 
+int bx_adj_device_bytes(const bx_params* params, int64_t nsteps, int32_t snapshots,
+                        int32_t stage0_cache_entries, int32_t keep_stage0, int64_t* bytes) {
+  if (!params || !bytes || nsteps <= 0 || snapshots < 1 || stage0_cache_entries < 2 ||
+      params->nx < 5 || params->ny < 5 || params->nz < 1)
+    return aerr(nullptr, BX_ERR_ARG, "bad arguments");
+  const __int128 n = (__int128)params->nx * params->ny * params->nz;
+  const __int128 snaps = std::min<long long>(snapshots, nsteps);
+  // what bx_adj_create, bx_adj_stage0_cache and bx_adj_keep_stage0 allocate:
+  // plane sets of 5 x n doubles (the initial state and the snapshots, seven
+  // work sets, the stage-0 cache entries), the 14 primitive and adjoint planes,
+  // the dt record and, kept, the stage-0 result of every step
+  __int128 d = 5 * n * (snaps + 1 + 7 + stage0_cache_entries) + 14 * n + nsteps;
+  if (keep_stage0) d += (__int128)nsteps * 5 * n;
+  d *= (__int128)sizeof(double);
+  *bytes = d > (__int128)INT64_MAX ? INT64_MAX : (int64_t)d;
+  return BX_OK;
+}
+
 int bx_adj_dts(bx_adj* A, double* dts) {
   if (!A || !dts) return BX_ERR_ARG;
   std::memcpy(dts, A->dts.data(), A->nsteps * sizeof(double));

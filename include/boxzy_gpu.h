@@ -287,6 +287,13 @@ int bx_adj_stats(bx_adj *a, double *ms_forward, double *ms_backward, int64_t *re
  * stores on its way.  Any output may be NULL. */
 int bx_adj_plan(int64_t nsteps, int32_t snapshots, int64_t *recomputed_first,
                 int64_t *recomputed_again, int32_t *chain_snapshots);
+/* Host only: the device bytes an engine for this grid holds (bx_adj_stats'
+ * device_bytes) with `snapshots` plane sets, `stage0_cache_entries` cache
+ * entries (>= 2; bx_adj_stage0_cache) and the stage-0 results of every step kept
+ * or not (bx_adj_keep_stage0), to size a run to the device before allocating.
+ * The handle beneath the engine adds its ghost tables and tile list. */
+int bx_adj_device_bytes(const bx_params *params, int64_t nsteps, int32_t snapshots,
+                        int32_t stage0_cache_entries, int32_t keep_stage0, int64_t *bytes);
 int bx_adj_dts(bx_adj *a, double *dts);
 const char *bx_adj_last_error(bx_adj *a);
 

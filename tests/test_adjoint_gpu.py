@@ -7,7 +7,7 @@ import pytest
 import oracle as O
 import tangent as TLM
 from boxzyhydro_b200 import grid as G
-from boxzyhydro_b200.adjoint import AdjointEngine, AdjointRun, plan
+from boxzyhydro_b200.adjoint import AdjointEngine, AdjointRun, device_bytes, plan
 from tests.helpers import small_random_box
 
 pytestmark = pytest.mark.gpu
@@ -140,6 +140,7 @@ def test_checkpoint_schedules_agree():
         assert st_["recomputed_steps"] <= s1["recomputed_steps"]
         # the host's plan of the schedule is the walk the engine took
         assert st_["recomputed_steps"] == plan(6, snaps)["recomputed_first"], snaps
+        assert st_["device_bytes"] == device_bytes(hp, 6, snaps), snaps
         eng.close()
 
 

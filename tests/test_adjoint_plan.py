@@ -16,7 +16,8 @@ import numpy as np
 import pytest
 
 from boxzyhydro_b200._lib import BoxzyError
-from boxzyhydro_b200.adjoint import plan
+from boxzyhydro_b200 import ic
+from boxzyhydro_b200.adjoint import device_bytes, plan
 
 
 def closed_c(l, s):
@@ -105,3 +106,24 @@ def test_bad_arguments_are_rejected():
         plan(0, 3)
     with pytest.raises(BoxzyError):
         plan(10, 0)
+
+
+@pytest.mark.parametrize("n,nsteps,snaps,entries,keep,measured", [
+    # engine_device_bytes of the adjoint bench runs on a B200
+    (128, 200, 15, 8, False, 3109558336),     # C4
+    (128, 200, 15, 2, True, 20957310016),     # C4, stage-0 results kept
+    (128, 200, 199, 2, True, 37885074496),    # C4, every state kept
+    (512, 400, 11, 6, False, 152775565952)])  # C5
+def test_device_bytes_match_the_engines_measured(n, nsteps, snaps, entries, keep, measured):
+    hp = ic.turbulent_params(n)
+    assert device_bytes(hp, nsteps, snaps, entries, keep) == measured
+
+
+def test_device_bytes_grow_by_one_plane_set_per_snapshot():
+    hp = ic.turbulent_params(32)
+    one = 5 * hp.ngrid * 8
+    assert device_bytes(hp, 50, 8) - device_bytes(hp, 50, 7) == one
+    assert device_bytes(hp, 50, 8, stage0_cache=5) - device_bytes(hp, 50, 8) == 3 * one
+    assert device_bytes(hp, 50, 80) == device_bytes(hp, 50, 50)  # at most one per step
+    with pytest.raises(BoxzyError):
+        device_bytes(hp, 50, 8, stage0_cache=1)
