@@ -9,7 +9,8 @@ backward after a forward run reverses the chain of snapshots the forward stored
 without advancing to them: F(l, s) = min_m F(l-m, s-1) + C(m, s), F(l, 0) = C(l, 0).
 The library solves the recursion by dynamic programming up to l^2 s = 4e8 and by
 closed-form split rules beyond; both are checked here, the second at sizes no GPU
-test reaches."""
+test reaches.  bx_adj_device_bytes, the engine's memory computed on the host, is
+checked against the device bytes the engine reported in the adjoint bench runs."""
 from math import comb
 
 import numpy as np
