@@ -403,3 +403,20 @@ def test_create_refuses_invalid_parameters(field, value, msg):
     assert L.bx_create(ctypes.byref(p), ctypes.byref(h)) == 1  # BX_ERR_ARG
     assert not h.value
     assert re.search(msg, L.bx_last_error(None).decode())
+
+
+def test_noalloc_sweep_refusals_need_no_device():
+    """bx_ghost_fill_noalloc checks its sizes and pointers before any device
+    call: negative or oversized counts and null pointers are refused with
+    BX_ERR_ARG and a message, an empty sweep is a no-op."""
+    L = _lib.lib()
+    msg = lambda: L.bx_noalloc_last_error().decode()  # noqa: E731
+    vp = ctypes.c_void_p
+    assert L.bx_ghost_fill_noalloc(None, 100, None, None, None, 0, None) == 0
+    assert L.bx_ghost_fill_noalloc(None, 100, None, None, None, -1, None) == 1
+    assert "nghost >= 0" in msg()
+    assert L.bx_ghost_fill_noalloc(None, 0, None, None, None, 5, None) == 1
+    assert L.bx_ghost_fill_noalloc(None, 1 << 30, None, None, None, (1 << 20) + 1, None) == 1
+    assert "1048576" in msg()
+    assert L.bx_ghost_fill_noalloc(vp(16), 100, None, vp(16), vp(16), 5, None) == 1
+    assert "null device pointer" in msg()
