@@ -420,3 +420,24 @@ def test_noalloc_sweep_refusals_need_no_device():
     assert "1048576" in msg()
     assert L.bx_ghost_fill_noalloc(vp(16), 100, None, vp(16), vp(16), 5, None) == 1
     assert "null device pointer" in msg()
+
+
+@pytest.mark.parametrize("change,msg", [
+    (dict(fluxangmom=True), "unsupported"),
+    (dict(h2stat=0), "unsupported"),
+    (dict(no_outflow_xl=True, no_outflow_xr=True, no_outflow_yl=True, no_outflow_yr=True,
+          no_outflow_zl=True, no_outflow_zr=True), "")])
+def test_batch_refuses_boxes_off_the_fused_path(change, msg):
+    """A box the fused stages do not run (angular-momentum fluxing, tabulated EOS,
+    a ghost fill that two sweeps do not resolve) is refused as unsupported while
+    the parameters are checked, before any device work."""
+    import dataclasses
+    from boxzyhydro_b200.batch import Batch
+    base = HydroParams(nx=20, ny=20, nz=20, dx=0.05, dy=0.05, dz=0.05, h2stat=-1,
+                       gammafix=1.4, no_outflow_xl=False, no_outflow_xr=False,
+                       no_outflow_yl=False, no_outflow_yr=False, no_outflow_zl=False,
+                       no_outflow_zr=False)
+    hp = dataclasses.replace(base, **change)
+    with pytest.raises(_lib.BoxzyError, match="UNSUPPORTED") as e:
+        Batch([hp])
+    assert msg in str(e.value)
