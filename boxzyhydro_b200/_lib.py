@@ -87,6 +87,8 @@ def lib():
         "bx_ghost": (C.c_int, [H]),
         "bx_flux": (C.c_int, [H, C.c_int32]),
         "bx_avisc": (C.c_int, [H]),
+        "bx_set_avmag": (C.c_int, [H, C.c_double, C.c_double, C.c_double]),
+        "bx_download_qq": (C.c_int, [H, C.c_void_p]),
         "bx_save_cons_old": (C.c_int, [H]),
         "bx_set_dt": (C.c_int, [H, C.c_double]),
         "bx_set_gforce": (C.c_int, [H, vp]),

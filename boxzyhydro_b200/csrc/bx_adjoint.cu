@@ -747,7 +747,8 @@ struct bx_adj {
   std::string err;
 };
 
-static std::string g_adj_err;
+// the message of the calling thread's last failed call made without a handle
+static thread_local std::string g_adj_err;
 
 // two timing events, destroyed when the scope ends (on the error returns too)
 struct EventPair {
@@ -820,14 +821,8 @@ static cudaError_t launch_rdir(const Geom& g, const double* P, const double* lam
   // x lines run along contiguous memory: long segments; y/z lines: 8 lines of
   // adjacent x per block (coalesced), short segments
   const RShape sh = DIR == 0 ? rshape(hi - lo + 2, 60, 128) : rshape(hi - lo + 2, 28, 256);
-  static size_t attr = 0;  // per instantiation; the attribute is per function
-  if (sh.smem > attr) {
-    cudaError_t e = cudaFuncSetAttribute(k_rdir<DIR, POW2>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sh.smem);
-    if (e != cudaSuccess) return e;
-    attr = sh.smem;
-  }
+  cudaError_t e = ensure_dyn_smem((const void*)k_rdir<DIR, POW2>, sh.smem);
+  if (e != cudaSuccess) return e;
   dim3 grid((unsigned)((nlines + sh.NL - 1) / sh.NL), (unsigned)sh.nseg);
   k_rdir<DIR, POW2><<<grid, sh.threads, sh.smem, s>>>(g, P, lamL, lscale, dt, PA, sh);
   return cudaGetLastError();
@@ -1330,6 +1325,18 @@ int bx_adj_device_bytes(const bx_params* params, int64_t nsteps, int32_t snapsho
   if (!params || !bytes || nsteps <= 0 || snapshots < 1 || stage0_cache_entries < 2 ||
       params->nx < 5 || params->ny < 5 || params->nz < 1)
     return aerr(nullptr, BX_ERR_ARG, "bad arguments");
+  if ((long long)params->nx * params->ny * params->nz >= (1ll << 31))
+    return aerr(nullptr, BX_ERR_ARG, "grid exceeds 2^31 cells");
+  // the grids bx_adj_create takes: those the fused stage kernels run
+  {
+    GhostTable T;
+    build_ghost_tables(*params, T);
+    if (!(T.resolved2 && T.face_rule_ok && !(params->flags & BX_FLAG_PHASE_ONLY) &&
+          !params->fluxangmom && params->h2stat == -1))
+      return aerr(nullptr, BX_ERR_UNSUPPORTED,
+                  "the adjoint follows the fused stage kernels, which this grid does not run "
+                  "(ghost fill not resolved within two sweeps, fluxangmom or a tabulated EOS)");
+  }
   const __int128 n = (__int128)params->nx * params->ny * params->nz;
   const __int128 snaps = std::min<long long>(snapshots, nsteps);
   // what bx_adj_create, bx_adj_stage0_cache and bx_adj_keep_stage0 allocate:

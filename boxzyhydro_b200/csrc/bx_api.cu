@@ -29,7 +29,8 @@ int stage_blocks_per_sm(int stage, int pm, bool threed);
 
 #include "bx_handle.h"
 
-static std::string g_create_err;
+// the message of the calling thread's last failed call made without a handle
+static thread_local std::string g_create_err;
 
 #define CK(expr)                                                                  \
   do {                                                                            \
@@ -468,8 +469,42 @@ int bx_flux(bx_handle* h, int32_t avg) {
   CK(phase_ghost(h->nghost, h->d_dst, h->d_src1, h->d_sgn1, h->pa, h->g.ng, h->stream));
   return pull_clock(h);
 }
+int bx_set_avmag(bx_handle* h, double avmagx, double avmagy, double avmagz) {
+  CHECK_H();
+  h->avmag[0] = avmagx;
+  h->avmag[1] = avmagy;
+  h->avmag[2] = avmagz;
+  return BX_OK;
+}
 int bx_avisc(bx_handle* h) {
   CHECK_H();
+  if (int r = to_phase(h)) return r;
+  if (!h->d_qq) {
+    if (cudaMalloc(&h->d_qq, 3 * h->g.ng * sizeof(double)) != cudaSuccess) {
+      cudaGetLastError();
+      h->d_qq = nullptr;
+      return set_err(h, BX_ERR_NOMEM, "cudaMalloc of the qq array failed");
+    }
+  }
+  CK(phase_avisc(h->g, h->pa.u, h->avmag, h->d_qq, h->stream));
+  h->launches += 1;
+  CK(cudaStreamSynchronize(h->stream));
+  return BX_OK;
+}
+int bx_download_qq(bx_handle* h, double* qq) {
+  CHECK_H();
+  if (!qq) return set_err(h, BX_ERR_ARG, "qq is NULL");
+  const long long n = h->g.ng;
+  if (!h->d_qq) {
+    // the reference's qq before any avisc call: zero (init_grid.f90:298)
+    std::memset(qq, 0, 3 * n * sizeof(double));
+    return BX_OK;
+  }
+  double* tmp = staging(h);
+  CK(soa_to_aos(h->d_qq, tmp, n, 3, h->stream));
+  h->launches += 1;
+  CK(cudaMemcpyAsync(qq, tmp, 3 * n * sizeof(double), cudaMemcpyDeviceToHost, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
   return BX_OK;
 }
 int bx_save_cons_old(bx_handle* h) {

@@ -76,7 +76,8 @@ struct bx_batch {
   std::string err;
 };
 
-static std::string g_batch_err;
+// the message of the calling thread's last failed call made without a handle
+static thread_local std::string g_batch_err;
 
 #define BCK(expr)                                                     \
   do {                                                                \

@@ -44,6 +44,10 @@ struct bx_handle {
   long long n_stage = 0;
   long long launches = 0;  // kernels of this library launched on the handle's stream
   double* d_eos = nullptr;  // device copy of the tabulated EOS (H2STAT >= 0)
+  // avisc: the hydro namelist's avmagx, avmagy, avmagz and the qq array (3
+  // planes, made by the first bx_avisc)
+  double avmag[3] = {0.0, 0.0, 0.0};
+  double* d_qq = nullptr;
   // bx_step_host: its tiles (thin z-chunks), the z slabs of the cell range
   // (groups of those chunks) with their ghost ranges, and the streams and
   // events that overlap the copies with the step (made on first use)

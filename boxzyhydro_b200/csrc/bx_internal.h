@@ -30,7 +30,7 @@ struct Ctrl {
   double dt;          // full step dt (main.f90:342)
   double dtold;       // main.f90:270-271
   double endtime;
-  double rate;        // last reduced dtrate (courant.f90:175)
+  double rate;        // last reduced dtrate (courant.f90:22)
   unsigned long long rate_bits;  // atomicMax accumulator (bit image of a double >= 0)
   long long step;
   long long max_step;
@@ -128,6 +128,12 @@ struct StageArgs {
   int nsrc;                // > 0: sources the input is short of; 0: per box (Ctrl::nsrc)
 };
 
+// Raises the dynamic shared-memory limit of kernel `fn` on the current device
+// to at least `bytes`.  The attribute is held per device, so it is set once per
+// (kernel, device) pair, under a lock: handles on several devices and several
+// host threads may launch the same kernel.
+cudaError_t ensure_dyn_smem(const void* fn, size_t bytes);
+
 // pm: 1 = every box has power-of-two spacings, 0 = otherwise
 cudaError_t launch_stage(int stage, int pm, bool threed, const StageArgs& a, int ntiles,
                          cudaStream_t s);
@@ -166,6 +172,9 @@ cudaError_t phase_ghost(int nghost, const int32_t* dst, const int32_t* src, cons
                         PhaseArrays& a, long long ng, cudaStream_t s);
 cudaError_t phase_flux(const Geom& g, PhaseArrays& a, Ctrl* ctrl, int avg, cudaStream_t s);
 cudaError_t phase_courant_finish(Ctrl* ctrl, cudaStream_t s);
+// avisc.f90:13-23 into qq (3 planes of ng) from the velocity array u
+cudaError_t phase_avisc(const Geom& g, const double* u, const double avmag[3], double* qq,
+                        cudaStream_t s);
 cudaError_t phase_copy_old(const Geom& g, PhaseArrays& a, cudaStream_t s);
 
 // fused <-> phase representation changes

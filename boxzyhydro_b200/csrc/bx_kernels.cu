@@ -21,10 +21,28 @@
 //    steps where the velocity limiter or the low-density EOS branch fires.
 #include <cuda_runtime.h>
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "bx_internal.h"
 #include "bx_math.cuh"
 
 namespace bx {
+
+cudaError_t ensure_dyn_smem(const void* fn, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> set;
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& have = set[{fn, dev}];
+  if (have >= bytes) return cudaSuccess;
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+  if (e == cudaSuccess) have = bytes;
+  return e;
+}
 
 namespace {
 
@@ -501,7 +519,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
           rate = fmax(rate, r0);
           if (!(r0 >= 0.0)) flags |= kFlagNonFinite;
         } else {
-          // source(1) energy, then the Courant rate of the next step (courant.f90:173-175)
+          // source(1) energy, then the Courant rate of the next step (courant.f90:20-22)
           const double E3 = source_energy(n[0], n[1], n[2], n[3], n[4], g.small_eps);
           const double pA = eos_pressure(n[0], E3, u1, u2, u3, g.gm1, g.small_eps);
           const double r0 = courant_rate<POW2>(n[0], pA, g.gam, u1, u2, u3, g.dx, g.dy, g.dz,
@@ -574,13 +592,8 @@ __global__ void __launch_bounds__(NT, 65536 / (NT * 128)) k_stage(StageArgs a) {
 template <int STAGE, int PM, bool THREED, bool GRAV>
 static cudaError_t launch_stage_t(const StageArgs& a, int ntiles, cudaStream_t s) {
   const size_t smem = SMEM_DOUBLES * sizeof(double);
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaError_t e = cudaFuncSetAttribute(k_stage<STAGE, PM, THREED, GRAV>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    attr_set = true;
-  }
+  cudaError_t e = ensure_dyn_smem((const void*)k_stage<STAGE, PM, THREED, GRAV>, smem);
+  if (e != cudaSuccess) return e;
   if (ntiles <= 0) return cudaSuccess;
   k_stage<STAGE, PM, THREED, GRAV><<<ntiles, NT, smem, s>>>(a);
   return cudaGetLastError();
@@ -626,7 +639,7 @@ __global__ void k_dt(Ctrl* ctrl, int n) {
   const double rate = __longlong_as_double((long long)c.rate_bits);
   c.rate = rate;
   c.rate_bits = 0ull;
-  double dt = c.cfl / rate;            // courant.f90:182
+  double dt = c.cfl / rate;            // courant.f90:28
   dt = dt * 1.0;                       // dt*f1, f1=one
   if (c.step > 1 && c.dtold > 0.0) dt = fmin(dt, c.dtold * 1.1);
   c.dtold = dt;
@@ -815,7 +828,7 @@ __global__ void k_phase_state(Geom g, PhaseArrays a, Ctrl* ctrl) {
   }
 }
 
-// velocity.f90:107-141
+// velocity.f90:18-53
 __global__ void k_phase_velocity(Geom g, PhaseArrays a, Ctrl* ctrl) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= g.ng) return;
@@ -844,7 +857,7 @@ __global__ void k_phase_velocity(Geom g, PhaseArrays a, Ctrl* ctrl) {
   for (int k = 0; k < 3; ++k) a.u[k * n + i] = u[k];
 }
 
-// courant.f90:172-176 (max over every cell, ghosts included)
+// courant.f90:19-23 (max over every cell, ghosts included)
 __global__ void k_phase_courant(Geom g, PhaseArrays a, Ctrl* ctrl) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   const long long n = g.ng;
@@ -867,6 +880,71 @@ __global__ void k_phase_courant(Geom g, PhaseArrays a, Ctrl* ctrl) {
     atomicMax(&ctrl->rate_bits, (unsigned long long)__double_as_longlong(m));
   }
   if (bad) atomicOr(&ctrl->flags, (unsigned)kFlagNonFinite);
+}
+
+// avisc (avisc.f90:13-23): qq(d) = avmag_d*min(0, u_d(b+) - u_d(b-))**2 on the
+// cells with boundary > 0 (the ghost layers -- the reference's test, kept as
+// written), zero elsewhere.  b are the cell's neighbours through get_boundary
+// (utils.f90:62-73): a neighbour in a ghost layer becomes the cell itself.  The
+// neighbour table is init_grid.f90:178-261: the outer layer (boundary 1) stores
+// only its donor, two cells inward, in ineigh(1) (the +y slot) and leaves the
+// other five at 0, an index outside grid(1:ngrid) that the reference reads
+// anyway; here such an entry resolves to the cell itself, like a ghost
+// neighbour.  The inner layer (boundary 2) has the six neighbours, with the z
+// pair set to the cell itself when nz < 6.
+__global__ void k_phase_avisc(Geom g, const double* u, double ax, double ay, double az,
+                              double* qq) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const long long n = g.ng;
+  if (i >= n) return;
+  const int x = (int)(i % g.nx), y = (int)((i / g.nx) % g.ny), z = (int)(i / g.sz);
+  // boundary flag of a cell (init_grid.f90:82-105), 0-based coordinates
+  auto flag = [&](int cx, int cy, int cz) -> int {
+    const bool zl = g.nz >= 6;
+    if (cx == 0 || cx == g.nx - 1 || cy == 0 || cy == g.ny - 1 ||
+        (zl && (cz == 0 || cz == g.nz - 1)))
+      return 1;
+    if (cx == 1 || cx == g.nx - 2 || cy == 1 || cy == g.ny - 2 ||
+        (zl && (cz == 1 || cz == g.nz - 2)))
+      return 2;
+    return 0;
+  };
+  const int b = flag(x, y, z);
+  double q1 = 0.0, q2 = 0.0, q3 = 0.0;
+  if (b > 0) {
+    // neighbours (+y, -y, +x, -x, +z, -z) as cell offsets, -1 = the cell itself
+    long long nb[6];
+    int cx[6], cy[6], cz[6];
+    for (int k = 0; k < 6; ++k) { nb[k] = -1; cx[k] = x; cy[k] = y; cz[k] = z; }
+    if (b == 1) {
+      // init_grid.f90:180-203: the donor, two cells inward, in ineigh(1)
+      if (x == 0) cx[0] = x + 2;
+      else if (x == g.nx - 1) cx[0] = x - 2;
+      else if (y == 0) cy[0] = y + 2;
+      else if (y == g.ny - 1) cy[0] = y - 2;
+      else if (z == 0) cz[0] = g.nz < 6 ? z : z + 2;
+      else cz[0] = g.nz < 6 ? z : z - 2;
+      nb[0] = 0;
+    } else {
+      cy[0] = y + 1; cy[1] = y - 1; cx[2] = x + 1; cx[3] = x - 1;
+      if (g.nz >= 6) { cz[4] = z + 1; cz[5] = z - 1; }
+      for (int k = 0; k < 6; ++k) nb[k] = 0;
+    }
+    long long bi[6];
+    for (int k = 0; k < 6; ++k) {
+      const long long j = cx[k] + cy[k] * g.sy + cz[k] * g.sz;
+      bi[k] = (nb[k] < 0 || flag(cx[k], cy[k], cz[k]) > 0) ? i : j;
+    }
+    const double m1 = fmin(0.0, u[bi[2]] - u[bi[3]]);
+    const double m2 = fmin(0.0, u[n + bi[0]] - u[n + bi[1]]);
+    const double m3 = fmin(0.0, u[2 * n + bi[4]] - u[2 * n + bi[5]]);
+    q1 = ax * (m1 * m1);
+    q2 = ay * (m2 * m2);
+    q3 = az * (m3 * m3);
+  }
+  qq[i] = q1;
+  qq[n + i] = q2;
+  qq[2 * n + i] = q3;
 }
 
 __global__ void k_phase_courant_finish(Ctrl* ctrl) {
@@ -1304,6 +1382,11 @@ cudaError_t phase_courant(const Geom& g, PhaseArrays& a, Ctrl* ctrl, cudaStream_
   k_phase_courant<<<nblk(g.ng), PB, 0, s>>>(g, a, ctrl);
   return cudaGetLastError();
 }
+cudaError_t phase_avisc(const Geom& g, const double* u, const double avmag[3], double* qq,
+                        cudaStream_t s) {
+  k_phase_avisc<<<nblk(g.ng), PB, 0, s>>>(g, u, avmag[0], avmag[1], avmag[2], qq);
+  return cudaGetLastError();
+}
 cudaError_t phase_courant_finish(Ctrl* ctrl, cudaStream_t s) {
   k_phase_courant_finish<<<1, 1, 0, s>>>(ctrl);
   return cudaGetLastError();
@@ -1437,7 +1520,7 @@ __global__ void k_box_check_ghosts(int nghost, const int32_t* dst, const int32_t
   ok = ok && X[3 * ps + d] == ((m & 4) ? -X[3 * ps + s] : X[3 * ps + s]);
   if (!ok) atomicOr(&ctrl->flags, (unsigned)kFlagNotClean);
 }
-// Courant rate (courant.f90:172-176) of a box whose planes hold the reference
+// Courant rate (courant.f90:19-23) of a box whose planes hold the reference
 // cons with u == m/rho: the max over interior cells (ghosts repeat them)
 __global__ void k_box_rate(Geom g, const double* X, long long ps, Ctrl* ctrl) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -1534,8 +1617,8 @@ int stage_blocks_per_sm(int stage, int pm, bool threed) {
   else
     fn = pm == 1 ? (threed ? (const void*)k_stage<1, 1, true> : (const void*)k_stage<1, 1, false>)
                  : (threed ? (const void*)k_stage<1, 0, true> : (const void*)k_stage<1, 0, false>);
-  cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, NT, smem) != cudaSuccess) {
+  if (ensure_dyn_smem(fn, smem) != cudaSuccess ||
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, NT, smem) != cudaSuccess) {
     cudaGetLastError();
     return 1;
   }

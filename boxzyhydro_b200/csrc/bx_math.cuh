@@ -48,7 +48,7 @@ BX_HD double kin_rho_u(double d, double u1, double u2, double u3) {
   return d * kHalf * (u1 * u1 + u2 * u2 + u3 * u3);
 }
 
-// half*(m1^2+m2^2+m3^2)/rho (velocity.f90:126, source.f90:176, flux.f90:227)
+// half*(m1^2+m2^2+m3^2)/rho (velocity.f90:37, source.f90:176, flux.f90:227)
 BX_HD double kin_mom(double d, double m1, double m2, double m3) {
   return kHalf * (m1 * m1 + m2 * m2 + m3 * m3) / d;
 }
@@ -103,7 +103,7 @@ BX_HD double cdiv(double x, double d, double r) {
   return x / d;
 }
 
-// Courant rate of one cell (courant.f90:173-174); idx etc. are 1/dx etc.: when
+// Courant rate of one cell (courant.f90:20-21); idx etc. are 1/dx etc.: when
 // the spacing is a power of two x/2^k and x*2^-k round identically, otherwise
 // cdiv gives the IEEE quotient.
 template <bool POW2>

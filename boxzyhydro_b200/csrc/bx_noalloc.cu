@@ -16,15 +16,20 @@
 // array's name as a device address (it names a host-side stand-in), so the
 // first call on each device, with that device current, looks the device
 // address up with cudaGetSymbolAddress and caches it; that first call should be
-// made before any stream capture begins.  All calls share the one array and it
+// made before any stream capture begins.  The cached address belongs to the
+// CUDA context that was current when it was looked up: a call that finds
+// another context current on the device (after cudaDeviceReset, or with a
+// context of the caller's own made current) looks the address up again, since
+// the library's module, and with it the array, lives at a new address in that
+// context.  All calls share the one array and it
 // keeps whatever the last call left there; nothing in it needs to start at
 // zero, because every slot the scatter reads was written by the gather of the
 // same call.  Calls that overlap on the GPU (on different streams, or from
 // different host threads) race on the array.
 #include <cuda_runtime.h>
 
-#include <atomic>
 #include <cstdio>
+#include <mutex>
 
 #include "../../include/boxzy_gpu.h"
 
@@ -35,8 +40,32 @@ constexpr int kMaxDevices = 64;
 
 __device__ __align__(256) double g_ghost_scratch[5 * kMaxGhosts];
 
-std::atomic<double*> g_scratch_addr[kMaxDevices];
-char g_noalloc_err[256];
+// per device: the context the scratch address was looked up in, and the address
+struct ScratchSlot {
+  void* ctx = nullptr;
+  double* addr = nullptr;
+};
+std::mutex g_scratch_mu;
+ScratchSlot g_scratch[kMaxDevices];
+// the message of the calling thread's last failed call
+thread_local char g_noalloc_err[256];
+
+// the driver's current context of the calling thread (cuCtxGetCurrent, found
+// through the runtime so the library does not link the driver library itself)
+cudaError_t current_context(void** ctx) {
+  using Fn = int (*)(void**);
+  static Fn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &p, 12000, cudaEnableDefault, &q) !=
+            cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<Fn>(p);
+  }();
+  if (!fn) return cudaErrorNotSupported;
+  return fn(ctx) == 0 ? cudaSuccess : cudaErrorDeviceUninitialized;
+}
 
 __global__ void k_noalloc_gather(long long nghost, const int32_t* __restrict__ src,
                                  const uint8_t* __restrict__ sgn, const double* __restrict__ cons,
@@ -84,15 +113,32 @@ extern "C" int bx_ghost_fill_noalloc(double* cons_soa, int64_t ngrid, const int3
   cudaError_t e = cudaGetDevice(&dev);
   if (e != cudaSuccess) return fail(BX_ERR_CUDA, cudaGetErrorString(e));
   if (dev < 0 || dev >= kMaxDevices) return fail(BX_ERR_ARG, "device ordinal out of range");
-  double* scratch = g_scratch_addr[dev].load(std::memory_order_acquire);
-  if (!scratch) {
-    // set-up, once per device, with that device current: the device address of
-    // the static scratch array
+  void* ctx = nullptr;
+  e = current_context(&ctx);
+  if (e != cudaSuccess) return fail(BX_ERR_CUDA, "cuCtxGetCurrent is not available");
+  if (!ctx) {
+    // no context is current on this thread yet: the runtime's symbol lookup
+    // makes the device's primary context current
     void* p = nullptr;
     e = cudaGetSymbolAddress(&p, g_ghost_scratch);
     if (e != cudaSuccess || !p) return fail(BX_ERR_CUDA, cudaGetErrorString(e));
-    scratch = static_cast<double*>(p);
-    g_scratch_addr[dev].store(scratch, std::memory_order_release);
+    e = current_context(&ctx);
+    if (e != cudaSuccess || !ctx) return fail(BX_ERR_CUDA, "no current CUDA context");
+  }
+  double* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_scratch_mu);
+    ScratchSlot& slot = g_scratch[dev];
+    if (slot.ctx != ctx || !slot.addr) {
+      // set-up, once per device and context, with that device current: the
+      // device address of the static scratch array
+      void* p = nullptr;
+      e = cudaGetSymbolAddress(&p, g_ghost_scratch);
+      if (e != cudaSuccess || !p) return fail(BX_ERR_CUDA, cudaGetErrorString(e));
+      slot.ctx = ctx;
+      slot.addr = static_cast<double*>(p);
+    }
+    scratch = slot.addr;
   }
   cudaStream_t s = static_cast<cudaStream_t>(cuda_stream);
   const int threads = 256;

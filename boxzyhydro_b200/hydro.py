@@ -174,7 +174,18 @@ class Hydro:
         self._c(lib().bx_flux(self._h, int(avg)))
 
     def avisc(self):
+        """avisc.f90:4-26 on the device: the qq array from the velocity array."""
         self._c(lib().bx_avisc(self._h))
+
+    def set_avmag(self, avmagx=0.0, avmagy=0.0, avmagz=0.0):
+        """The hydro namelist's avmagx/y/z (parameters.f90:77) that avisc reads."""
+        self._c(lib().bx_set_avmag(self._h, float(avmagx), float(avmagy), float(avmagz)))
+
+    def qq(self):
+        """The artificial-viscosity array qq(3, ngrid), as (ngrid, 3)."""
+        out = np.empty((self.params.ngrid, 3))
+        self._c(lib().bx_download_qq(self._h, out.ctypes.data))
+        return out
 
     def save_cons_old(self):
         self._c(lib().bx_save_cons_old(self._h))

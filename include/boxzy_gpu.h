@@ -40,7 +40,7 @@ extern "C" {
 #define BX_ERR_NOMEM 5        /* device allocation failed */
 
 /* status bits reported by bx_status */
-#define BX_STATUS_VLIMIT 1u     /* velocity limiter fired (velocity.f90:122-139) */
+#define BX_STATUS_VLIMIT 1u     /* velocity limiter fired (velocity.f90:31-50) */
 #define BX_STATUS_LOWRHO 2u     /* low-density EOS branch taken (state.f90:52-56) */
 #define BX_STATUS_NONFINITE 4u  /* NaN or Inf produced */
 #define BX_STATUS_ZEROWAVE 8u   /* ap+am == 0 at a face (flux.f90:588) */
@@ -54,10 +54,10 @@ typedef struct bx_params {
   int32_t h2stat;         /* eos_input H2STAT: -1 fixed gamma (state.f90:49-59); >= 0
                              tabulated EOS (state.f90:60-79, bx_set_eos_table) */
   double dx, dy, dz;      /* grid_params dx,dy,dz */
-  double cfl;             /* hydro cfl (courant.f90:182) */
+  double cfl;             /* hydro cfl (courant.f90:28) */
   double small_rho;       /* hydro small_rho (flux.f90:225) */
   double small_eps;       /* hydro small_eps */
-  double vlimit;          /* hydro vlimit (velocity.f90:122) */
+  double vlimit;          /* hydro vlimit (velocity.f90:32) */
   double gammafix;        /* eos_input gammafix */
   double muc;             /* mean molecular weight, eos.f90:144 */
   double rgas;            /* scale%rgas of get_units, units.f90:17 */
@@ -171,14 +171,26 @@ int bx_set_eos_table(bx_handle *h, const bx_eos_table *t);
 /* Per-phase entry points on the handle's module arrays, for bisection against the
  * reference.  They act exactly like the subroutines they replace. */
 int bx_state(bx_handle *h);                /* state.f90:6-89 (H2STAT=-1 branch) */
-int bx_velocity(bx_handle *h);             /* velocity.f90:93-153 */
-int bx_courant(bx_handle *h, double *dt);  /* courant.f90:157-192; sets and returns dt */
+int bx_velocity(bx_handle *h);             /* velocity.f90:4-64 */
+int bx_courant(bx_handle *h, double *dt);  /* courant.f90:4-39; sets and returns dt */
 int bx_source(bx_handle *h, int32_t siter);/* source.f90:5-205 (gravity coupling via gforce) */
 int bx_ghost(bx_handle *h);                /* utils.f90:305-480 set_ghost_cells */
 int bx_flux(bx_handle *h, int32_t avg);    /* flux.f90:6-235 */
-int bx_avisc(bx_handle *h);                /* avisc.f90:197-219: never called by the reference
-                                              and its result qq is never read; a no-op */
+int bx_avisc(bx_handle *h);                /* avisc.f90:4-26 into the handle's qq array;
+                                              the reference never calls it or reads qq */
 int bx_save_cons_old(bx_handle *h);        /* main.f90:327-333 */
+/* The hydro namelist's avmagx, avmagy, avmagz (input.f90:12, parameters.f90:77; all 0 by
+ * default) for bx_avisc. */
+int bx_set_avmag(bx_handle *h, double avmagx, double avmagy, double avmagz);
+/* The artificial-viscosity array qq(3,ngrid) (grid_commons.f90:14), host layout: what the
+ * last bx_avisc computed, zero before the first (init_grid.f90:298).  qq is computed
+ * as avisc.f90:13-23 writes it: qq(d) = avmag_d*min(0, u_d(+) - u_d(-))**2 on the cells
+ * with boundary > 0, the ghost layers (the reference's test, kept as written), and 0
+ * on the interior cells; neighbours in a ghost layer resolve to the cell itself
+ * (get_boundary, utils.f90:62-73), and so do the five neighbour slots that
+ * init_grid.f90:178 leaves at 0 for the outer ghost layer (the reference reads
+ * grid(0) there, outside the array). */
+int bx_download_qq(bx_handle *h, double *qq);
 int bx_set_dt(bx_handle *h, double dt);    /* the module variable dt (grid_commons.f90:12) */
 
 /* Gravitational acceleration gforce(3,ngrid) consumed by source() (source.f90:161-182);
@@ -291,7 +303,10 @@ int bx_adj_plan(int64_t nsteps, int32_t snapshots, int64_t *recomputed_first,
  * device_bytes) with `snapshots` plane sets, `stage0_cache_entries` cache
  * entries (>= 2; bx_adj_stage0_cache) and the stage-0 results of every step kept
  * or not (bx_adj_keep_stage0), to size a run to the device before allocating.
- * The handle beneath the engine adds its ghost tables and tile list. */
+ * The handle beneath the engine adds its ghost tables and tile list.  Grids that
+ * bx_adj_create refuses are refused here too: BX_ERR_ARG beyond 2^31 cells,
+ * BX_ERR_UNSUPPORTED for grids off the fused stage kernels (checked on the host
+ * by building the grid's ghost plan). */
 int bx_adj_device_bytes(const bx_params *params, int64_t nsteps, int32_t snapshots,
                         int32_t stage0_cache_entries, int32_t keep_stage0, int64_t *bytes);
 int bx_adj_dts(bx_adj *a, double *dts);
@@ -306,15 +321,19 @@ const char *bx_adj_last_error(bx_adj *a);
  * static device array of BX_NOALLOC_MAX_GHOSTS x 5 doubles (40 MiB) that every GPU
  * loading the library holds until exit; larger nghost is rejected with BX_ERR_ARG.
  * The first call on a device looks up that array's device address (make it before
- * any stream capture); calls that overlap on the GPU race on the shared array.
- * Errors are reported by bx_noalloc_last_error. */
+ * any stream capture), and so does the first call after another CUDA context became
+ * current on the device (cudaDeviceReset, or a context of the caller's own); calls
+ * that overlap on the GPU race on the shared array.  Errors are reported by
+ * bx_noalloc_last_error, per host thread. */
 #define BX_NOALLOC_MAX_GHOSTS 1048576
 int bx_ghost_fill_noalloc(double *cons_soa, int64_t ngrid, const int32_t *dst,
                           const int32_t *src, const uint8_t *sgn, int64_t nghost,
                           void *cuda_stream);
 const char *bx_noalloc_last_error(void);
 
-/* Message of the last error on the handle (or of the last failed bx_create when h is NULL). */
+/* Message of the last error on the handle (or, when h is NULL, of the calling thread's
+ * last failed bx_create; bx_batch_last_error(NULL) and bx_adj_last_error(NULL) likewise
+ * report the calling thread's last failed bx_batch_create / bx_adj_create). */
 const char *bx_last_error(bx_handle *h);
 
 #ifdef __cplusplus

@@ -986,6 +986,39 @@ void ox_save_cons_old(ox_sim *s) {
   memcpy(s->cons_old, s->cons, s->ng * 5 * sizeof(double));
 }
 
+/* get_boundary (utils.f90:62-73): neighbour idx of igrid, or igrid itself when
+ * the neighbour lies in a ghost layer.  An unset slot (init_grid.f90:178 leaves
+ * five of them at 0 for the outer ghost layer, an index outside grid(1:ngrid)
+ * that the reference reads anyway) resolves to igrid as well. */
+static int64_t get_boundary_1(const ox_sim *s, int64_t igrid, int idx) {
+  const int64_t b = s->ineigh[igrid * 6 + idx];
+  if (b < 0 || s->bnd[b] > 0) return igrid;
+  return b;
+}
+
+/* avisc.f90:4-26, the condition as written (boundary > 0) */
+void ox_avisc(const ox_sim *s, double avmagx, double avmagy, double avmagz, double *qq) {
+  const int64_t ng = s->ng;
+#pragma omp parallel for schedule(static)
+  for (int64_t igrid = 0; igrid < ng; ++igrid) {
+    double *q = qq + igrid * 3;
+    if (s->bnd[igrid] > 0) {
+      int64_t b[6];
+      for (int k = 0; k < 6; ++k) b[k] = get_boundary_1(s, igrid, k);
+      const double m1 = fmin_f(ZERO, s->u[b[2] * 3 + 0] - s->u[b[3] * 3 + 0]);
+      const double m2 = fmin_f(ZERO, s->u[b[0] * 3 + 1] - s->u[b[1] * 3 + 1]);
+      const double m3 = fmin_f(ZERO, s->u[b[4] * 3 + 2] - s->u[b[5] * 3 + 2]);
+      q[0] = avmagx * (m1 * m1);
+      q[1] = avmagy * (m2 * m2);
+      q[2] = avmagz * (m3 * m3);
+    } else {
+      q[0] = ZERO;
+      q[1] = ZERO;
+      q[2] = ZERO;
+    }
+  }
+}
+
 /* main.f90:212-545, default flags (no gravity solver, radiation or particles) */
 int ox_step(ox_sim *s, double endtime) {
   if (s->time >= endtime || s->step >= 1000000) return 1;

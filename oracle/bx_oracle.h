@@ -84,6 +84,8 @@ void ox_set_ghost_cells(ox_sim *s);
 void ox_flux(ox_sim *s, int avg);
 void ox_flux_ang(ox_sim *s, int avg); /* flux_ang.f90:6-281 */
 void ox_save_cons_old(ox_sim *s);
+/* avisc.f90:4-26: qq(3,ngrid) (host layout) from the velocity array u */
+void ox_avisc(const ox_sim *s, double avmagx, double avmagy, double avmagz, double *qq);
 
 /* one iteration of the main loop (main.f90:212-545); returns 0 if it ran,
  * 1 if the loop would have exited (time>=endtime). */

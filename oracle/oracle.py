@@ -66,6 +66,7 @@ def lib():
                    "ox_save_cons_old"):
             getattr(L, fn).argtypes = [P]
         L.ox_source.argtypes = [P, C.c_int]
+        L.ox_avisc.argtypes = [P, C.c_double, C.c_double, C.c_double, C.c_void_p]
         L.ox_flux.argtypes = [P, C.c_int]
         L.ox_flux_ang.argtypes = [P, C.c_int]
         L.ox_step.argtypes = [P, C.c_double]
@@ -251,6 +252,12 @@ class Oracle:
 
     def save_cons_old(self):
         lib().ox_save_cons_old(self._h)
+
+    def avisc(self, avmagx=0.0, avmagy=0.0, avmagz=0.0):
+        """qq(3, ngrid) of avisc.f90:4-26 from the current velocity array, (ngrid, 3)."""
+        qq = np.empty((self.ng, 3))
+        lib().ox_avisc(self._h, float(avmagx), float(avmagy), float(avmagz), qq.ctypes.data)
+        return qq
 
     def step(self, endtime=1e300):
         return lib().ox_step(self._h, float(endtime)) == 0

@@ -128,3 +128,20 @@ def test_device_bytes_grow_by_one_plane_set_per_snapshot():
     assert device_bytes(hp, 50, 80) == device_bytes(hp, 50, 50)  # at most one per step
     with pytest.raises(BoxzyError):
         device_bytes(hp, 50, 8, stage0_cache=1)
+
+
+def test_device_bytes_refuses_the_grids_the_engine_refuses():
+    import dataclasses
+    hp = ic.turbulent_params(16)
+    with pytest.raises(BoxzyError) as e:
+        device_bytes(dataclasses.replace(hp, fluxangmom=True), 20, 4)
+    assert e.value.code == 3  # BX_ERR_UNSUPPORTED: flux_ang runs on the per-phase kernels
+    # a reflective 3-D box: its corner ghosts lag one sweep, so it runs the per-phase kernels
+    walls = {f"no_outflow_{w}": True for w in ("xl", "xr", "yl", "yr", "zl", "zr")}
+    with pytest.raises(BoxzyError) as e:
+        device_bytes(dataclasses.replace(hp, **walls), 20, 4)
+    assert e.value.code == 3
+    with pytest.raises(BoxzyError) as e:  # int32 cell indices, as bx_create
+        device_bytes(dataclasses.replace(hp, nx=1300, ny=1300, nz=1300), 20, 4)
+    assert e.value.code == 1
+    assert device_bytes(hp, 20, 4) > 0

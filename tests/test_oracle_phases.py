@@ -124,3 +124,50 @@ def test_source_with_a_force_on_the_interior(box):
     work = dt * c[:, 0] * ((u[:, 0] * g[:, 0] + u[:, 1] * g[:, 1]) + u[:, 2] * g[:, 2])
     c[:, 4] = np.maximum(c[:, 4] - ekin + work, hp.small_eps) + ekin
     assert np.array_equal(c1[inner], c)
+
+
+def avisc_numpy(hp, u, avmag):
+    """avisc.f90:13-23 from the grid coordinates: the neighbour table of
+    init_grid.f90:178-261 (outer ghost layer: its donor two cells inward in
+    slot 1, the other slots unset; inner ghost layer: +y, -y, +x, -x, +z, -z, the
+    z pair the cell itself when nz < 6), each neighbour in a ghost layer -- or
+    unset -- replaced by the cell (get_boundary, utils.f90:62-73)."""
+    nx, ny, nz = hp.nx, hp.ny, hp.nz
+    flag = G.boundary_flags(nx, ny, nz)
+    qq = np.zeros((hp.ngrid, 3))
+    for i in np.nonzero(flag > 0)[0]:
+        x, y, z = i % nx, (i // nx) % ny, i // (nx * ny)
+        nb = [None] * 6
+        if flag[i] == 1:
+            if x == 0: nb[0] = i + 2
+            elif x == nx - 1: nb[0] = i - 2
+            elif y == 0: nb[0] = i + 2 * nx
+            elif y == ny - 1: nb[0] = i - 2 * nx
+            elif z == 0: nb[0] = i if nz < 6 else i + 2 * nx * ny
+            else: nb[0] = i if nz < 6 else i - 2 * nx * ny
+        else:
+            zs = 0 if nz < 6 else nx * ny
+            nb = [i + nx, i - nx, i + 1, i - 1, i + zs, i - zs]
+        b = [i if (j is None or flag[j] > 0) else j for j in nb]
+        m1 = min(0.0, u[b[2], 0] - u[b[3], 0])
+        m2 = min(0.0, u[b[0], 1] - u[b[1], 1])
+        m3 = min(0.0, u[b[4], 2] - u[b[5], 2])
+        qq[i] = (avmag[0] * (m1 * m1), avmag[1] * (m2 * m2), avmag[2] * (m3 * m3))
+    return qq
+
+
+@pytest.mark.parametrize("shape", [(11, 10, 9), (12, 9, 4), (8, 8, 6)])
+def test_avisc_matches_the_formula_on_the_ghost_layers(shape):
+    """qq on the boundary > 0 cells (the reference's condition as written),
+    zero on the interior, bit for bit; zero everywhere at the default avmag = 0."""
+    nx, ny, nz = shape
+    st = small_random_box(nx=nx, ny=ny, nz=nz, walls=(0,) * 6, seed=nx * ny + nz, amp=0.4)
+    o = fresh(st)
+    avmag = (0.7, 1.3, 2.1)
+    qq = o.avisc(*avmag)
+    ref = avisc_numpy(st.params, st.u, avmag)
+    assert np.array_equal(qq, ref)
+    flag = G.boundary_flags(nx, ny, nz)
+    assert not qq[flag == 0].any()
+    assert qq[flag > 0].any()  # compressions in a random field
+    assert not o.avisc().any()

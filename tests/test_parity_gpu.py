@@ -39,7 +39,7 @@ def test_phases_one_by_one():
     o.state(); g.state()
     o.velocity(); g.velocity(); compare(o, g, "after flux(0)")
     o.flux(1); g.flux(1); compare(o, g, "flux(1)")
-    g.avisc()  # never called by the reference; must not change anything
+    g.avisc()  # never called by the reference; it writes qq only
     compare(o, g, "avisc")
 
 
@@ -91,7 +91,7 @@ def test_phase_only_flag():
 
 
 def test_velocity_limiter_fallback():
-    """|u| > vlimit in some cells: the limiter rewrites cons (velocity.f90:125-139)."""
+    """|u| > vlimit in some cells: the limiter rewrites cons (velocity.f90:36-50)."""
     st = small_random_box(nx=16, ny=13, nz=9, walls=(0,) * 6, seed=8, amp=0.6, vlimit=0.55)
     o, g = make_pair(st)
     step_both(o, g, 6)
@@ -178,6 +178,25 @@ def test_sod_512_tube_matches_oracle_first_steps():
     step_both(o, g, 25, check_every=5)
 
 
+def test_sod_512_tube_matches_oracle_at_end_of_run():
+    """The C1 configuration (512x4x4 interior Sod tube, gamma 1.4, reflective walls)
+    run to t = 0.2 by both sides (about 4830 steps; the GPU through bx_run's
+    graph-replayed chunks): the same number of steps, the same clock and
+    identical end states, far inside the 1e-10 end-of-run bound."""
+    st = ic.sod_x(n_active=512, ny=8, nz=4)
+    o, g = make_pair(st)
+    n_o = o.run(endtime=0.2)
+    n_g = g.run(endtime=0.2)
+    assert n_o == n_g and n_o > 4000
+    co, cg = o.clock(), g.clock()
+    for key in ("time", "dt", "dtold", "step"):
+        assert co[key] == cg[key], (key, co[key], cg[key])
+    assert cg["time"] == 0.2
+    compare(o, g, "end of the C1 run")
+    g.close()
+    o.close()
+
+
 def test_upload_download_roundtrip_and_clock():
     st = small_random_box(nx=9, ny=8, nz=7, seed=12)
     g = Hydro(st.params)
@@ -224,3 +243,28 @@ def test_upload_conserved_continues_bit_for_bit():
         g2.step()
     assert g2.status()[1] == 1
     assert np.array_equal(g.download()[0], g2.download()[0])
+
+
+@pytest.mark.parametrize("shape,walls", [((15, 13, 9), (0,) * 6), ((14, 12, 4), (1, 0, 0, 1, 1, 0)),
+                                         ((12, 11, 8), (1,) * 6)])
+def test_avisc_qq_matches_the_oracle(shape, walls):
+    """avisc.f90:4-26 on the device: qq bit for bit against the oracle's
+    restatement, zero before the first call and at the default avmag = 0, the
+    state untouched; again after fused steps (qq reads the reference's u)."""
+    nx, ny, nz = shape
+    st = small_random_box(nx=nx, ny=ny, nz=nz, walls=walls, seed=nx + nz, amp=0.4)
+    o, g = make_pair(st)
+    assert not g.qq().any()
+    g.avisc()
+    assert not g.qq().any()
+    avmag = (0.7, 1.3, 2.1)
+    g.set_avmag(*avmag)
+    g.avisc()
+    assert np.array_equal(g.qq(), o.avisc(*avmag))
+    assert g.qq()[G.boundary_flags(nx, ny, nz) > 0].any()
+    compare(o, g, "avisc leaves the state alone")
+    step_both(o, g, 3)
+    g.avisc()
+    assert np.array_equal(g.qq(), o.avisc(*avmag))
+    g.close()
+    o.close()
