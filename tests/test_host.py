@@ -1,6 +1,6 @@
 """Host-side logic that needs no GPU: the C ABI library loads and exports every
 symbol of include/boxzy_gpu.h, the ctypes layer and the Fortran interface module
-of the integration guide bind those prototypes with matching argument types, its
+(include/boxzy_gpu.f90) bind those prototypes with matching argument types, its
 ghost-fill plans reproduce the oracle's set_ghost_cells sweeps exactly (and grids
 beyond int32 cell indices are refused), namelist parsing, and grid geometry."""
 import ctypes
@@ -240,16 +240,17 @@ def _split_top(s):
     return out
 
 
-def _fortran_blocks():
-    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    return re.findall(r"```fortran\n(.*?)```", text, flags=re.S)
+def _fortran_source(name):
+    text = open(os.path.join(ROOT, "include", name)).read()
+    src = re.sub(r"!.*", "", text)
+    return re.sub(r"&\s*\n\s*", " ", src)
 
 
 def fortran_module():
-    mod = [b for b in _fortran_blocks() if b.startswith("module boxzy_gpu")]
-    assert len(mod) == 1
-    src = re.sub(r"!.*", "", mod[0])
-    return re.sub(r"&\s*\n\s*", " ", src)
+    """The interface module (include/boxzy_gpu.f90) up to its `contains`."""
+    src = _fortran_source("boxzy_gpu.f90")
+    assert src.count("module boxzy_gpu") == 2
+    return src.split("\ncontains\n")[0]
 
 
 def _fortran_decls(body):
@@ -310,11 +311,12 @@ def _fortran_matches(decl, c_param):
 
 
 def test_fortran_interfaces_match_the_header():
-    """The ISO_C_BINDING module of the integration guide (what a maintainer adds
-    to the reference) against include/boxzy_gpu.h: every interface binds an
-    exported C name with the right argument count, kinds, widths and passing
-    (value or reference), its bind(c) types lay out the C structs field by field,
-    and every bx_ call of the guide's Fortran snippets has an interface."""
+    """The ISO_C_BINDING module include/boxzy_gpu.f90 (what a maintainer adds to
+    the reference) against include/boxzy_gpu.h: every interface binds an exported
+    C name with the right argument count, kinds, widths and passing (value or
+    reference), its bind(c) types lay out the C structs field by field, and every
+    bx_ call of its procedures and of the main loop (include/boxzy_gpu_loop.f90)
+    has an interface."""
     src = fortran_module()
     protos = {n: (r, p) for n, r, p in header_prototypes()}
     bad, fnames = [], set()
@@ -351,15 +353,19 @@ def test_fortran_interfaces_match_the_header():
                 fields += [(mm.group(1), _F_KINDS[left.strip()])] * int(mm.group(3) or 1)
         if fields != structs.get(name):
             bad.append(f"type {name}: {fields} vs C {structs.get(name)}")
-    # calls in the guide's Fortran snippets
+    # calls in the module's own procedures and in the main loop
+    helpers = _fortran_source("boxzy_gpu.f90").split("\ncontains\n")[1]
+    own = set(re.findall(r"function\s+(bx_\w+)\s*\(", helpers))
+    assert {"bx_message", "bx_advance_to"} <= own
+    loop = _fortran_source("boxzy_gpu_loop.f90")
+    assert "subroutine bx_main_loop" in loop
     called = set()
-    for b in _fortran_blocks():
-        if b.startswith("module boxzy_gpu"):
-            continue
-        called |= set(re.findall(r"\b(bx_\w+)\s*\(", re.sub(r"!.*", "", b)))
+    for body in (helpers, loop):
+        called |= set(re.findall(r"\b(bx_\w+)\s*\(", body))
     types = {"bx_params", "bx_eos_table"}
-    missing = sorted(called - fnames - types - {"bx_message"})
+    missing = sorted(called - fnames - types - own - {"bx_main_loop"})
     assert not missing, missing
+    assert {"bx_run", "bx_step", "bx_download", "bx_advance_to"} <= called
     assert not bad, bad
 
 
