@@ -18,12 +18,17 @@ The JSON line also carries the end-to-end figure through the C ABI with host
 arrays (bx_step_host: cons from pinned memory in, one step, cons back, every
 step; the three separate calls and the full cons/u/p arrays beside it), the
 HBM roofline of the dominant stage kernel, the FP64 roofline, nvidia-smi clocks
-sampled during the timed region and the oracle timed on the host cores.
+sampled during the timed region, the oracle timed on the host cores, the GPU
+path against the oracle on the same 256^3 state after a few steps (`parity`),
+and the other two figures of the metric at their own configurations:
+`adjoint_c4` (adjoint/forward time ratio, 128^3, 200 steps, 15 snapshots, with
+finite-difference checks) and `batched_c3` (4096 Riemann boxes, 50 steps,
+boxes/s against the plain path looped over the same ensemble).
 
 reference: the reference's algorithm on the CPU (oracle/bx_oracle.c, a
 line-by-line C restatement of the Fortran, OpenMP on all host cores, ghost loop
-parallel like the reference's) on a bounded sample of the same workload; rank 0
-only.
+parallel like the reference's) on the same 256^3 workload (--ref-n to shrink
+it), K steps after W warm-up steps; rank 0 only.
 """
 from __future__ import annotations
 
@@ -140,6 +145,44 @@ def cpu_sample(st, steps=2, seconds=10.0, threads=None):
     return cells * n / dt, threads, dt, n
 
 
+def parity_full_size(st, steps):
+    """The GPU path and the oracle advanced `steps` steps from the same full-size
+    state (the oracle with the sequential ghost sweep, the order the GPU
+    implements); the reference's arrays after the last step and the clock after
+    every step compared.  Bit-identical results give zero differences."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from boxzyhydro_b200.hydro import Hydro
+    O.set_threads(os.cpu_count())
+    o = O.Oracle(st.params)
+    o.set_state(st.cons, st.u, st.p, st.adindx)
+    g = Hydro(st.params)
+    g.upload_state(st)
+    clock_equal, paths = True, []
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        if not (o.step() and g.step()):
+            break
+        paths.append(g.status()[1])
+        co, cg = o.clock(), g.clock()
+        clock_equal &= all(co[k] == cg[k] for k in ("time", "dt", "dtold", "step"))
+    c0, u0, p0, _ = o.get_state()
+    c1, u1, p1 = g.download()
+    g.close()
+    o.close()
+    rel = float(np.max(np.abs(c0 - c1) / np.maximum(np.abs(c0), 1e-300)))
+    return {"steps": len(paths), "max_rel_diff_cons": rel,
+            "max_abs_diff_u": float(np.max(np.abs(u0 - u1))),
+            "max_abs_diff_p": float(np.max(np.abs(p0 - p1))),
+            "bit_identical": bool(np.array_equal(c0, c1) and np.array_equal(u0, u1)
+                                  and np.array_equal(p0, p1)),
+            "clock_equal": bool(clock_equal),
+            "gpu_path_per_step": ["fused" if x == 1 else "per-phase" for x in paths],
+            "oracle": "oracle/bx_oracle.c, sequential ghost sweep, OpenMP",
+            "wall_s": time.perf_counter() - t0}
+
+
 def physics_arm(args, rank, world, local):
     """The rows beyond the plain step on the turbulent box: angular-momentum
     fluxing (fluxangmom, yoffset 0.25), the tabulated EOS (H2STAT >= 0 with
@@ -155,7 +198,7 @@ def physics_arm(args, rank, world, local):
     import torch
     from boxzyhydro_b200 import grid as G
     from boxzyhydro_b200 import ic
-    from boxzyhydro_b200.eos_table import synthetic_table
+    from tests.eos_tables import synthetic_table
     from boxzyhydro_b200.hydro import Hydro
 
     if rank != 0:
@@ -276,7 +319,7 @@ def reference_arm(args, rank):
     dt = time.perf_counter() - t0
     cells = st.params.n_active()
     value = cells * args.steps / dt
-    sample = (f"{n}^3-interior box of the same turbulent workload ({cells} cells), "
+    sample = (f"{n}^3-interior turbulent box ({cells} cells), "
               f"{args.steps} steps after {args.warmup} warm-up, C restatement of the "
               "reference loop (oracle/bx_oracle.c), OpenMP, parallel ghost loop")
     line = {
@@ -284,8 +327,10 @@ def reference_arm(args, rank):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": dt / args.steps * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": f"turbulent box {n}^3 interior (sample of the 256^3 workload), "
-                               "gamma=5/3, CFL 0.4, outflow walls", "cells_per_step": cells},
+        "config": {"workload": f"turbulent box {n}^3 interior ({st.params.nx}x{st.params.ny}x"
+                               f"{st.params.nz} with ghosts), lognormal rho sigma_ln=0.5, "
+                               "solenoidal Mach-1 v, p=1, gamma=5/3, CFL 0.4, outflow walls",
+                   "cells_per_step": cells},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                          "sample": sample},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
@@ -296,6 +341,13 @@ def reference_arm(args, rank):
 
 
 def batched_arm(args, rank, world, local):
+    line = batched_measure(args, rank, world, local)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def batched_measure(args, rank, world, local, init_dist=True):
     """C3: an ensemble of independent Riemann boxes (sides drawn from
     {32,48,64,96}, interior), each with its own gamma and dt, advanced `steps`
     steps in CUDA-graph runs of the batched path; boxes/s = boxes x steps / device
@@ -310,7 +362,7 @@ def batched_arm(args, rank, world, local):
     from boxzyhydro_b200.hydro import Hydro
 
     torch.cuda.set_device(local)
-    if world > 1:
+    if world > 1 and init_dist:
         import torch.distributed as dist
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=300),
@@ -416,14 +468,21 @@ def batched_arm(args, rank, world, local):
         "gpu_launches": launches,
         "wall_s": time.perf_counter() - t_wall0,
     }
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    if world > 1:
+    if world > 1 and init_dist:
+        import torch.distributed as dist
         dist.destroy_process_group()
-    return 0
+    return line
 
 
 def adjoint_arm(args, rank, world, local):
+    if rank != 0:
+        return 0  # one GPU: the adjoint runs on rank 0 only
+    line = adjoint_measure(args, local)
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def adjoint_measure(args, local):
     """Discrete adjoint of an n^3 run of `steps` steps.  Loss
     0.5*||rho(T) - rho_target||^2 over interior cells; rho_target is the run of
     the unperturbed state (x-split state) or 1.01*rho(T) (turbulent state).
@@ -439,8 +498,6 @@ def adjoint_arm(args, rank, world, local):
     from boxzyhydro_b200 import ic
     from boxzyhydro_b200.adjoint import AdjointEngine
 
-    if rank != 0:
-        return 0  # one GPU: the adjoint runs on rank 0 only
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
     n = args.n
@@ -559,9 +616,7 @@ def adjoint_arm(args, rank, world, local):
                      "per_direction": rel},
     }
     eng.close()
-    if rank == 0:
-        print(json.dumps(line), flush=True)
-    return 0
+    return line
 
 
 def main():
@@ -571,7 +626,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--n", type=int, default=256)
-    ap.add_argument("--ref-n", type=int, default=128, dest="ref_n")
+    ap.add_argument("--ref-n", type=int, default=0, dest="ref_n",
+                    help="box of the reference arm (default: --n, the headline box)")
     ap.add_argument("--seed", type=int, default=1234)
     ap.add_argument("--e2e-steps", type=int, default=10, dest="e2e_steps")
     ap.add_argument("--cpu-steps", type=int, default=2, dest="cpu_steps",
@@ -590,8 +646,14 @@ def main():
     ap.add_argument("--check-boxes", type=int, default=16, dest="check_boxes")
     ap.add_argument("--no-autotune", action="store_true", dest="no_autotune")
     ap.add_argument("--loop-sample", type=int, default=8, dest="loop_sample")
+    ap.add_argument("--parity-steps", type=int, default=3, dest="parity_steps",
+                    help="steps of the full-size GPU-vs-oracle comparison (0: skip)")
+    ap.add_argument("--no-extra", action="store_true", dest="no_extra",
+                    help="skip the adjoint (C4) and batched (C3) figures of the default line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
+    if args.ref_n <= 0:
+        args.ref_n = args.n
 
     rank = env_int("RANK", 0)
     world = env_int("WORLD_SIZE", 1)
@@ -782,6 +844,38 @@ def main():
                          "the reference loop), OpenMP on all host threads"}
 
     g.close()
+    del g
+
+    # ---- GPU against the oracle on the full-size workload (rank 0, one GPU)
+    parity = None
+    if rank == 0 and world == 1 and not args.no_cpu and args.parity_steps > 0:
+        parity = parity_full_size(st, args.parity_steps)
+
+    # ---- the other two BASELINE figures at their configurations (one GPU):
+    # the adjoint/forward time ratio (C4: 128^3, 200 steps, 15 snapshots) and
+    # the batched ensemble's boxes/s against the looped plain path (C3: 4096 boxes)
+    adjoint_c4 = batched_c3 = None
+    if world == 1 and not args.no_extra:
+        import argparse as _ap
+        del st
+        torch.cuda.empty_cache()
+        a4 = _ap.Namespace(**vars(args))
+        a4.n, a4.steps, a4.snapshots, a4.stage0_cache = 128, 200, 15, 8
+        a4.keep_stage0, a4.adj_ic, a4.fd_dirs = False, "blob", 16
+        try:
+            adjoint_c4 = adjoint_measure(a4, local)
+        except Exception as e:  # noqa: BLE001
+            adjoint_c4 = {"error": f"{type(e).__name__}: {e}"}
+        torch.cuda.empty_cache()
+        a3 = _ap.Namespace(**vars(args))
+        a3.nbox, a3.steps, a3.warmup, a3.check_boxes = 4096, 50, 3, 16
+        a3.no_autotune, a3.loop_sample = False, 8
+        try:
+            batched_c3 = batched_measure(a3, rank, world, local, init_dist=False)
+        except Exception as e:  # noqa: BLE001
+            batched_c3 = {"error": f"{type(e).__name__}: {e}"}
+        torch.cuda.empty_cache()
+
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world,
@@ -800,6 +894,9 @@ def main():
             "roofline_fp64": fp64,
             "e2e": e2e,
             "cpu_baseline": cpu,
+            "parity": parity,
+            "adjoint_c4": adjoint_c4,
+            "batched_c3": batched_c3,
             "gpu_launches": prof["launches"],
             "path": "fused stage kernels" if path == 1 else "per-phase kernels",
             "status_bits": bits,

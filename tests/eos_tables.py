@@ -7,7 +7,7 @@ from __future__ import annotations
 
 import numpy as np
 
-from . import celldump as CD
+from boxzyhydro_b200 import celldump as CD
 
 
 def synthetic_table(neos: int = 40, neos_rho: int = 9, seed: int = 0) -> dict:

@@ -1,9 +1,8 @@
 """Regenerate the golden fixtures of this directory from the reference's own files.
 
-Run in a container where the reference tree is mounted (path as first argument,
-default /root/reference):
+Run where the reference tree is available, with its path as the argument:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path to the reference tree>
 
 * sod_exact_t0.4.txt   -- analysis/sod.ana unchanged: the exact Sod solution the
   reference ships (x, rho, u, p at t=0.4, gamma=1.4, diaphragm at 0).
@@ -39,4 +38,6 @@ def main(ref):
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_golden.py <path to the reference tree>")
+    main(sys.argv[1])

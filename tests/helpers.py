@@ -68,6 +68,6 @@ def step_both(o, g, nsteps, endtime=1e300, check_every=1):
 
 def synthetic_eos_table(neos=40, neos_rho=9, seed=0):
     """Tables in the layout of the eos module for the tabulated state() path
-    (boxzyhydro_b200.eos_table.synthetic_table)."""
-    from boxzyhydro_b200.eos_table import synthetic_table
+    (tests/eos_tables.py)."""
+    from tests.eos_tables import synthetic_table
     return synthetic_table(neos, neos_rho, seed)

@@ -255,7 +255,7 @@ def test_tabulated_state_of_an_ideal_gas_table_is_the_fixed_gamma_state():
     eos.f90:653-699) gives the fixed-gamma pressure (state.f90:49-59) to
     rounding, and gamma and mu exactly; energies beyond the table are clamped."""
     import dataclasses
-    from boxzyhydro_b200.eos_table import synthetic_table
+    from tests.eos_tables import synthetic_table
     st = small_random_box(nx=12, ny=11, nz=10, walls=(0,) * 6, seed=7)
     hp = st.params
     gam, mu = 5.0 / 3.0, 2.3
