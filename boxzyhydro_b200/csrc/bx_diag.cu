@@ -49,6 +49,7 @@ __global__ void k_divcheck(unsigned long long n, unsigned long long seed, int er
     double a = rnd(z2, erange, true);
     if ((i & 7) == 0) a = d * (double)(long long)(z2 % 1000003ull);  // exact multiples
     if ((i & 15) == 1) a = __longlong_as_double(__double_as_longlong(d) + (long long)(z2 % 5) - 2);
+    if ((i & 31) == 2) a = ((z2 >> 7) & 1) ? -0.0 : 0.0;  // signed zeros
     const bx::SharedDiv div(d);
     const double q = div(a), q2 = bx::cdiv(a, d, 1.0 / d), ref = a / d;
     const bool ok1 = __double_as_longlong(q) == __double_as_longlong(ref) || (q == 0.0 && ref == 0.0);
@@ -56,7 +57,14 @@ __global__ void k_divcheck(unsigned long long n, unsigned long long seed, int er
     const bool in_window = d >= 0x1p-450 && d <= 0x1p+450;
     const bool ok2 = !in_window || __double_as_longlong(q2) == __double_as_longlong(ref) ||
                      (q2 == 0.0 && ref == 0.0);
-    if (!(ok1 && ok2)) {
+    // the HLL form: every bit of the IEEE quotient, the sign of a zero included,
+    // wherever quot_fast_ok admits the numerator and d lies in the window
+    bool ok3 = true;
+    if (in_window && bx::quot_fast_ok(a)) {
+      const double q3 = bx::quot_fast(a, d, __drcp_rn(d));
+      ok3 = __double_as_longlong(q3) == __double_as_longlong(ref);
+    }
+    if (!(ok1 && ok2 && ok3)) {
       if (atomicAdd(bad, 1ull) == 0) { example[0] = a; example[1] = d; }
     }
   }

@@ -37,9 +37,21 @@ BX_HD double slope3(double c0, double c1, double c2) {
   const double d1 = c1 - c0, d2 = c2 - c0, d3 = c2 - c1;
   const double x1 = kTheta * d1, x2 = kHalf * d2, x3 = kTheta * d3;
   const double m = fmin(fabs(x1), fmin(fabs(x2), fabs(x3)));
+#ifdef __CUDA_ARCH__
+  // The same selection on the bit images, off the FP64 pipe: when d1 or d3 is
+  // a zero, x1 or x3 is one and m = 0, the reference's +0; otherwise d1 and d3
+  // share a strict sign exactly when their sign bits agree, and the result is
+  // m with that sign.  So: m != 0 and equal sign bits give m with d1's sign bit,
+  // anything else +0 (NaN inputs, which the guards flag, aside).
+  const int h1 = __double2hiint(d1), h3 = __double2hiint(d3);
+  const int hm = __double2hiint(m), lm = __double2loint(m);
+  const bool take = ((h1 ^ h3) >= 0) && ((hm | lm) != 0);
+  return take ? __hiloint2double(hm | (h1 & (int)0x80000000), lm) : 0.0;
+#else
   const bool pos = (d1 > 0.0) && (d3 > 0.0);
   const bool neg = (d1 < 0.0) && (d3 < 0.0);
   return pos ? m : (neg ? -m : 0.0);
+#endif
 }
 
 // K = rho*half*(u1^2+u2^2+u3^2) (state.f90:32,47) and the same value written
@@ -117,6 +129,15 @@ BX_HD double courant_rate(double d, double p, double gam, double u1, double u2, 
          cdiv(sound + fabs(u3), dz, idz);
 }
 
+#ifdef __CUDACC__
+// courant_rate with the division by rho through a SharedDiv of rho
+template <bool POW2>
+__device__ __forceinline__ double courant_rate_q(const struct SharedDiv& qd, double p, double gam,
+                                                 double u1, double u2, double u3, double dx,
+                                                 double dy, double dz, double idx, double idy,
+                                                 double idz);
+#endif
+
 // calculate_states for one cell and one direction (flux.f90:327-351):
 // lambda_p = max(u_d+c,0)*dt/ds, lambda_m = min(u_d-c,0)*dt/ds,
 // q- = q + half*(-1-lambda_m)*s, q+ = q + half*(1-lambda_p)*s.
@@ -157,6 +178,27 @@ BX_HD void ghost_states(const Prim& q, FaceState& mi, FaceState& pl) {
   pl = mi;
 }
 
+// The shared-denominator quotient below is exact for a numerator a when a = +-0
+// or |a| lies in [2^-450, 2^451): an integer test on the exponent field of its
+// bit image (biased exponents 573..1473), so it costs no FP64 instruction.
+__device__ __forceinline__ bool quot_fast_ok(double a) {
+  const unsigned hi = (unsigned)__double2hiint(a), lo = (unsigned)__double2loint(a);
+  const unsigned e = (hi >> 20) & 0x7ffu;
+  return (e - 573u <= 900u) || (((hi << 1) | lo) == 0u);
+}
+
+// q = a/d for five numerators over one denominator d, given r = RN(1/d) with d
+// in [2^-450, 2^450] and every a passing quot_fast_ok: q0 = RN(a r) and the
+// residual e = RN(a - d q0), exact under a fused multiply-add, give the
+// correctly rounded quotient RN(q0 + e r) (Markstein's theorem).  The residual
+// is formed as -RN(d q0 - a), the same value for every nonzero a, so that a = -0
+// yields -0 like a/d (q0 = -0 and e = -0).
+__device__ __forceinline__ double quot_fast(double a, double d, double r) {
+  const double q0 = a * r;
+  const double e = -fma(d, q0, -a);
+  return fma(e, r, q0);
+}
+
 // a/d for several numerators sharing one denominator d > 0.  With r the
 // correctly rounded reciprocal of d, q0 = RN(a*r) is within one ulp of a/d and
 // the residual a - d*q0 is exact under a fused multiply-add, so
@@ -164,8 +206,9 @@ BX_HD void ghost_states(const Prim& q, FaceState& mi, FaceState& pl) {
 // theorem, as used for IEEE division on FMA hardware).  The theorem needs the
 // quotient and the residual away from the overflow and subnormal ranges:
 // with d and |a| in [2^-450, 2^450] the quotient lies in [2^-900, 2^900] and
-// the residual (about |a|*2^-53) stays normal.  Outside that window (and for
-// a = 0) the IEEE division is taken instead.
+// the residual (about |a|*2^-53) stays normal.  quot_fast computes it (signed
+// zeros included) wherever quot_fast_ok admits a; outside that window the IEEE
+// division is taken instead.
 struct SharedDiv {
   double d, r;
   bool ok;
@@ -174,16 +217,34 @@ struct SharedDiv {
     r = ok ? __drcp_rn(den) : 0.0;
   }
   __device__ __forceinline__ double operator()(double a) const {
-    const double aa = fabs(a);
-    if (ok && aa >= 0x1p-450 && aa <= 0x1p+450) {
-      const double q0 = a * r;
-      const double e = fma(-d, q0, a);
-      return fma(e, r, q0);
-    }
-    if (ok && aa == 0.0) return a * r;  // signed zero, as a/d
+    if (ok && quot_fast_ok(a)) return quot_fast(a, d, r);
     return a / d;
   }
 };
+
+template <bool POW2>
+__device__ __forceinline__ double courant_rate_q(const SharedDiv& qd, double p, double gam,
+                                                 double u1, double u2, double u3, double dx,
+                                                 double dy, double dz, double idx, double idy,
+                                                 double idz) {
+  const double sound = sqrt(qd(gam * p));
+  if (POW2)
+    return (sound + fabs(u1)) * idx + (sound + fabs(u2)) * idy + (sound + fabs(u3)) * idz;
+  return cdiv(sound + fabs(u1), dx, idx) + cdiv(sound + fabs(u2), dy, idy) +
+         cdiv(sound + fabs(u3), dz, idz);
+}
+
+// half*(m1^2+m2^2+m3^2)/rho and the zero-force source() energy update with the
+// division by rho through a SharedDiv of rho
+__device__ __forceinline__ double kin_mom_q(const SharedDiv& qd, double m1, double m2,
+                                            double m3) {
+  return qd(kHalf * (m1 * m1 + m2 * m2 + m3 * m3));
+}
+__device__ __forceinline__ double source_energy_q(const SharedDiv& qd, double m1, double m2,
+                                                  double m3, double E, double small_eps) {
+  const double ek = kin_mom_q(qd, m1, m2, m3);
+  return fmax(E - ek, small_eps) + ek;
+}
 
 // HLL flux through one face normal to axis DIR (0,1,2) from the plus state of
 // the cell on the low side (L) and the minus state of the cell on the high side
@@ -191,44 +252,66 @@ struct SharedDiv {
 // Returns a nonzero code when ap+am == 0 (the reference divides by zero).
 template <int DIR>
 BX_HD void hll_flux(const FaceState& L, const FaceState& R, double gam, double F[5]) {
-  const double dl = L.d, pl = L.p, el = L.e, vxl = L.u1, vyl = L.u2, vzl = L.u3;
-  const double dr = R.d, pr = R.p, er = R.e, vxr = R.u1, vyr = R.u2, vzr = R.u3;
-  double sl[5], sr[5], fl[5], fr[5];
-  sl[0] = dl;
-  sl[1] = dl * vxl;
-  sl[2] = dl * vyl;
-  sl[3] = dl * vzl;
-  sl[4] = el + kHalf * dl * (vxl * vxl + vyl * vyl + vzl * vzl);
-  sr[0] = dr;
-  sr[1] = dr * vxr;
-  sr[2] = dr * vyr;
-  sr[3] = dr * vzr;
-  sr[4] = er + kHalf * dr * (vxr * vxr + vyr * vyr + vzr * vzr);
-  const double vl = DIR == 0 ? vxl : (DIR == 1 ? vyl : vzl);
-  const double vr = DIR == 0 ? vxr : (DIR == 1 ? vyr : vzr);
-  fl[0] = sl[0] * vl;
-  fr[0] = sr[0] * vr;
-  // fluxes_l(2..4) = (p on the normal component, 0 elsewhere) + states*v
-  fl[1] = DIR == 0 ? pl + sl[1] * vl : sl[1] * vl;
-  fl[2] = DIR == 1 ? pl + sl[2] * vl : sl[2] * vl;
-  fl[3] = DIR == 2 ? pl + sl[3] * vl : sl[3] * vl;
-  fr[1] = DIR == 0 ? pr + sr[1] * vr : sr[1] * vr;
-  fr[2] = DIR == 1 ? pr + sr[2] * vr : sr[2] * vr;
-  fr[3] = DIR == 2 ? pr + sr[3] * vr : sr[3] * vr;
-  fl[4] = (sl[4] + pl) * vl;
-  fr[4] = (sr[4] + pr) * vr;
-  const double cr = sqrt(gam * pr / dr);
-  const double cl = sqrt(gam * pl / dl);
+  // The wave speeds come first, then each component from its own state and
+  // flux terms, so only the two face states and the speeds stay live across
+  // the components (every expression is the reference's, in its order).
+  const double vl = DIR == 0 ? L.u1 : (DIR == 1 ? L.u2 : L.u3);
+  const double vr = DIR == 0 ? R.u1 : (DIR == 1 ? R.u2 : R.u3);
+  const double cr = sqrt(gam * R.p / R.d);
+  const double cl = sqrt(gam * L.p / L.d);
   const double ap = fmax(fmax(0.0, vr + cr), vl + cl);
   const double am = fmax(fmax(0.0, -(vr - cr)), -(vl - cl));
   const double apam = ap * am;
   const double den = ap + am;
+  // the numerators first; they all share the denominator ap+am
+#define BX_HLL_Q(x) (x)
+  // component 0: the mass flux
+  {
+    const double sl = L.d, sr = R.d;
+    const double fl = sl * vl, fr = sr * vr;
+    F[0] = BX_HLL_Q(ap * fl + am * fr - apam * (sr - sl));
+  }
+  // components 1-3: momenta, with the pressure on the normal component
+  {
+    const double sl = L.d * L.u1, sr = R.d * R.u1;
+    const double fl = DIR == 0 ? L.p + sl * vl : sl * vl;
+    const double fr = DIR == 0 ? R.p + sr * vr : sr * vr;
+    F[1] = BX_HLL_Q(ap * fl + am * fr - apam * (sr - sl));
+  }
+  {
+    const double sl = L.d * L.u2, sr = R.d * R.u2;
+    const double fl = DIR == 1 ? L.p + sl * vl : sl * vl;
+    const double fr = DIR == 1 ? R.p + sr * vr : sr * vr;
+    F[2] = BX_HLL_Q(ap * fl + am * fr - apam * (sr - sl));
+  }
+  {
+    const double sl = L.d * L.u3, sr = R.d * R.u3;
+    const double fl = DIR == 2 ? L.p + sl * vl : sl * vl;
+    const double fr = DIR == 2 ? R.p + sr * vr : sr * vr;
+    F[3] = BX_HLL_Q(ap * fl + am * fr - apam * (sr - sl));
+  }
+  // component 4: the energy, states(5) = eps + half*rho*|u|^2
+  {
+    const double sl = L.e + kHalf * L.d * (L.u1 * L.u1 + L.u2 * L.u2 + L.u3 * L.u3);
+    const double sr = R.e + kHalf * R.d * (R.u1 * R.u1 + R.u2 * R.u2 + R.u3 * R.u3);
+    const double fl = (sl + L.p) * vl, fr = (sr + R.p) * vr;
+    F[4] = BX_HLL_Q(ap * fl + am * fr - apam * (sr - sl));
+  }
+#undef BX_HLL_Q
 #ifdef __CUDA_ARCH__
-  const SharedDiv div(den);
+  const bool fast = den >= 0x1p-450 && den <= 0x1p+450 && quot_fast_ok(F[0]) &&
+                    quot_fast_ok(F[1]) && quot_fast_ok(F[2]) && quot_fast_ok(F[3]) &&
+                    quot_fast_ok(F[4]);
+  if (fast) {
+    const double r = __drcp_rn(den);
 #pragma unroll
-  for (int i = 0; i < 5; ++i) F[i] = div(ap * fl[i] + am * fr[i] - apam * (sr[i] - sl[i]));
+    for (int i = 0; i < 5; ++i) F[i] = quot_fast(F[i], den, r);
+  } else {
+#pragma unroll
+    for (int i = 0; i < 5; ++i) F[i] = F[i] / den;
+  }
 #else
-  for (int i = 0; i < 5; ++i) F[i] = (ap * fl[i] + am * fr[i] - apam * (sr[i] - sl[i])) / den;
+  for (int i = 0; i < 5; ++i) F[i] = F[i] / den;
 #endif
 }
 

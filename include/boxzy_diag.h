@@ -19,9 +19,10 @@ int bx_fp64_peak(double *tflops, double *ms);
 /* Self-check of the divisions by a shared denominator (HLL flux) and by a grid
  * constant with a precomputed reciprocal (cell sizes, cell volume): n random
  * (numerator, denominator) pairs with exponents in [-exp_range, exp_range] (plus
- * exact multiples and near-ties) are divided both ways on the device; returns the
- * number of results that differ from IEEE division in any bit (zeros of either
- * sign compare equal) and one example. */
+ * exact multiples, near-ties and signed zeros) are divided each way on the device;
+ * returns the number of results that differ from IEEE division in any bit (zeros of
+ * either sign compare equal, except for the five-numerator form of the HLL flux,
+ * whose zeros keep the IEEE sign) and one example. */
 int bx_check_shared_division(unsigned long long n, unsigned long long seed, int exp_range,
                              unsigned long long *mismatches, double *example_a,
                              double *example_d);
