@@ -3,7 +3,8 @@
 The reference advances one grid per process.  `Batch` advances many grids at
 once -- each with its own size, gamma, CFL number, dt and clock -- with the same
 stage kernels as `Hydro`, so every box evolves exactly as it would alone; a run
-of n steps is one CUDA graph launch.
+of n steps is one CUDA graph launch (four kernels per step, or one persistent
+kernel for the whole run).
 """
 from __future__ import annotations
 
@@ -67,10 +68,22 @@ class Batch:
     def run(self, nsteps, endtime=1e300, graph=True):
         self._c(lib().bx_batch_run(self._h, int(nsteps), float(endtime), 1 if graph else 0))
 
+    def set_persistent(self, enable=True):
+        """One launch per run (a queue of step/stage/tile items) instead of four
+        launches per step; the same results."""
+        self._c(lib().bx_batch_set_persistent(self._h, 1 if enable else 0))
+
+    @property
+    def persistent(self):
+        e = C.c_int32()
+        self._c(lib().bx_batch_get_persistent(self._h, C.byref(e)))
+        return bool(e.value)
+
     def autotune(self, reps=2):
-        """Pick the ensemble's tile depth by timing trial steps from the current
+        """Pick the ensemble's tile depth, then the launch form (four launches per
+        step or one persistent launch), by timing trial steps from the current
         states (left unchanged): returns (depth, ms per step); depth 0 is the
-        default rule, >= 2**30 whole box depths."""
+        default rule, >= 2**30 whole box depths; `persistent` tells the form."""
         zc = C.c_int32()
         ms = C.c_double()
         self._c(lib().bx_batch_autotune(self._h, int(reps), C.byref(zc), C.byref(ms)))
@@ -97,9 +110,20 @@ class Batch:
                     pool_cells=cells.value)
 
 
+def wait_selftest(poll_limit: int):
+    """The persistent launch's bounded wait on a counter nothing advances: returns
+    (gave_up, ms)."""
+    g = C.c_int32()
+    ms = C.c_double()
+    rc = lib().bx_batch_wait_selftest(int(poll_limit), C.byref(g), C.byref(ms))
+    if rc:
+        raise BoxzyError(rc, lib().bx_batch_last_error(None).decode())
+    return bool(g.value), ms.value
+
+
 def pool_bytes(params_list) -> int:
     """Device bytes a Batch of these boxes allocates (three plane sets)."""
     return sum(3 * 5 * 8 * hp.ngrid for hp in params_list)
 
 
-__all__ = ["Batch", "pool_bytes"]
+__all__ = ["Batch", "pool_bytes", "wait_selftest"]

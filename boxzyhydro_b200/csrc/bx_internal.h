@@ -191,6 +191,34 @@ cudaError_t box_check_clean(const Geom& g, const double* X, long long ps, int ng
                             Ctrl* ctrl, cudaStream_t s);
 cudaError_t box_rate(const Geom& g, const double* X, long long ps, Ctrl* ctrl, cudaStream_t s);
 cudaError_t launch_dt_batch(Ctrl* ctrl, int nbox, cudaStream_t s);
+
+// Persistent batched run: one launch works through a queue of items (step,
+// stage, tile) in step-major order; an item waits (bounded) for what it reads:
+// a stage-0 tile for its box's dt of the step, a stage-1 tile for all stage-0
+// tiles of its box.  The last stage-1 tile of a box advances the box's clock
+// (k_end_batch) and sets the next step's dt (k_dt_batch).
+struct PersistArgs {
+  StageArgs a;               // ctrl, geom, tiles (longest first), plane stride, U; nsrc 0
+  double* buf[3];            // the pooled plane sets
+  int cur;                   // plane set that holds the run's input
+  int nsteps;
+  int ntiles;
+  const int* tiles_of_box;   // tiles of each box in the list
+  unsigned* done0;           // per box: stage-0 tiles finished so far in the run
+  unsigned* done1;           // per box: stage-1 tiles finished so far in the run
+  unsigned* ready;           // per box: steps of the run whose dt is set
+  unsigned long long* head;  // next queue item
+  int* status;               // bit 0: a wait gave up
+  long long poll_limit;      // polls before a wait gives up
+};
+// the launch of a run (after launch_dt_batch for its first step); blocks_out:
+// the blocks launched (resident blocks per SM x SMs)
+cudaError_t launch_batch_persistent(const PersistArgs& p, int pm, bool threed, int nbox,
+                                    cudaStream_t s, int* blocks_out);
+// a wait of the persistent kernel on a counter nothing advances, with the given
+// poll limit: *gave_up = 1 when it returned without the counter (the check of
+// the bounded wait)
+cudaError_t persistent_wait_selftest(long long poll_limit, int* gave_up, float* ms);
 cudaError_t launch_end_batch(Ctrl* ctrl, int nbox, cudaStream_t s);
 
 

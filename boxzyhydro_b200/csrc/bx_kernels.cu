@@ -21,6 +21,7 @@
 //    steps where the velocity limiter or the low-density EOS branch fires.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <map>
 #include <mutex>
 #include <utility>
@@ -46,7 +47,14 @@ cudaError_t ensure_dyn_smem(const void* fn, size_t bytes) {
 
 namespace {
 
-__device__ __forceinline__ double ldg(const double* p) { return __ldg(p); }
+// Loads of the stage inputs: through the read-only path when the planes stay
+// unchanged for the whole launch (one launch per stage), from L2 (cg) in the
+// persistent batched kernel, whose other blocks write planes that this block
+// reads later in the same launch.
+template <bool CG = false>
+__device__ __forceinline__ double ldg(const double* p) {
+  return CG ? __ldcg(p) : __ldg(p);
+}
 
 // donor of a coordinate along one axis for a face ghost (fused path)
 __device__ __forceinline__ int remap_axis(int c, int a0, int a1, int wl, int wr, bool& flip) {
@@ -65,6 +73,7 @@ struct Cons {
   double d, m1, m2, m3, E;
 };
 
+template <bool CG = false>
 __device__ __forceinline__ Cons load_cons(const double* B, long long PS, const Geom& g, int x,
                                           int y, int z) {
   bool fx = false, fy = false, fz = false;
@@ -73,11 +82,11 @@ __device__ __forceinline__ Cons load_cons(const double* B, long long PS, const G
   const int zz = g.threed ? remap_axis(z, g.az0, g.az1, g.wall[4], g.wall[5], fz) : z;
   const long long c = g.base + xx + (long long)yy * g.sy + (long long)zz * g.sz;
   Cons r;
-  r.d = ldg(B + c);
-  r.m1 = ldg(B + PS + c);
-  r.m2 = ldg(B + 2 * PS + c);
-  r.m3 = ldg(B + 3 * PS + c);
-  r.E = ldg(B + 4 * PS + c);
+  r.d = ldg<CG>(B + c);
+  r.m1 = ldg<CG>(B + PS + c);
+  r.m2 = ldg<CG>(B + 2 * PS + c);
+  r.m3 = ldg<CG>(B + 3 * PS + c);
+  r.E = ldg<CG>(B + 4 * PS + c);
   if (fx) r.m1 = -r.m1;
   if (fy) r.m2 = -r.m2;
   if (fz) r.m3 = -r.m3;
@@ -86,6 +95,7 @@ __device__ __forceinline__ Cons load_cons(const double* B, long long PS, const G
 
 // the step input's velocity m/rho at a cell, as stage 0 stored it for the
 // interior cells (ghost cells read their source cell, reflected components negated)
+template <bool CG = false>
 __device__ __forceinline__ void load_u(const double* U, long long PS, const Geom& g, int x, int y,
                                        int z, double& u1, double& u2, double& u3) {
   bool fx = false, fy = false, fz = false;
@@ -93,9 +103,9 @@ __device__ __forceinline__ void load_u(const double* U, long long PS, const Geom
   const int yy = remap_axis(y, g.ay0, g.ay1, g.wall[2], g.wall[3], fy);
   const int zz = g.threed ? remap_axis(z, g.az0, g.az1, g.wall[4], g.wall[5], fz) : z;
   const long long c = g.base + xx + (long long)yy * g.sy + (long long)zz * g.sz;
-  u1 = ldg(U + c);
-  u2 = ldg(U + PS + c);
-  u3 = ldg(U + 2 * PS + c);
+  u1 = ldg<CG>(U + c);
+  u2 = ldg<CG>(U + PS + c);
+  u3 = ldg<CG>(U + 2 * PS + c);
   if (fx) u1 = -u1;
   if (fy) u2 = -u2;
   if (fz) u3 = -u3;
@@ -136,50 +146,89 @@ __device__ __forceinline__ void apply_sources(Cons& c, int nsrc, double small_ep
 //           sources still pending, then source(0) with the force, which kicks
 //           the momenta; state() then reads the velocity array of before the
 //           kick (main.f90:318-319 call state() before velocity()).
-template <int STAGE, bool GRAV = false>
-__device__ __forceinline__ Prim load_prim(const StageArgs& a, const Geom& g, int x, int y, int z,
-                                          unsigned& flags, int nsrc, double dth,
-                                          bool need_c = true) {
+// The values a cell's primitives are computed from: its conserved variables
+// (X in stage 0, Y in stage 1) and, in stage 1, the stage-0 velocity U, or,
+// in stage 0 with a force, the acceleration G.
+struct Raw {
+  Cons c;
+  double v1, v2, v3;
+};
+
+template <int STAGE, bool GRAV = false, bool CG = false>
+__device__ __forceinline__ Raw load_raw(const StageArgs& a, const Geom& g, int x, int y, int z) {
   const long long PS = a.ncells_total;
+  Raw r;
+  if (STAGE == 0) {
+    r.c = load_cons<CG>(a.X, PS, g, x, y, z);
+    if (GRAV) load_g(a.G, PS, g, x, y, z, r.v1, r.v2, r.v3);
+  } else {
+    r.c = load_cons<CG>(a.Y, PS, g, x, y, z);
+    load_u<CG>(a.U, PS, g, x, y, z, r.v1, r.v2, r.v3);
+  }
+  return r;
+}
+
+// Every division here is by the cell's density (the sources leave it alone):
+// one correctly rounded reciprocal serves them all (SharedDiv, exact).
+template <int STAGE, bool GRAV = false>
+__device__ __forceinline__ Prim prim_of(const Geom& g, Raw r, unsigned& flags, int nsrc,
+                                        double dth, bool need_c = true) {
   Prim q;
+  const SharedDiv qd(r.c.d);
   if (STAGE == 0 && GRAV) {
-    Cons c = load_cons(a.X, PS, g, x, y, z);
-    double g1, g2, g3, v1, v2, v3;
-    load_g(a.G, PS, g, x, y, z, g1, g2, g3);
+    Cons c = r.c;
+    double v1, v2, v3;
     apply_sources(c, nsrc - 1, g.small_eps);
-    gravity_source0(c, g1, g2, g3, dth, g.small_eps, v1, v2, v3);
+    gravity_source0(c, r.v1, r.v2, r.v3, dth, g.small_eps, v1, v2, v3);
     q.d = c.d;
-    q.u1 = c.m1 / c.d;
-    q.u2 = c.m2 / c.d;
-    q.u3 = c.m3 / c.d;
+    q.u1 = qd(c.m1);
+    q.u2 = qd(c.m2);
+    q.u3 = qd(c.m3);
     q.e = recon_eps(q.d, c.E, q.u1, q.u2, q.u3, g.small_eps);
     q.p = eos_pressure(q.d, c.E, v1, v2, v3, g.gm1, g.small_eps);
   } else if (STAGE == 0) {
-    Cons c = load_cons(a.X, PS, g, x, y, z);
-    apply_sources(c, nsrc, g.small_eps);
+    Cons c = r.c;
+    for (int k = 0; k < nsrc; ++k) c.E = source_energy_q(qd, c.m1, c.m2, c.m3, c.E, g.small_eps);
     q.d = c.d;
-    q.u1 = c.m1 / c.d;
-    q.u2 = c.m2 / c.d;
-    q.u3 = c.m3 / c.d;
+    q.u1 = qd(c.m1);
+    q.u2 = qd(c.m2);
+    q.u3 = qd(c.m3);
     q.e = recon_eps(q.d, c.E, q.u1, q.u2, q.u3, g.small_eps);
     q.p = q.e * g.gm1;
   } else {
-    const Cons c1 = load_cons(a.Y, PS, g, x, y, z);
-    double s1, s2, s3;
-    load_u(a.U, PS, g, x, y, z, s1, s2, s3);
+    const Cons c1 = r.c;
     q.d = c1.d;
-    q.u1 = c1.m1 / c1.d;
-    q.u2 = c1.m2 / c1.d;
-    q.u3 = c1.m3 / c1.d;
+    q.u1 = qd(c1.m1);
+    q.u2 = qd(c1.m2);
+    q.u3 = qd(c1.m3);
     q.e = recon_eps(q.d, c1.E, q.u1, q.u2, q.u3, g.small_eps);
-    q.p = eos_pressure(q.d, c1.E, s1, s2, s3, g.gm1, g.small_eps);
+    q.p = eos_pressure(q.d, c1.E, r.v1, r.v2, r.v3, g.gm1, g.small_eps);
   }
   // the sound speed enters only the lambdas of cells whose face states are built
-  q.c = need_c ? sqrt(q.p * g.gam / q.d) : 0.0;
+  q.c = need_c ? sqrt(qd(q.p * g.gam)) : 0.0;
   if (q.d < kLowRho) flags |= kFlagLowRho;
   if (fabs(q.u1) > g.vlimit || fabs(q.u2) > g.vlimit || fabs(q.u3) > g.vlimit)
     flags |= kFlagVlimit;
   return q;
+}
+
+// Primitives seen by flux(avg) at a cell.
+//  stage 0: cons = src^nsrc(X); u = m/rho (velocity at main.f90:318); p from
+//           state() with the velocity array of the previous step, which equals
+//           m/rho of the same momenta (source adds zero momentum).
+//  stage 1: cons = Y; u = m/rho of Y (velocity at main.f90:355); p from state()
+//           with the stage-0 velocity m0/rho0 (main.f90:353 uses the stale u),
+//           which stage 0 stored in U (the same quotient, so the same bits).
+//  GRAV (a gravitational force this step): stage 0 takes the nsrc-1 force-free
+//           sources still pending, then source(0) with the force, which kicks
+//           the momenta; state() then reads the velocity array of before the
+//           kick (main.f90:318-319 call state() before velocity()).
+template <int STAGE, bool GRAV = false, bool CG = false>
+__device__ __forceinline__ Prim load_prim(const StageArgs& a, const Geom& g, int x, int y, int z,
+                                          unsigned& flags, int nsrc, double dth,
+                                          bool need_c = true) {
+  return prim_of<STAGE, GRAV>(g, load_raw<STAGE, GRAV, CG>(a, g, x, y, z), flags, nsrc, dth,
+                              need_c);
 }
 
 template <bool POW2>
@@ -209,6 +258,7 @@ constexpr int NZS = 16;
 // the face fluxes of phases C/D alias the primitives of phases A/B
 constexpr int NR0 = (7 * NP > 5 * (NFX + NFY)) ? 7 * NP : 5 * (NFX + NFY);
 constexpr int SMEM_DOUBLES = NR0 + 12 * NSX + 12 * NSY + NZS * NT;
+static_assert(4 * (TX + TY) <= NT, "one halo cell per thread and plane at most");
 
 __device__ __forceinline__ void put_prim(double* SP, int i, const Prim& q) {
   SP[0 * NP + i] = q.d;
@@ -259,19 +309,20 @@ __device__ __forceinline__ double warp_max(double v) {
 // ------------------------------------------------------------------ stage kernel
 // One tile of one stage.  FULL: the tile is a whole TX x TY block of interior
 // columns, so its extents are compile-time constants.
-template <int STAGE, bool POW2, bool THREED, bool FULL, bool GRAV>
+// dt: the step's full dt; nsrc: the sources the stage input is short of (both
+// read from the box's control block by the caller).  CG: inputs through L2 (the
+// persistent batched kernel).
+template <int STAGE, bool POW2, bool THREED, bool FULL, bool GRAV, bool CG = false>
 __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, const Geom& g,
-                                           Ctrl* C, double* sm, double* red_rate,
-                                           unsigned* red_flags) {
+                                           Ctrl* C, double dt, int nsrc, double* sm,
+                                           double* red_rate, unsigned* red_flags) {
   double* SP = sm;                    // [7][TY+4][TX+4] primitives of the plane
   double* SX = sm + NR0;              // [12][TY][TX+2] x states (minus 0..5, plus 6..11)
   double* SY = SX + 12 * NSX;         // [12][TY+2][TX] y states
   double* FX = sm;                    // [5][TY][TX+1] x face fluxes (aliases SP)
   double* FY = sm + 5 * NFX;          // [5][TY+1][TX] y face fluxes
   double* ZS = SY + 12 * NSY;         // [16][NT]: Fzm 0-4, Fzp 5-9, plus state 10-15
-  const double dt = C->dt;
   const double dth = dt * kHalf;  // the sources' half step (main.f90:282,471)
-  const int nsrc = a.nsrc > 0 ? a.nsrc : C->nsrc;
 
   const int tid = threadIdx.x;
   const int tx = tid % TX, ty = tid / TX;
@@ -295,10 +346,10 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
 
   const int z0 = g.az0 + t.z0, z1 = g.az0 + t.z1;
   if (THREED && own) {
-    const Prim Pm2 = load_prim<STAGE, GRAV>(a, g, gx, gy, z0 - 2, flags, nsrc, dth);
-    const Prim Pm1 = load_prim<STAGE, GRAV>(a, g, gx, gy, z0 - 1, flags, nsrc, dth);
-    Pk = load_prim<STAGE, GRAV>(a, g, gx, gy, z0, flags, nsrc, dth);
-    Pk1 = load_prim<STAGE, GRAV>(a, g, gx, gy, z0 + 1, flags, nsrc, dth);
+    const Prim Pm2 = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z0 - 2, flags, nsrc, dth);
+    const Prim Pm1 = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z0 - 1, flags, nsrc, dth);
+    Pk = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z0, flags, nsrc, dth);
+    Pk1 = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z0 + 1, flags, nsrc, dth);
     FaceState mm, pm, m0;
     if (z0 - 1 < g.az0) {
       ghost_states(Pm1, mm, pm);
@@ -335,9 +386,9 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
     FaceState mz1, pz1;
     if (own) {
       if (THREED) {
-        P2 = load_prim<STAGE, GRAV>(a, g, gx, gy, z + 2, flags, nsrc, dth);
+        P2 = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z + 2, flags, nsrc, dth);
       } else {
-        Pk = load_prim<STAGE, GRAV>(a, g, gx, gy, z, flags, nsrc, dth);
+        Pk = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z, flags, nsrc, dth);
       }
       put_prim(SP, (ty + 2) * PW + (tx + 2), Pk);
       if (STAGE == 0) {
@@ -348,7 +399,10 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         a.U[2 * PS + o] = Pk.u3;
       }
     }
-    // halo cells go first to the threads without a column of their own
+    // halo cells go first to the threads without a column of their own (at most
+    // one per thread: 4*(TX+TY) <= NT).  Their loads are not issued before the
+    // own column's arithmetic: holding both cells' values at once spills
+    // registers and measured 14 % slower.
     for (int i = (tid + NT - TX * TY) % NT; i < nhalo; i += NT) {
       int cx, cy;
       if (i < 4 * h) {
@@ -365,7 +419,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
       const int fx = bx0 + cx, fy = by0 + cy;
       const bool near = cx >= -1 && cx <= w && cy >= -1 && cy <= h;
       const bool inner = fx >= g.ax0 && fx < g.ax1 && fy >= g.ay0 && fy < g.ay1;
-      const Prim q = load_prim<STAGE, GRAV>(a, g, fx, fy, z, flags, nsrc, dth, near && inner);
+      const Prim q = load_prim<STAGE, GRAV, CG>(a, g, fx, fy, z, flags, nsrc, dth, near && inner);
       put_prim(SP, (cy + 2) * PW + (cx + 2), q);
     }
     if (THREED && own) {
@@ -462,7 +516,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         if (THREED) sum = sum + g.axy * (zs(5 + q) - zs(q));
         ft[q] = POW2 ? -sum * dt * g.ivol : cdiv(-sum * dt, g.vol, g.ivol);
       }
-      Cons c0 = load_cons(a.X, PS, g, gx, gy, z);
+      Cons c0 = load_cons<CG>(a.X, PS, g, gx, gy, z);
       double go1 = 0.0, go2 = 0.0, go3 = 0.0;  // the own cell's acceleration
       if (GRAV) {
         load_g(a.G, PS, g, gx, gy, z, go1, go2, go3);
@@ -470,7 +524,9 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         apply_sources(c0, nsrc - 1, g.small_eps);
         gravity_source0(c0, go1, go2, go3, dth, g.small_eps, v1, v2, v3);
       } else {
-        apply_sources(c0, nsrc, g.small_eps);
+        const SharedDiv q0(c0.d);
+        for (int k = 0; k < nsrc; ++k)
+          c0.E = source_energy_q(q0, c0.m1, c0.m2, c0.m3, c0.E, g.small_eps);
       }
       double n[5];
       if (STAGE == 0) {
@@ -480,7 +536,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         n[3] = c0.m3 + ft[3];
         n[4] = c0.E + ft[4];
       } else {
-        const Cons c1 = load_cons(a.Y, PS, g, gx, gy, z);
+        const Cons c1 = load_cons<CG>(a.Y, PS, g, gx, gy, z);
         n[0] = kHalf * (c0.d + c1.d + ft[0]);
         n[1] = kHalf * (c0.m1 + c1.m1 + ft[1]);
         n[2] = kHalf * (c0.m2 + c1.m2 + ft[2]);
@@ -493,7 +549,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         flags |= kFlagNonFinite;
       if (STAGE == 1) {
         // state/velocity after flux(1) and after source(1) (main.f90:372-380,490-515)
-        const double u1 = n[1] / n[0], u2 = n[2] / n[0], u3 = n[3] / n[0];
+        const SharedDiv qn(n[0]);
+        const double u1 = qn(n[1]), u2 = qn(n[2]), u3 = qn(n[3]);
         if (n[0] < kLowRho) flags |= kFlagLowRho;
         if (fabs(u1) > g.vlimit || fabs(u2) > g.vlimit || fabs(u3) > g.vlimit)
           flags |= kFlagVlimit;
@@ -520,10 +577,10 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
           if (!(r0 >= 0.0)) flags |= kFlagNonFinite;
         } else {
           // source(1) energy, then the Courant rate of the next step (courant.f90:20-22)
-          const double E3 = source_energy(n[0], n[1], n[2], n[3], n[4], g.small_eps);
+          const double E3 = source_energy_q(qn, n[1], n[2], n[3], n[4], g.small_eps);
           const double pA = eos_pressure(n[0], E3, u1, u2, u3, g.gm1, g.small_eps);
-          const double r0 = courant_rate<POW2>(n[0], pA, g.gam, u1, u2, u3, g.dx, g.dy, g.dz,
-                                               g.idx, g.idy, g.idz);
+          const double r0 = courant_rate_q<POW2>(qn, pA, g.gam, u1, u2, u3, g.dx, g.dy, g.dz,
+                                                 g.idx, g.idy, g.idz);
           rate = fmax(rate, r0);
           if (!(r0 >= 0.0)) flags |= kFlagNonFinite;
         }
@@ -575,18 +632,263 @@ __global__ void __launch_bounds__(NT, 65536 / (NT * 128)) k_stage(StageArgs a) {
   __syncthreads();
   Ctrl* C = a.ctrl + t.box;
   if (!C->active) return;
+  const double dt = C->dt;
+  const int nsrc = a.nsrc > 0 ? a.nsrc : C->nsrc;
   const bool full = (t.x0 + TX <= sg.ax1 - sg.ax0) && (t.y0 + TY <= sg.ay1 - sg.ay0);
   if (PM == 1) {
     if (full)
-      stage_tile<STAGE, true, THREED, true, GRAV>(a, t, sg, C, sm, red_rate, red_flags);
+      stage_tile<STAGE, true, THREED, true, GRAV>(a, t, sg, C, dt, nsrc, sm, red_rate, red_flags);
     else
-      stage_tile<STAGE, true, THREED, false, GRAV>(a, t, sg, C, sm, red_rate, red_flags);
+      stage_tile<STAGE, true, THREED, false, GRAV>(a, t, sg, C, dt, nsrc, sm, red_rate, red_flags);
   } else {
     if (full)
-      stage_tile<STAGE, false, THREED, true, GRAV>(a, t, sg, C, sm, red_rate, red_flags);
+      stage_tile<STAGE, false, THREED, true, GRAV>(a, t, sg, C, dt, nsrc, sm, red_rate, red_flags);
     else
-      stage_tile<STAGE, false, THREED, false, GRAV>(a, t, sg, C, sm, red_rate, red_flags);
+      stage_tile<STAGE, false, THREED, false, GRAV>(a, t, sg, C, dt, nsrc, sm, red_rate,
+                                                    red_flags);
   }
+}
+
+// A batched box's clock at the start of a step (dt control of main.f90:266-281
+// and 342, with the clock saved for a trip) and at its end (main.f90:471,544-545,
+// or the trip of a box whose step raised a guard: its planes then keep the
+// step's input and its clock is put back)
+__device__ __forceinline__ void box_begin_step(Ctrl& c) {
+  c.run_step += 1;
+  if (c.tripped || !(c.time < c.endtime) || c.step >= 1000000 || c.step >= c.max_step) {
+    c.active = 0;
+    return;
+  }
+  c.time0 = c.time;
+  c.dtold0 = c.dtold;
+  c.step0 = c.step;
+  c.rate_bits0 = c.rate_bits;
+  c.step = c.step + 1;
+  const double rate = __longlong_as_double((long long)c.rate_bits);
+  c.rate = rate;
+  c.rate_bits = 0ull;
+  double dt = c.cfl / rate;
+  dt = dt * 1.0;
+  if (c.step > 1 && c.dtold > 0.0) dt = fmin(dt, c.dtold * 1.1);
+  c.dtold = dt;
+  if (dt + c.time > c.endtime) dt = c.endtime - c.time;
+  dt = dt * kHalf;
+  dt = dt * 2.0;
+  c.dt = dt;
+  c.active = 1;
+}
+__device__ __forceinline__ void box_end_step(Ctrl& c) {
+  if (!c.active) return;
+  if (c.flags & (kFlagVlimit | kFlagLowRho | kFlagNonFinite)) {
+    c.tripped = 1;
+    c.trip_step = c.run_step - 1;
+    c.time = c.time0;
+    c.dtold = c.dtold0;
+    c.step = c.step0;
+    c.rate_bits = c.rate_bits0;
+    c.active = 0;
+    return;
+  }
+  double dt = kHalf * c.dt;
+  dt = dt * 2.0;
+  c.time = c.time + dt;
+  c.nsrc = 2;
+}
+namespace {
+__device__ __forceinline__ unsigned ld_acquire_u32(const unsigned* p) {
+  unsigned v;
+  asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+// polls *p until it reaches target; false after `limit` polls (~0.1 us apart)
+__device__ bool wait_at_least(const unsigned* p, unsigned target, long long limit) {
+  for (long long k = 0; k < limit; ++k) {
+    if (ld_acquire_u32(p) >= target) return true;
+    __nanosleep(100);
+  }
+  return false;
+}
+static_assert(sizeof(Ctrl) % 8 == 0, "Ctrl moves as 8-byte words");
+// a box's control block through L2 (other blocks of the launch write it)
+__device__ __forceinline__ Ctrl ctrl_load_cg(const Ctrl* p) {
+  Ctrl c;
+  const unsigned long long* s = reinterpret_cast<const unsigned long long*>(p);
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(&c);
+#pragma unroll
+  for (int k = 0; k < (int)(sizeof(Ctrl) / 8); ++k) d[k] = __ldcg(s + k);
+  return c;
+}
+__device__ __forceinline__ void ctrl_store_cg(Ctrl* p, const Ctrl& c) {
+  unsigned long long* d = reinterpret_cast<unsigned long long*>(p);
+  const unsigned long long* s = reinterpret_cast<const unsigned long long*>(&c);
+#pragma unroll
+  for (int k = 0; k < (int)(sizeof(Ctrl) / 8); ++k) __stcg(d + k, s[k]);
+}
+}  // namespace
+
+// one tile of one stage in the persistent kernel; not inlined, so each stage
+// and tile kind gets a register allocation of its own
+template <int STAGE, int PM, bool THREED, bool FULL>
+__device__ __noinline__ void persistent_tile_k(const StageArgs& a, const Tile& t, const Geom& g,
+                                               Ctrl* C, double dt, int nsrc, double* sm,
+                                               double* red_rate, unsigned* red_flags) {
+  stage_tile<STAGE, PM == 1, THREED, FULL, false, true>(a, t, g, C, dt, nsrc, sm, red_rate,
+                                                        red_flags);
+}
+template <int STAGE, int PM, bool THREED>
+__device__ __forceinline__ void persistent_tile(const StageArgs& a, const Tile& t, const Geom& g,
+                                                Ctrl* C, double dt, int nsrc, double* sm,
+                                                double* red_rate, unsigned* red_flags) {
+  if ((t.x0 + TX <= g.ax1 - g.ax0) && (t.y0 + TY <= g.ay1 - g.ay0))
+    persistent_tile_k<STAGE, PM, THREED, true>(a, t, g, C, dt, nsrc, sm, red_rate, red_flags);
+  else
+    persistent_tile_k<STAGE, PM, THREED, false>(a, t, g, C, dt, nsrc, sm, red_rate, red_flags);
+}
+
+template <int PM, bool THREED>
+__global__ void __launch_bounds__(NT, 65536 / (NT * 128)) k_batch_persistent(PersistArgs p) {
+  extern __shared__ double sm[];
+  __shared__ Geom sg;
+  __shared__ double red_rate[NT / 32];
+  __shared__ unsigned red_flags[NT / 32];
+  __shared__ long long s_item;
+  __shared__ int s_run, s_nsrc;
+  __shared__ double s_dt;
+  const long long nt = p.ntiles;
+  const long long total = 2 * nt * p.nsteps;
+  for (;;) {
+    if (threadIdx.x == 0) s_item = (long long)atomicAdd(p.head, 1ull);
+    __syncthreads();
+    const long long w = s_item;
+    if (w >= total) break;
+    const int step = (int)(w / (2 * nt));
+    const int stage = (int)((w / nt) % 2);
+    const Tile t = p.a.tiles[w % nt];
+    Ctrl* C = p.a.ctrl + t.box;
+    const unsigned ntb = (unsigned)p.tiles_of_box[t.box];
+    if (threadIdx.x == 0) {
+      sg = p.a.geom[t.box];
+      // a stage-0 tile needs its box's dt of the step; a stage-1 tile every
+      // stage-0 tile of its box (the halo of its stencil)
+      const bool ok = stage == 0
+                          ? wait_at_least(p.ready + t.box, (unsigned)step + 1u, p.poll_limit)
+                          : wait_at_least(p.done0 + t.box, ((unsigned)step + 1u) * ntb,
+                                          p.poll_limit);
+      if (!ok) atomicOr(p.status, 1);
+      __threadfence();
+      s_run = ok && __ldcg(&C->active);
+      s_dt = __ldcg(&C->dt);
+      s_nsrc = __ldcg(&C->nsrc);
+    }
+    __syncthreads();
+    if (s_run) {
+      const int X = (p.cur + 2 * step) % 3, Y = (X + 1) % 3, Z = (X + 2) % 3;
+      StageArgs a = p.a;
+      a.X = p.buf[X];
+      if (stage == 0) {
+        a.Y = nullptr;
+        a.out = p.buf[Y];
+        persistent_tile<0, PM, THREED>(a, t, sg, C, s_dt, s_nsrc, sm, red_rate, red_flags);
+      } else {
+        a.Y = p.buf[Y];
+        a.out = p.buf[Z];
+        persistent_tile<1, PM, THREED>(a, t, sg, C, s_dt, s_nsrc, sm, red_rate, red_flags);
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      // the block's writes (planes, the box's flags and Courant rate) before the count
+      __threadfence();
+      if (stage == 0) {
+        atomicAdd(p.done0 + t.box, 1u);
+      } else if (atomicAdd(p.done1 + t.box, 1u) + 1u == ((unsigned)step + 1u) * ntb) {
+        // the box's last stage-1 tile of the step: its clock advances
+        // (k_end_batch) and, unless the run ends here, the next dt is set
+        // (k_dt_batch); then the box's next step may start
+        __threadfence();
+        Ctrl c = ctrl_load_cg(C);
+        box_end_step(c);
+        if (step + 1 < p.nsteps) box_begin_step(c);
+        ctrl_store_cg(C, c);
+        __threadfence();
+        atomicExch(p.ready + t.box, (unsigned)step + 2u);
+      }
+    }
+  }
+}
+
+__global__ void k_persist_init(PersistArgs p, int nbox) {
+  const int b = blockIdx.x * blockDim.x + threadIdx.x;
+  if (b == 0) {
+    *p.head = 0ull;
+    *p.status = 0;
+  }
+  if (b >= nbox) return;
+  p.done0[b] = 0u;
+  p.done1[b] = 0u;
+  p.ready[b] = 1u;  // the first step's dt was set by k_dt_batch
+}
+
+__global__ void k_wait_selftest(unsigned* never, long long limit, int* status) {
+  if (!wait_at_least(never, 1u, limit)) atomicOr(status, 1);
+}
+
+template <int PM, bool THREED>
+static cudaError_t launch_persistent_t(const PersistArgs& p, int nbox, cudaStream_t s,
+                                       int* blocks_out) {
+  const size_t smem = SMEM_DOUBLES * sizeof(double);
+  const void* fn = (const void*)k_batch_persistent<PM, THREED>;
+  cudaError_t e = ensure_dyn_smem(fn, smem);
+  if (e != cudaSuccess) return e;
+  int dev = 0, sms = 0, per_sm = 0;
+  if ((e = cudaGetDevice(&dev)) != cudaSuccess) return e;
+  if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess)
+    return e;
+  if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, NT, smem)) != cudaSuccess)
+    return e;
+  const int blocks = std::max(1, per_sm) * sms;
+  k_persist_init<<<(nbox + 127) / 128, 128, 0, s>>>(p, nbox);
+  k_batch_persistent<PM, THREED><<<blocks, NT, smem, s>>>(p);
+  if (blocks_out) *blocks_out = blocks;
+  return cudaGetLastError();
+}
+
+cudaError_t launch_batch_persistent(const PersistArgs& p, int pm, bool threed, int nbox,
+                                    cudaStream_t s, int* blocks_out) {
+  if (pm == 1)
+    return threed ? launch_persistent_t<1, true>(p, nbox, s, blocks_out)
+                  : launch_persistent_t<1, false>(p, nbox, s, blocks_out);
+  return threed ? launch_persistent_t<0, true>(p, nbox, s, blocks_out)
+                : launch_persistent_t<0, false>(p, nbox, s, blocks_out);
+}
+
+cudaError_t persistent_wait_selftest(long long poll_limit, int* gave_up, float* ms) {
+  unsigned* never = nullptr;
+  int* status = nullptr;
+  cudaError_t e = cudaMalloc(&never, sizeof(unsigned));
+  if (e != cudaSuccess) return e;
+  if ((e = cudaMalloc(&status, sizeof(int))) != cudaSuccess) {
+    cudaFree(never);
+    return e;
+  }
+  cudaMemset(never, 0, sizeof(unsigned));
+  cudaMemset(status, 0, sizeof(int));
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  cudaEventRecord(e0);
+  k_wait_selftest<<<1, 1>>>(never, poll_limit, status);
+  cudaEventRecord(e1);
+  e = cudaEventSynchronize(e1);
+  if (e == cudaSuccess && ms) cudaEventElapsedTime(ms, e0, e1);
+  int h = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&h, status, sizeof(int), cudaMemcpyDeviceToHost);
+  if (gave_up) *gave_up = h;
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  cudaFree(never);
+  cudaFree(status);
+  return e;
 }
 
 template <int STAGE, int PM, bool THREED, bool GRAV>
@@ -666,49 +968,12 @@ __global__ void k_end(Ctrl* ctrl, int n) {
 __global__ void k_dt_batch(Ctrl* ctrl, int n) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n) return;
-  Ctrl& c = ctrl[b];
-  c.run_step += 1;
-  if (c.tripped || !(c.time < c.endtime) || c.step >= 1000000 || c.step >= c.max_step) {
-    c.active = 0;
-    return;
-  }
-  c.time0 = c.time;
-  c.dtold0 = c.dtold;
-  c.step0 = c.step;
-  c.rate_bits0 = c.rate_bits;
-  c.step = c.step + 1;
-  const double rate = __longlong_as_double((long long)c.rate_bits);
-  c.rate = rate;
-  c.rate_bits = 0ull;
-  double dt = c.cfl / rate;
-  dt = dt * 1.0;
-  if (c.step > 1 && c.dtold > 0.0) dt = fmin(dt, c.dtold * 1.1);
-  c.dtold = dt;
-  if (dt + c.time > c.endtime) dt = c.endtime - c.time;
-  dt = dt * kHalf;
-  dt = dt * 2.0;
-  c.dt = dt;
-  c.active = 1;
+  box_begin_step(ctrl[b]);
 }
 __global__ void k_end_batch(Ctrl* ctrl, int n) {
   const int b = blockIdx.x * blockDim.x + threadIdx.x;
   if (b >= n) return;
-  Ctrl& c = ctrl[b];
-  if (!c.active) return;
-  if (c.flags & (kFlagVlimit | kFlagLowRho | kFlagNonFinite)) {
-    c.tripped = 1;
-    c.trip_step = c.run_step - 1;
-    c.time = c.time0;
-    c.dtold = c.dtold0;
-    c.step = c.step0;
-    c.rate_bits = c.rate_bits0;
-    c.active = 0;
-    return;
-  }
-  double dt = kHalf * c.dt;
-  dt = dt * 2.0;
-  c.time = c.time + dt;
-  c.nsrc = 2;
+  box_end_step(ctrl[b]);
 }
 cudaError_t launch_dt_batch(Ctrl* ctrl, int nbox, cudaStream_t s) {
   k_dt_batch<<<(nbox + 127) / 128, 128, 0, s>>>(ctrl, nbox);

@@ -46,6 +46,62 @@ def test_batch_matches_single_grid_runs(graph):
     b.close()
 
 
+@pytest.mark.parametrize("graph", [True, False])
+def test_persistent_launch_matches_single_grid_runs(graph):
+    """One persistent launch per run (items taken from a queue, per-box waits):
+    every box as it would run alone, bit for bit, over two runs; three launches
+    per run."""
+    boxes = ensemble(14, seed=21, sides=(8, 12, 20, 13, 40))
+    b = Batch([st.params for st in boxes])
+    b.set_persistent(True)
+    assert b.persistent
+    for i, st in enumerate(boxes):
+        b.upload(i, st.cons)
+    b.run(6, graph=graph)
+    assert b.info()["launches"] == 3
+    b.run(5, graph=graph)
+    for i, st in enumerate(boxes):
+        (c0, u0, p0), clk0 = alone(st, 11)
+        c1, u1, p1 = b.download(i)
+        assert np.array_equal(c0, c1) and np.array_equal(u0, u1) and np.array_equal(p0, p1), i
+        clk1 = b.clock(i)
+        for k in ("time", "dt", "dtold", "step"):
+            assert clk0[k] == clk1[k], (i, k)
+    b.close()
+
+
+def test_persistent_launch_with_a_box_leaving_the_fused_path():
+    boxes = ensemble(6, seed=9)
+    boxes[2].params.vlimit = 0.6
+    boxes[2].params.validate()
+    b = Batch([s.params for s in boxes])
+    b.set_persistent(True)
+    for i, s in enumerate(boxes):
+        b.upload(i, s.cons)
+    b.run(7)
+    assert b.info()["solo_boxes"] >= 1
+    for i, s in enumerate(boxes):
+        (c0, u0, p0), clk0 = alone(s, 7)
+        c1, u1, p1 = b.download(i)
+        assert np.array_equal(c0, c1) and np.array_equal(u0, u1) and np.array_equal(p0, p1), i
+        assert b.clock(i)["step"] == clk0["step"] == 7
+    b.close()
+
+
+def test_persistent_wait_gives_up_at_its_poll_limit():
+    """The wait of the persistent launch on a counter nothing advances ends by
+    itself after its poll limit and reports it, with the device usable after."""
+    from boxzyhydro_b200.batch import wait_selftest
+    gave_up, ms = wait_selftest(2000)
+    assert gave_up and 0.0 < ms < 1000.0
+    boxes = ensemble(3, seed=2)
+    b = Batch([s.params for s in boxes])
+    for i, s in enumerate(boxes):
+        b.upload(i, s.cons)
+    b.run(2)
+    b.close()
+
+
 def test_batch_box_leaving_the_fused_path():
     boxes = ensemble(6, seed=9)
     # a box whose velocity limiter fires: |v| up to 1 against vlimit 0.6
