@@ -396,10 +396,13 @@ def batched_measure(args, rank, world, local, init_dist=True):
             b.upload(i, ic.riemann_box_cons(s["side"], s["axis"], s["left"], s["right"],
                                             s["gamma"]))
         b.run(args.warmup)
+        if args.persistent:
+            b.set_persistent(True)
         if not args.no_autotune:
             zc, tms = b.autotune(reps=2)
             tuned.append({"tile_depth": "whole box" if zc >= 1 << 30 else
-                          ("default rule" if zc == 0 else zc), "trial_ms_per_step": tms})
+                          ("default rule" if zc == 0 else zc), "trial_ms_per_step": tms,
+                          "launch_form": "persistent" if b.persistent else "4 per step"})
         b.run(args.steps)
         inf = b.info()
         total_ms += inf["last_run_ms"]
@@ -596,6 +599,32 @@ def adjoint_measure(args, local):
         fd = (vals[0] - vals[1]) * 0.5 / (2 * h)
         rel.append(abs(fd - adj) / max(abs(adj), 1e-300))
         del v
+    # the same differences with every branch held where the unperturbed run takes
+    # it (bx_adj_forward_branches): smooth, so they check the adjoint at the ties
+    # where the step is not differentiable
+    rel_fb = []
+    t_fb = time.perf_counter()
+    gen.manual_seed(args.seed + 99)
+    ob = torch.empty_like(c0)
+    for k in range(min(args.fd_dirs, args.fd_frozen_dirs)):
+        v = torch.randn(c0.shape, generator=gen, device=dev, dtype=torch.float64)
+        v.mul_(scale).mul_(m)
+        adj = float(torch.sum(grad * v))
+        vals = []
+        for sgn in (1.0, -1.0):
+            x = torch.add(c0, v, alpha=sgn * h)
+            op = torch.empty_like(c0)
+            torch.cuda.synchronize()
+            eng.forward_branches_ptr(c0.data_ptr(), x.data_ptr(), ob.data_ptr(), op.data_ptr())
+            torch.cuda.synchronize()
+            used()
+            vals.append(float(torch.sum((op[0] - target) ** 2 * m)))
+            del x, op
+        fd = (vals[0] - vals[1]) * 0.5 / (2 * h)
+        rel_fb.append(abs(fd - adj) / max(abs(adj), 1e-300))
+        del v
+    t_fb = time.perf_counter() - t_fb
+    del ob
     line = {
         "metric": "adjoint/forward time ratio", "value": ratio, "unit": "x",
         "higher_is_better": False, "n_gpus": 1, "steps": args.steps, "warmup": 0,
@@ -614,6 +643,13 @@ def adjoint_measure(args, local):
         "fd_check": {"directions": args.fd_dirs, "h": h, "max_rel_diff": max(rel) if rel else None,
                      "median_rel_diff": float(np.median(rel)) if rel else None,
                      "per_direction": rel},
+        "fd_frozen_branches": {
+            "directions": len(rel_fb), "h": h,
+            "max_rel_diff": max(rel_fb) if rel_fb else None,
+            "median_rel_diff": float(np.median(rel_fb)) if rel_fb else None,
+            "per_direction": rel_fb, "wall_s": t_fb,
+            "map": "bx_adj_forward_branches: the run from the perturbed state with the dt "
+                   "sequence and every branch of the unperturbed run"},
     }
     eng.close()
     return line
@@ -639,12 +675,16 @@ def main():
     ap.add_argument("--workload", default="turb", choices=["turb", "batched", "adjoint", "physics"])
     ap.add_argument("--snapshots", type=int, default=15)
     ap.add_argument("--fd-dirs", type=int, default=16, dest="fd_dirs")
+    ap.add_argument("--fd-frozen-dirs", type=int, default=16, dest="fd_frozen_dirs",
+                    help="of the finite-difference directions, those also taken with frozen branches")
     ap.add_argument("--adj-ic", default="blob", choices=["blob", "turb"], dest="adj_ic")
     ap.add_argument("--keep-stage0", action="store_true", dest="keep_stage0")
     ap.add_argument("--stage0-cache", type=int, default=0, dest="stage0_cache")
     ap.add_argument("--nbox", type=int, default=4096)
     ap.add_argument("--check-boxes", type=int, default=16, dest="check_boxes")
     ap.add_argument("--no-autotune", action="store_true", dest="no_autotune")
+    ap.add_argument("--persistent", action="store_true",
+                    help="batched: one persistent launch per run (the autotuner may still choose)")
     ap.add_argument("--loop-sample", type=int, default=8, dest="loop_sample")
     ap.add_argument("--parity-steps", type=int, default=3, dest="parity_steps",
                     help="steps of the full-size GPU-vs-oracle comparison (0: skip)")
@@ -861,7 +901,7 @@ def main():
         torch.cuda.empty_cache()
         a4 = _ap.Namespace(**vars(args))
         a4.n, a4.steps, a4.snapshots, a4.stage0_cache = 128, 200, 15, 8
-        a4.keep_stage0, a4.adj_ic, a4.fd_dirs = False, "blob", 16
+        a4.keep_stage0, a4.adj_ic, a4.fd_dirs, a4.fd_frozen_dirs = False, "blob", 16, 4
         try:
             adjoint_c4 = adjoint_measure(a4, local)
         except Exception as e:  # noqa: BLE001
@@ -869,7 +909,7 @@ def main():
         torch.cuda.empty_cache()
         a3 = _ap.Namespace(**vars(args))
         a3.nbox, a3.steps, a3.warmup, a3.check_boxes = 4096, 50, 3, 16
-        a3.no_autotune, a3.loop_sample = False, 8
+        a3.no_autotune, a3.loop_sample, a3.persistent = False, 8, False
         try:
             batched_c3 = batched_measure(a3, rank, world, local, init_dist=False)
         except Exception as e:  # noqa: BLE001

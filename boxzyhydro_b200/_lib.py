@@ -112,6 +112,9 @@ def lib():
         "bx_batch_get_clock": (C.c_int, [H, C.c_int32, dp, dp, dp, i64p]),
         "bx_batch_run": (C.c_int, [H, C.c_int64, C.c_double, C.c_int32]),
         "bx_batch_autotune": (C.c_int, [H, C.c_int32, i32p, dp]),
+        "bx_batch_set_persistent": (C.c_int, [H, C.c_int32]),
+        "bx_batch_get_persistent": (C.c_int, [H, i32p]),
+        "bx_batch_wait_selftest": (C.c_int, [C.c_int64, i32p, dp]),
         "bx_batch_download": (C.c_int, [H, C.c_int32, vp, vp, vp]),
         "bx_batch_info": (C.c_int, [H, dp, i64p, i32p, i64p]),
         "bx_batch_last_error": (C.c_char_p, [H]),
@@ -121,6 +124,7 @@ def lib():
         "bx_adj_keep_stage0": (C.c_int, [H, C.c_int32]),
         "bx_adj_stage0_cache": (C.c_int, [H, C.c_int32]),
         "bx_adj_forward": (C.c_int, [H, vp, vp, C.c_int32]),
+        "bx_adj_forward_branches": (C.c_int, [H, vp, vp, vp, vp]),
         "bx_adj_backward": (C.c_int, [H, vp, vp]),
         "bx_adj_stats": (C.c_int, [H, dp, dp, i64p, i64p]),
         "bx_adj_dts": (C.c_int, [H, dp]),

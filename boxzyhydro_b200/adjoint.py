@@ -61,6 +61,13 @@ class AdjointEngine:
         self._c(lib().bx_adj_forward(self._h, C.c_void_p(cons0_ptr), C.c_void_p(consT_ptr),
                                      1 if frozen else 0))
 
+    def forward_branches_ptr(self, base_ptr, pert_ptr, baseT_ptr, pertT_ptr):
+        """The last unfrozen forward run from a base and a perturbed initial state,
+        the perturbed run taking every branch the base run takes (dt sequence
+        held too): a smooth map whose central differences check the backward."""
+        self._c(lib().bx_adj_forward_branches(self._h, C.c_void_p(base_ptr), C.c_void_p(pert_ptr),
+                                              C.c_void_p(baseT_ptr), C.c_void_p(pertT_ptr)))
+
     def backward_ptr(self, lamT_ptr, lam0_ptr):
         self._c(lib().bx_adj_backward(self._h, C.c_void_p(lamT_ptr), C.c_void_p(lam0_ptr)))
 

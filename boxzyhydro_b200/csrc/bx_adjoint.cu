@@ -559,7 +559,13 @@ __global__ void k_rcell(Geom g, const double* SA, const double* SB, const double
   for (int q = 0; q < 5; ++q) { a[q] = gA[q]; a[5 + q] = gB[q]; }
   const bool edge = x == g.ax0 || x == g.ax1 - 1 || y == g.ay0 || y == g.ay1 - 1 ||
                     (g.threed && (z == g.az0 || z == g.az1 - 1));
-  if (edge) ghost_fold<STAGE>(g, SA, SB, P, PA, x, y, z, i, a);
+  if (edge) {
+    // the fold takes its array through memory; only the edge cells pay for that
+    double e[10];
+    for (int q = 0; q < 10; ++q) e[q] = a[q];
+    ghost_fold<STAGE>(g, SA, SB, P, PA, x, y, z, i, e);
+    for (int q = 0; q < 10; ++q) a[q] = e[q];
+  }
   if constexpr (STAGE == 1) {
     for (int q = 0; q < 5; ++q) {
       const double h = kHalf * li[q];
@@ -572,14 +578,15 @@ __global__ void k_rcell(Geom g, const double* SA, const double* SB, const double
     for (int q = 0; q < 5; ++q) l[q] = (li[q] + a[q]) + a[5 + q];
     if (nsrc > 0) {
       const double d = xs[0], m[3] = {xs[1], xs[2], xs[3]};
-      double Es[3];
-      Es[0] = xs[4];
-      for (int k = 0; k < nsrc; ++k)
-        Es[k + 1] = source_energy(d, m[0], m[1], m[2], Es[k], g.small_eps);
+      // the energies before each of the (at most two) sources, unrolled so they
+      // stay in registers
+      const double E0 = xs[4];
+      const double E1 = source_energy(d, m[0], m[1], m[2], E0, g.small_eps);
       const double K = kin_mom(d, m[0], m[1], m[2]);
-      for (int k = nsrc - 1; k >= 0; --k) {
+#pragma unroll
+      for (int k = 1; k >= 0; --k) {
         // E' = max(E - K, eps) + K
-        if (!(Es[k] - K > g.small_eps)) {
+        if (k < nsrc && !((k == 0 ? E0 : E1) - K > g.small_eps)) {
           const double gE = l[4];
           l[4] = 0.0;
           for (int j = 0; j < 3; ++j) l[1 + j] += gE * m[j] / d;
@@ -640,6 +647,291 @@ __global__ void k_set_clock(Ctrl* c, double dt, int active) {
   c->active = active;
 }
 __global__ void k_record_dt(const Ctrl* c, double* dts, long long k) { dts[k] = c->dt; }
+
+// ---- frozen-branch forward.  A base state and a perturbed state advance
+// together through the fused step (dt frozen at the recorded sequence); the
+// base values are the stage kernels' own, bit for bit (the same functions in
+// the same order; their fast divisions are exact), and every max, min, floor,
+// limiter selection and wave-speed choice of the perturbed state is the one the
+// base values make, by the reverse kernels' tie rules.  The perturbed run is
+// then a smooth function of its input near the base, whose derivative at the
+// base is what the adjoint transposes: central differences of it check the
+// adjoint where the step itself is not differentiable (ties of the limiter or
+// of the wave speeds in flat or symmetric regions).
+struct FB {  // one quantity of the base and the perturbed state
+  double b, p;
+};
+
+// the sources of one cell (source.f90:176-182 with zero force), nsrc times;
+// the floor max(E-K, eps) is taken where the base's E-K > eps says
+__device__ __forceinline__ void fb_sources(double db, double m1b, double m2b, double m3b,
+                                           double& Eb, double dp, double m1p, double m2p,
+                                           double m3p, double& Ep, int nsrc, double eps) {
+  const double Kb = kin_mom(db, m1b, m2b, m3b), Kp = kin_mom(dp, m1p, m2p, m3p);
+  for (int k = 0; k < nsrc; ++k) {
+    const bool act = Eb - Kb > eps;
+    Eb = fmax(Eb - Kb, eps) + Kb;
+    Ep = (act ? Ep - Kp : eps) + Kp;
+  }
+}
+
+// primitives of an interior cell for both states (load_prim of the stage kernels)
+template <int STAGE>
+__global__ void k_fb_prims(Geom g, const double* Xb, const double* Xp, const double* Ub,
+                           const double* Up, int nsrc, double* Pb, double* Pp, double* Uob,
+                           double* Uop) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= g.ng) return;
+  int x, y, z;
+  decode(g, i, x, y, z);
+  if (!ainterior(g, x, y, z)) return;
+  const long long n = g.ng;
+  double db = Xb[i], m1b = Xb[n + i], m2b = Xb[2 * n + i], m3b = Xb[3 * n + i], Eb = Xb[4 * n + i];
+  double dp = Xp[i], m1p = Xp[n + i], m2p = Xp[2 * n + i], m3p = Xp[3 * n + i], Ep = Xp[4 * n + i];
+  if (STAGE == 0) fb_sources(db, m1b, m2b, m3b, Eb, dp, m1p, m2p, m3p, Ep, nsrc, g.small_eps);
+  const double u1b = m1b / db, u2b = m2b / db, u3b = m3b / db;
+  const double u1p = m1p / dp, u2p = m2p / dp, u3p = m3p / dp;
+  // eps = max(E - rho K/2, small_eps), floor where the base's says
+  const double teb = Eb - kHalf * db * (u1b * u1b + u2b * u2b + u3b * u3b);
+  const double eb = fmax(teb, g.small_eps);
+  const double ep = teb > g.small_eps ? Ep - kHalf * dp * (u1p * u1p + u2p * u2p + u3p * u3p)
+                                      : g.small_eps;
+  double pb, pp;
+  if (STAGE == 0) {
+    pb = eb * g.gm1;
+    pp = ep * g.gm1;
+  } else {
+    // state() with the stage-0 velocity (stored by stage 0 of the pair)
+    const double s1b = Ub[i], s2b = Ub[n + i], s3b = Ub[2 * n + i];
+    const double s1p = Up[i], s2p = Up[n + i], s3p = Up[2 * n + i];
+    const double tpb = Eb - kin_rho_u(db, s1b, s2b, s3b);
+    pb = fmax(tpb, g.small_eps) * g.gm1;
+    pp = (tpb > g.small_eps ? Ep - kin_rho_u(dp, s1p, s2p, s3p) : g.small_eps) * g.gm1;
+  }
+  const double qb[7] = {db, u1b, u2b, u3b, pb, eb, sqrt(pb * g.gam / db)};
+  const double qp[7] = {dp, u1p, u2p, u3p, pp, ep, sqrt(pp * g.gam / dp)};
+  for (int q = 0; q < 7; ++q) {
+    Pb[q * n + i] = qb[q];
+    Pp[q * n + i] = qp[q];
+  }
+  if (STAGE == 0) {
+    Uob[i] = u1b; Uob[n + i] = u2b; Uob[2 * n + i] = u3b;
+    Uop[i] = u1p; Uop[n + i] = u2p; Uop[2 * n + i] = u3p;
+  }
+}
+
+// primitives of both states at (x,y,z) through the donor rule
+__device__ __forceinline__ void fb_prim(const Geom& g, const double* Pb, const double* Pp, int x,
+                                        int y, int z, Prim& qb, Prim& qp) {
+  long long c;
+  unsigned sg;
+  bool fx = false, fy = false, fz = false;
+  const int xx = amap(x, g.ax0, g.ax1, g.wall[0], g.wall[1], fx);
+  const int yy = amap(y, g.ay0, g.ay1, g.wall[2], g.wall[3], fy);
+  const int zz = g.threed ? amap(z, g.az0, g.az1, g.wall[4], g.wall[5], fz) : z;
+  c = xx + (long long)yy * g.sy + (long long)zz * g.sz;
+  sg = (fx ? 1u : 0u) | (fy ? 2u : 0u) | (fz ? 4u : 0u);
+  const long long n = g.ng;
+  qb = Prim{Pb[c], Pb[n + c], Pb[2 * n + c], Pb[3 * n + c], Pb[4 * n + c], Pb[5 * n + c],
+            Pb[6 * n + c]};
+  qp = Prim{Pp[c], Pp[n + c], Pp[2 * n + c], Pp[3 * n + c], Pp[4 * n + c], Pp[5 * n + c],
+            Pp[6 * n + c]};
+  if (sg & 1) { qb.u1 = -qb.u1; qp.u1 = -qp.u1; }
+  if (sg & 2) { qb.u2 = -qb.u2; qp.u2 = -qp.u2; }
+  if (sg & 4) { qb.u3 = -qb.u3; qp.u3 = -qp.u3; }
+}
+
+// the perturbed slope with the base's selection (slope_and_sel's rule)
+__device__ __forceinline__ double fb_slope(double c0b, double c1b, double c2b, double c0p,
+                                           double c1p, double c2p) {
+  int sel;
+  slope_and_sel(c0b, c1b, c2b, sel);
+  if (sel == 1) return kTheta * (c1p - c0p);
+  if (sel == 2) return kHalf * (c2p - c0p);
+  if (sel == 3) return kTheta * (c2p - c1p);
+  return 0.0;
+}
+
+// minus and plus states of the middle cell along DIR for both states
+template <int DIR>
+__device__ __forceinline__ void fb_dir_states(const Geom& g, const Prim* mb, const Prim* mp,
+                                              double dt, FaceState& mib, FaceState& plb,
+                                              FaceState& mip, FaceState& plp) {
+  const double ds = DIR == 0 ? g.dx : DIR == 1 ? g.dy : g.dz;
+  const double ids = DIR == 0 ? g.idx : DIR == 1 ? g.idy : g.idz;
+  const Prim &a = mb[0], &c = mb[1], &e = mb[2];
+  const double udb = DIR == 0 ? c.u1 : DIR == 1 ? c.u2 : c.u3;
+  // the base as the stage kernels' face states (dir_states; cdiv is exact,
+  // and equals the multiplication by the reciprocal for power-of-two spacings)
+  muscl_states<false>(c, udb, slope3(a.d, c.d, e.d), slope3(a.u1, c.u1, e.u1),
+                      slope3(a.u2, c.u2, e.u2), slope3(a.u3, c.u3, e.u3), slope3(a.p, c.p, e.p),
+                      slope3(a.e, c.e, e.e), dt, ds, ids, mib, plb);
+  const Prim &ap = mp[0], &cp = mp[1], &ep = mp[2];
+  const double udp = DIR == 0 ? cp.u1 : DIR == 1 ? cp.u2 : cp.u3;
+  const double sd = fb_slope(a.d, c.d, e.d, ap.d, cp.d, ep.d);
+  const double s1 = fb_slope(a.u1, c.u1, e.u1, ap.u1, cp.u1, ep.u1);
+  const double s2 = fb_slope(a.u2, c.u2, e.u2, ap.u2, cp.u2, ep.u2);
+  const double s3 = fb_slope(a.u3, c.u3, e.u3, ap.u3, cp.u3, ep.u3);
+  const double sp = fb_slope(a.p, c.p, e.p, ap.p, cp.p, ep.p);
+  const double se = fb_slope(a.e, c.e, e.e, ap.e, cp.e, ep.e);
+  // lambdas: max(u+c, 0) and min(u-c, 0) where the base's u+c > 0 and u-c < 0 say
+  const double lp = (udb + c.c > 0.0 ? udp + cp.c : 0.0) * dt / ds;
+  const double lm = (udb - c.c < 0.0 ? udp - cp.c : 0.0) * dt / ds;
+  const double hm = kHalf * (-1.0 - lm), hp = kHalf * (1.0 - lp);
+  mip = FaceState{cp.d + hm * sd, cp.u1 + hm * s1, cp.u2 + hm * s2, cp.u3 + hm * s3,
+                  cp.p + hm * sp, cp.e + hm * se};
+  plp = FaceState{cp.d + hp * sd, cp.u1 + hp * s1, cp.u2 + hp * s2, cp.u3 + hp * s3,
+                  cp.p + hp * sp, cp.e + hp * se};
+}
+
+// HLL flux of both states; the perturbed wave speeds take the base's choice
+// (hll_vjp's rule)
+template <int DIR>
+__device__ __forceinline__ void fb_hll(const FaceState& Lb, const FaceState& Rb,
+                                       const FaceState& Lp, const FaceState& Rp, double gam,
+                                       double Fb[5], double Fp[5]) {
+  hll_flux<DIR>(Lb, Rb, gam, Fb);
+  const double vlb = DIR == 0 ? Lb.u1 : DIR == 1 ? Lb.u2 : Lb.u3;
+  const double vrb = DIR == 0 ? Rb.u1 : DIR == 1 ? Rb.u2 : Rb.u3;
+  const double crb = sqrt(gam * Rb.p / Rb.d), clb = sqrt(gam * Lb.p / Lb.d);
+  const double a1 = vrb + crb, a2 = vlb + clb, b1 = -(vrb - crb), b2 = -(vlb - clb);
+  const int sap = (a2 > fmax(0.0, a1)) ? 2 : (a1 > 0.0 ? 1 : 0);
+  const int sam = (b2 > fmax(0.0, b1)) ? 2 : (b1 > 0.0 ? 1 : 0);
+  const double vl = DIR == 0 ? Lp.u1 : DIR == 1 ? Lp.u2 : Lp.u3;
+  const double vr = DIR == 0 ? Rp.u1 : DIR == 1 ? Rp.u2 : Rp.u3;
+  const double cr = sqrt(gam * Rp.p / Rp.d), cl = sqrt(gam * Lp.p / Lp.d);
+  const double ap = sap == 1 ? vr + cr : (sap == 2 ? vl + cl : 0.0);
+  const double am = sam == 1 ? -(vr - cr) : (sam == 2 ? -(vl - cl) : 0.0);
+  const double sl[5] = {Lp.d, Lp.d * Lp.u1, Lp.d * Lp.u2, Lp.d * Lp.u3,
+                        Lp.e + kHalf * Lp.d * (Lp.u1 * Lp.u1 + Lp.u2 * Lp.u2 + Lp.u3 * Lp.u3)};
+  const double sr[5] = {Rp.d, Rp.d * Rp.u1, Rp.d * Rp.u2, Rp.d * Rp.u3,
+                        Rp.e + kHalf * Rp.d * (Rp.u1 * Rp.u1 + Rp.u2 * Rp.u2 + Rp.u3 * Rp.u3)};
+  double fl[5], fr[5];
+  for (int k = 0; k < 5; ++k) {
+    fl[k] = sl[k] * vl;
+    fr[k] = sr[k] * vr;
+  }
+  fl[1 + DIR] += Lp.p;
+  fr[1 + DIR] += Rp.p;
+  fl[4] = (sl[4] + Lp.p) * vl;
+  fr[4] = (sr[4] + Rp.p) * vr;
+  for (int k = 0; k < 5; ++k) Fp[k] = (ap * fl[k] + am * fr[k] - ap * am * (sr[k] - sl[k])) / (ap + am);
+}
+
+// the flux of both states through the face between cells lo and lo+1 along DIR
+// (lo given by its coordinates); a cell outside the interior along DIR takes
+// ghost states (no slopes, flux.f90:53-54)
+template <int DIR>
+__device__ __forceinline__ void fb_face(const Geom& g, const double* Pb, const double* Pp,
+                                        int x, int y, int z, double dt, double Fb[5],
+                                        double Fp[5]) {
+  const int ex = DIR == 0, ey = DIR == 1, ez = DIR == 2;
+  FaceState Lb, Lp, Rb, Rp, t0, t1;
+  Prim mb[3], mp[3];
+  auto outside = [&](int cx, int cy, int cz) {
+    const int c = DIR == 0 ? cx : DIR == 1 ? cy : cz;
+    const int a0 = DIR == 0 ? g.ax0 : DIR == 1 ? g.ay0 : g.az0;
+    const int a1 = DIR == 0 ? g.ax1 : DIR == 1 ? g.ay1 : g.az1;
+    return c < a0 || c >= a1;
+  };
+  // plus state of the low cell
+  for (int k = 0; k < 3; ++k)
+    fb_prim(g, Pb, Pp, x + (k - 1) * ex, y + (k - 1) * ey, z + (k - 1) * ez, mb[k], mp[k]);
+  if (outside(x, y, z)) {
+    ghost_states(mb[1], t0, Lb);
+    ghost_states(mp[1], t1, Lp);
+  } else {
+    fb_dir_states<DIR>(g, mb, mp, dt, t0, Lb, t1, Lp);
+  }
+  // minus state of the high cell
+  const int hx = x + ex, hy = y + ey, hz = z + ez;
+  for (int k = 0; k < 3; ++k)
+    fb_prim(g, Pb, Pp, hx + (k - 1) * ex, hy + (k - 1) * ey, hz + (k - 1) * ez, mb[k], mp[k]);
+  if (outside(hx, hy, hz)) {
+    ghost_states(mb[1], Rb, t0);
+    ghost_states(mp[1], Rp, t1);
+  } else {
+    fb_dir_states<DIR>(g, mb, mp, dt, Rb, t0, Rp, t1);
+  }
+  fb_hll<DIR>(Lb, Rb, Lp, Rp, g.gam, Fb, Fp);
+}
+
+// the conservative update of an interior cell for both states (the epilogue of
+// the stage kernels: C1 = C0' + L(C0') or C2 = (C0' + C1 + L(C1))/2, floors)
+template <int STAGE>
+__global__ void k_fb_update(Geom g, const double* Pb, const double* Pp, const double* Xb,
+                            const double* Xp, const double* Yb, const double* Yp, int nsrc,
+                            double dt, double* Ob, double* Op) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= g.ng) return;
+  int x, y, z;
+  decode(g, i, x, y, z);
+  if (!ainterior(g, x, y, z)) return;
+  const long long n = g.ng;
+  double hb[5], hp[5], lb[5], lp[5], sb[5], sp[5];
+  fb_face<0>(g, Pb, Pp, x - 1, y, z, dt, lb, lp);
+  fb_face<0>(g, Pb, Pp, x, y, z, dt, hb, hp);
+  for (int q = 0; q < 5; ++q) { sb[q] = g.ayz * (hb[q] - lb[q]); sp[q] = g.ayz * (hp[q] - lp[q]); }
+  fb_face<1>(g, Pb, Pp, x, y - 1, z, dt, lb, lp);
+  fb_face<1>(g, Pb, Pp, x, y, z, dt, hb, hp);
+  for (int q = 0; q < 5; ++q) {
+    sb[q] = sb[q] + g.axz * (hb[q] - lb[q]);
+    sp[q] = sp[q] + g.axz * (hp[q] - lp[q]);
+  }
+  if (g.threed) {
+    fb_face<2>(g, Pb, Pp, x, y, z - 1, dt, lb, lp);
+    fb_face<2>(g, Pb, Pp, x, y, z, dt, hb, hp);
+    for (int q = 0; q < 5; ++q) {
+      sb[q] = sb[q] + g.axy * (hb[q] - lb[q]);
+      sp[q] = sp[q] + g.axy * (hp[q] - lp[q]);
+    }
+  }
+  double cb[5], cp[5], nb[5], np[5];
+  for (int q = 0; q < 5; ++q) { cb[q] = Xb[q * n + i]; cp[q] = Xp[q * n + i]; }
+  fb_sources(cb[0], cb[1], cb[2], cb[3], cb[4], cp[0], cp[1], cp[2], cp[3], cp[4], nsrc,
+             g.small_eps);
+  for (int q = 0; q < 5; ++q) {
+    const double fb = (-sb[q] * dt) / g.vol, fp = (-sp[q] * dt) / g.vol;
+    if (STAGE == 0) {
+      nb[q] = cb[q] + fb;
+      np[q] = cp[q] + fp;
+    } else {
+      nb[q] = kHalf * (cb[q] + Yb[q * n + i] + fb);
+      np[q] = kHalf * (cp[q] + Yp[q * n + i] + fp);
+    }
+  }
+  // floors (flux.f90:223-230) where the base's values put them
+  const bool dfl = !(nb[0] >= g.small_rho), efl = nb[4] < 0.0;
+  floors(nb[0], nb[1], nb[2], nb[3], nb[4], g.small_rho, g.small_eps);
+  if (dfl) np[0] = g.small_rho;
+  if (efl) np[4] = kin_mom(np[0], np[1], np[2], np[3]) + g.small_eps;
+  for (int q = 0; q < 5; ++q) {
+    Ob[q * n + i] = nb[q];
+    Op[q * n + i] = np[q];
+  }
+}
+
+// reference cons of interior cells at the end of the run: the planes plus the
+// source still pending (k_f2p_interior with nsrc 2), for both states
+__global__ void k_fb_finish(Geom g, const double* Xb, const double* Xp, double* Ob, double* Op) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= g.ng) return;
+  int x, y, z;
+  decode(g, i, x, y, z);
+  const long long n = g.ng;
+  if (!ainterior(g, x, y, z)) {
+    for (int q = 0; q < 5; ++q) Ob[q * n + i] = Op[q * n + i] = 0.0;
+    return;
+  }
+  double cb[5], cp[5];
+  for (int q = 0; q < 5; ++q) { cb[q] = Xb[q * n + i]; cp[q] = Xp[q * n + i]; }
+  fb_sources(cb[0], cb[1], cb[2], cb[3], cb[4], cp[0], cp[1], cp[2], cp[3], cp[4], 1,
+             g.small_eps);
+  for (int q = 0; q < 5; ++q) {
+    Ob[q * n + i] = cb[q];
+    Op[q * n + i] = cp[q];
+  }
+}
 
 }  // namespace
 
@@ -1347,6 +1639,37 @@ int bx_adj_device_bytes(const bx_params* params, int64_t nsteps, int32_t snapsho
   if (keep_stage0) d += (__int128)nsteps * 5 * n;
   d *= (__int128)sizeof(double);
   *bytes = d > (__int128)INT64_MAX ? INT64_MAX : (int64_t)d;
+  return BX_OK;
+}
+
+int bx_adj_forward_branches(bx_adj* A, const double* cons_base0, const double* cons_pert0,
+                            double* consT_base, double* consT_pert) {
+  if (!A || !cons_base0 || !cons_pert0 || !consT_base || !consT_pert)
+    return aerr(A, BX_ERR_ARG, "bad arguments");
+  if (!A->have_forward) return aerr(A, BX_ERR_STATE, "no recorded dt sequence");
+  bx_handle* h = A->h;
+  const Geom& g = h->g;
+  cudaStream_t s = h->stream;
+  const long long n = g.ng, n5 = 5 * n;
+  // scratch: the engine's work planes (a frozen forward uses them too); the
+  // snapshot pool, the stage-0 cache and the final state stay untouched
+  double *Xb = A->lamA, *Xp = A->lamB, *Yb = A->lamC1, *Yp = A->W0;
+  double *Ub = A->W1, *Up = A->W2, *Pb = A->P, *Pp = A->PA;
+  ACK(cudaMemcpyAsync(Xb, cons_base0, n5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  ACK(cudaMemcpyAsync(Xp, cons_pert0, n5 * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  for (long long k = 0; k < A->nsteps; ++k) {
+    const int nsrc = A->step_nsrc[k];
+    const double dt = A->dts[k];
+    k_fb_prims<0><<<ablk(n), AB, 0, s>>>(g, Xb, Xp, nullptr, nullptr, nsrc, Pb, Pp, Ub, Up);
+    k_fb_update<0><<<ablk(n), AB, 0, s>>>(g, Pb, Pp, Xb, Xp, nullptr, nullptr, nsrc, dt, Yb, Yp);
+    k_fb_prims<1><<<ablk(n), AB, 0, s>>>(g, Yb, Yp, Ub, Up, nsrc, Pb, Pp, nullptr, nullptr);
+    // in place: each cell reads only its own step input and stage-0 result
+    k_fb_update<1><<<ablk(n), AB, 0, s>>>(g, Pb, Pp, Xb, Xp, Yb, Yp, nsrc, dt, Xb, Xp);
+    ACK(cudaGetLastError());
+  }
+  k_fb_finish<<<ablk(n), AB, 0, s>>>(g, Xb, Xp, consT_base, consT_pert);
+  ACK(cudaGetLastError());
+  ACK(cudaStreamSynchronize(s));
   return BX_OK;
 }
 

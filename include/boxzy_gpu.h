@@ -248,14 +248,28 @@ int bx_batch_upload(bx_batch *b, int32_t box, const double *cons);
 int bx_batch_set_clock(bx_batch *b, int32_t box, double time, double dtold, int64_t step);
 int bx_batch_get_clock(bx_batch *b, int32_t box, double *time, double *dt, double *dtold,
                        int64_t *step);
-/* nsteps iterations of every box's main loop (boxes at endtime stop). */
+/* nsteps iterations of every box's main loop (boxes at endtime stop).  use_graph != 0:
+ * the run is captured once into a CUDA graph and replayed.  The launches are four per
+ * step (dt, stage 0, stage 1, clock), or, in persistent mode (bx_batch_set_persistent,
+ * or chosen by bx_batch_autotune), one launch for the whole run after the first
+ * step's dt: its blocks take (step, stage, tile) items from a queue in step order and
+ * wait for what an item reads (a stage-0 tile for its box's dt, a stage-1 tile for
+ * every stage-0 tile of its box), each wait bounded by a poll limit (BX_ERR_STATE
+ * if one gave up).  Both forms give the same results bit for bit. */
 int bx_batch_run(bx_batch *b, int64_t nsteps, double endtime, int32_t use_graph);
-/* Tile shape of the ensemble picked by measurement: every candidate tile depth
+int bx_batch_set_persistent(bx_batch *b, int32_t enable);
+int bx_batch_get_persistent(bx_batch *b, int32_t *enabled);
+/* The bounded wait of the persistent launch, run on a counter that nothing advances
+ * with the given poll limit: *gave_up = 1 when the wait ended without it (the limit
+ * ran out), *ms its device time.  A check of the limit that needs no fault. */
+int bx_batch_wait_selftest(int64_t poll_limit, int32_t *gave_up, double *ms);
+/* Run configuration of the ensemble picked by measurement: every candidate tile depth
  * (the default rule, whole box depths, 64, 32, 16, 8 planes) runs reps trial steps
  * from the boxes' current states, which the trials leave unchanged (inputs are
  * not overwritten; clocks are restored), and the fastest is kept for the following
- * runs.  *zc = the chosen depth (0 = default rule, >= 2^30 = whole depths), *ms =
- * its trial step time.  Results do not depend on the tiling. */
+ * runs; at that depth the persistent launch is timed too and kept if faster
+ * (bx_batch_get_persistent).  *zc = the chosen depth (0 = default rule, >= 2^30 =
+ * whole depths), *ms = its trial step time.  Results do not depend on either. */
 int bx_batch_autotune(bx_batch *b, int32_t reps, int32_t *zc, double *ms);
 int bx_batch_download(bx_batch *b, int32_t box, double *cons, double *u, double *p);
 /* device time of the last run (ms), kernels it launched, boxes running on their own
@@ -310,6 +324,17 @@ int bx_adj_plan(int64_t nsteps, int32_t snapshots, int64_t *recomputed_first,
 int bx_adj_device_bytes(const bx_params *params, int64_t nsteps, int32_t snapshots,
                         int32_t stage0_cache_entries, int32_t keep_stage0, int64_t *bytes);
 int bx_adj_dts(bx_adj *a, double *dts);
+/* The last unfrozen forward run, with its dt sequence, from two initial states at once
+ * (device SoA planes as for bx_adj_forward): a base state and a perturbed one.  Every
+ * max/min, floor, limiter selection and HLL wave-speed choice of the perturbed run is
+ * the one the base run makes (by the rules the backward pass differentiates), so the
+ * perturbed run is smooth in its input; central differences of it, with the base the
+ * unperturbed state, check bx_adj_backward where the step itself is not differentiable
+ * (limiter and wave-speed ties).  consT_base equals bx_adj_forward's consT on the
+ * interior cells bit for bit; ghost entries of both outputs are zero.  Uses the engine's
+ * work planes (like a frozen bx_adj_forward), not its snapshots. */
+int bx_adj_forward_branches(bx_adj *a, const double *cons_base0, const double *cons_pert0,
+                            double *consT_base, double *consT_pert);
 const char *bx_adj_last_error(bx_adj *a);
 
 /* No counterpart in the reference.  One set_ghost_cells sweep -- the same result as

@@ -84,6 +84,27 @@ def test_dot_product(walls, dims, dx):
     eng.close()
 
 
+def test_dot_product_32cubed_twenty_steps():
+    """The dot-product test on a 32^3-interior box over 20 steps with 5 snapshots
+    (the checkpoint schedule recomputes), 1e-12 relative."""
+    st, eng = setup((0,) * 6, (36, 36, 36), nsteps=20, snaps=5, dx=1.0 / 32)
+    hp = st.params
+    consT = fwd(eng, st.cons, frozen=False)
+    dts = eng.dts()
+    rng = np.random.default_rng(17)
+    v = rand_dir(hp, rng, np.array([1.0, 0.3, 0.3, 0.3, 2.0]))
+    cT, dT = TLM.run(hp, st.cons, v, dts)
+    m = interior_mask(hp)
+    assert np.allclose(cT[m], consT[m], rtol=1e-13, atol=0), "TLM forward differs from GPU"
+    lamT = rand_dir(hp, rng, np.ones(5))
+    lam0 = bwd(eng, lamT)
+    assert eng.stats()["recomputed_steps"] > 0
+    d1 = float(np.sum(lamT[m] * dT[m]))
+    d2 = float(np.sum(lam0[m] * v[m]))
+    assert abs(d1 - d2) <= 1e-12 * abs(d1), (d1, d2)
+    eng.close()
+
+
 def test_finite_differences_gpu_and_oracle():
     st, eng = setup()
     hp = st.params
@@ -118,6 +139,62 @@ def test_finite_differences_gpu_and_oracle():
             o.close()
         fdo = float(np.sum(lamT[m] * (vals[0][m] - vals[1][m]))) / (2 * h)
         assert abs(fdo - adj) <= 1e-6 * abs(adj), (fdo, adj)
+    eng.close()
+
+
+def fwd_branches(eng, base, pert):
+    torch = _torch()
+    b = torch.tensor(np.ascontiguousarray(base.T), device="cuda")
+    p = torch.tensor(np.ascontiguousarray(pert.T), device="cuda")
+    ob, op = torch.empty_like(b), torch.empty_like(p)
+    torch.cuda.synchronize()
+    eng.forward_branches_ptr(b.data_ptr(), p.data_ptr(), ob.data_ptr(), op.data_ptr())
+    return ob.cpu().numpy().T.copy(), op.cpu().numpy().T.copy()
+
+
+@pytest.mark.parametrize("walls,dims", [((0,) * 6, (20, 18, 16)), ((1, 1, 1, 1, 0, 0), (30, 12, 4))])
+def test_frozen_branch_differences_on_a_state_with_ties(walls, dims):
+    """A state with flat regions at rest (a split state plus a blob, like the
+    128^3 adjoint configuration): genminmod and the HLL wave speeds sit on ties
+    there, so central differences of the step itself do not converge.  With the
+    branches held where the base run takes them (bx_adj_forward_branches) they
+    match the adjoint to 1e-6.  The base of that run is bx_adj_forward's run bit
+    for bit, and a perturbed run from the base state is the base run."""
+    from boxzyhydro_b200 import ic
+    nx, ny, nz = dims
+    hp = small_random_box(nx=nx, ny=ny, nz=nz, walls=walls, cfl=0.4, dx=1.0 / 16).params
+    g = G.cell_centres(hp.nx, hp.ny, hp.nz, hp.dx, hp.dy, hp.dz)
+    x, y, z = g
+    rho = np.where(x < 0.0, 1.0, 0.125) * (1.0 + 0.05 * np.exp(-((x - 0.1) ** 2 + y ** 2 + z ** 2) / 0.01))
+    p = np.where(x < 0.0, 1.0, 0.1)
+    cons = np.zeros((hp.ngrid, 5))
+    cons[:, 0] = rho
+    cons[:, 4] = p / (hp.gammafix - 1.0)
+    from boxzyhydro_b200.hydro import apply_ghost_plan, ghost_plan
+    pl = ghost_plan(hp)
+    cons = apply_ghost_plan(cons, pl["src2"], pl["sgn2"], pl["dst"])
+    eng = AdjointEngine(hp, 6, 2)
+    consT = fwd(eng, cons, frozen=False)
+    m = interior_mask(hp)
+    ob, op = fwd_branches(eng, cons, cons)
+    assert np.array_equal(ob[m], consT[m]), "base run differs from the forward run"
+    assert np.array_equal(op[m], ob[m]), "perturbed run from the base state differs"
+    rng = np.random.default_rng(31)
+    lamT = np.zeros((hp.ngrid, 5))
+    lamT[m, 0] = rng.standard_normal(m.sum())
+    lam0 = bwd(eng, lamT)
+    h = 1e-7
+    free, frozen = [], []
+    for k in range(4):
+        v = rand_dir(hp, rng, np.array([1.0, 0.3, 0.3, 0.3, 2.0]))
+        adj = float(np.sum(lam0[m] * v[m]))
+        _, fp = fwd_branches(eng, cons, cons + h * v)
+        _, fm = fwd_branches(eng, cons, cons - h * v)
+        frozen.append(abs(float(np.sum(lamT[m] * (fp[m] - fm[m]))) / (2 * h) - adj) / abs(adj))
+        gp = fwd(eng, cons + h * v, frozen=True)
+        gm = fwd(eng, cons - h * v, frozen=True)
+        free.append(abs(float(np.sum(lamT[m] * (gp[m] - gm[m]))) / (2 * h) - adj) / abs(adj))
+    assert max(frozen) <= 1e-6, (frozen, free)
     eng.close()
 
 
