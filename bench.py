@@ -788,7 +788,10 @@ def main():
             ach = flops / (tdom * 1e-3) / 1e12
             fp64 = {"bound": "fp64", "achieved": ach, "peak": peak64, "unit": "TFLOP/s",
                     "frac": ach / peak64, "peak_source": "measured DFMA probe (bx_fp64_peak)",
-                    "flops_source": "ncu executed FP64 instructions per launch"}
+                    "flops_source": "FP64 operations of the method per cell, frozen from ncu "
+                                    "(every division and square root at its IEEE instruction "
+                                    "cost; profiles/stage_flops.json)",
+                    "executed_fp64_flops_per_cell": fl.get("executed_now", {}).get(f"stage{dom}")}
         else:
             fp64 = {"bound": "fp64", "peak": peak64, "unit": "TFLOP/s"}
     except Exception as e:  # noqa: BLE001

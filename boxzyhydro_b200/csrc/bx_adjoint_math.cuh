@@ -13,6 +13,18 @@ struct FS6 {  // a face state or its adjoint: rho, u1, u2, u3, p, eps
 
 __device__ __forceinline__ FS6 fs_zero() { return FS6{0, 0, 0, 0, 0, 0}; }
 
+// 1/x for the derivative terms (which need not round like the forward): the
+// hardware's approximate reciprocal refined by two Newton steps,
+// y <- y + y (1 - x y), each squaring the relative error; within a few ulps,
+// with no branch.  Not for values the forward's branches depend on.
+__device__ __forceinline__ double rcp_deriv(double x) {
+  double y;
+  asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+  y = fma(y, fma(-x, y, 1.0), y);
+  y = fma(y, fma(-x, y, 1.0), y);
+  return y;
+}
+
 // --- HLL flux (flux.f90:504-590): adjoints of the two face states from gF.
 template <int DIR>
 __device__ __forceinline__ void hll_vjp(const FaceState& L, const FaceState& R, double gam,
@@ -45,7 +57,7 @@ __device__ __forceinline__ void hll_vjp(const FaceState& L, const FaceState& R, 
   const double t2 = fmax(0.0, b1);
   const double am = fmax(t2, b2);
   const int sam = (b2 > t2) ? 2 : (b1 > 0.0 ? 1 : 0);
-  const double iD = 1.0 / (ap + am);
+  const double iD = rcp_deriv(ap + am);
   const double apm = ap * am;
   double gN[5], gD = 0.0, gap = 0.0, gam_ = 0.0;
   for (int k = 0; k < 5; ++k) {
@@ -74,8 +86,16 @@ __device__ __forceinline__ void hll_vjp(const FaceState& L, const FaceState& R, 
   double gpl = 0, gpr = 0, gdl = 0, gdr = 0, gel = 0, ger = 0;
   double gul[3] = {0, 0, 0}, gur[3] = {0, 0, 0};
   // c = sqrt(gam p / d): dc/dp = c/(2p) = gam/(2 d c), dc/dd = -c/(2d) = -c^2/(2 d c)
-  if (cl > 0.0) { const double t = kHalf * gcl / (dl * cl); gpl += gam * t; gdl -= cl * cl * t; }
-  if (cr > 0.0) { const double t = kHalf * gcr / (dr * cr); gpr += gam * t; gdr -= cr * cr * t; }
+  if (cl > 0.0) {
+    const double t = kHalf * gcl * rcp_deriv(dl * cl);
+    gpl += gam * t;
+    gdl -= cl * cl * t;
+  }
+  if (cr > 0.0) {
+    const double t = kHalf * gcr * rcp_deriv(dr * cr);
+    gpr += gam * t;
+    gdr -= cr * cr * t;
+  }
   // fluxes: f0 = d v, f(1+j) = [j == DIR] p + s(1+j) v, f4 = (s4 + p) v
   gdl = fma(gfl[0], vl, gdl); gvl = fma(gfl[0], sl[0], gvl);
   gdr = fma(gfr[0], vr, gdr); gvr = fma(gfr[0], sr[0], gvr);

@@ -168,14 +168,64 @@ __device__ __forceinline__ Raw load_raw(const StageArgs& a, const Geom& g, int x
   return r;
 }
 
-// Every division here is by the cell's density (the sources leave it alone):
-// one correctly rounded reciprocal serves them all (SharedDiv, exact).
+// Primitives of a cell without a force (stage 0 with the nsrc pending sources,
+// or stage 1 with the stale velocity v), every division by the cell's density
+// (the sources leave it alone) through one correctly rounded reciprocal and the
+// residual correction (exact).  The corrections are valid while the numerators'
+// exponents lie in their window; one check of all of them at the end, rather
+// than a branch per division, and false sends the caller to prim_ieee.
+template <int STAGE>
+__device__ __forceinline__ bool prim_fast(const Geom& g, const Cons& c, double v1, double v2,
+                                          double v3, int nsrc, bool need_c, Prim& q) {
+  const double d = c.d;
+  bool ok = d >= 0x1p-450 && d <= 0x1p+450;
+  const double r = ok ? __drcp_rn(d) : 1.0;
+  double E = c.E;
+  if (STAGE == 0) {
+    // source(): E = max(E - K, eps) + K with K = half*|m|^2/rho, the same K each time
+    const double kn = kHalf * (c.m1 * c.m1 + c.m2 * c.m2 + c.m3 * c.m3);
+    ok = ok && quot_fast_ok(kn);
+    const double ek = quot_fast(kn, d, r);
+    for (int k = 0; k < nsrc; ++k) E = fmax(E - ek, g.small_eps) + ek;
+  }
+  ok = ok && quot_fast_ok(c.m1) && quot_fast_ok(c.m2) && quot_fast_ok(c.m3);
+  q.d = d;
+  q.u1 = quot_fast(c.m1, d, r);
+  q.u2 = quot_fast(c.m2, d, r);
+  q.u3 = quot_fast(c.m3, d, r);
+  q.e = recon_eps(d, E, q.u1, q.u2, q.u3, g.small_eps);
+  q.p = STAGE == 0 ? q.e * g.gm1 : eos_pressure(d, E, v1, v2, v3, g.gm1, g.small_eps);
+  q.c = 0.0;
+  if (need_c) {
+    const double pn = q.p * g.gam;
+    ok = ok && quot_fast_ok(pn);
+    q.c = sqrt(quot_fast(pn, d, r));
+  }
+  return ok;
+}
+
+// the same with IEEE divisions (taken only outside the window)
+template <int STAGE>
+__device__ __forceinline__ Prim prim_ieee(double small_eps, double gm1, double gam, Cons c, double v1,
+                                       double v2, double v3, int nsrc, bool need_c) {
+  Prim q;
+  if (STAGE == 0) apply_sources(c, nsrc, small_eps);
+  q.d = c.d;
+  q.u1 = c.m1 / c.d;
+  q.u2 = c.m2 / c.d;
+  q.u3 = c.m3 / c.d;
+  q.e = recon_eps(q.d, c.E, q.u1, q.u2, q.u3, small_eps);
+  q.p = STAGE == 0 ? q.e * gm1 : eos_pressure(q.d, c.E, v1, v2, v3, gm1, small_eps);
+  q.c = need_c ? sqrt(q.p * gam / q.d) : 0.0;
+  return q;
+}
+
 template <int STAGE, bool GRAV = false>
 __device__ __forceinline__ Prim prim_of(const Geom& g, Raw r, unsigned& flags, int nsrc,
                                         double dth, bool need_c = true) {
   Prim q;
-  const SharedDiv qd(r.c.d);
   if (STAGE == 0 && GRAV) {
+    const SharedDiv qd(r.c.d);
     Cons c = r.c;
     double v1, v2, v3;
     apply_sources(c, nsrc - 1, g.small_eps);
@@ -186,26 +236,11 @@ __device__ __forceinline__ Prim prim_of(const Geom& g, Raw r, unsigned& flags, i
     q.u3 = qd(c.m3);
     q.e = recon_eps(q.d, c.E, q.u1, q.u2, q.u3, g.small_eps);
     q.p = eos_pressure(q.d, c.E, v1, v2, v3, g.gm1, g.small_eps);
-  } else if (STAGE == 0) {
-    Cons c = r.c;
-    for (int k = 0; k < nsrc; ++k) c.E = source_energy_q(qd, c.m1, c.m2, c.m3, c.E, g.small_eps);
-    q.d = c.d;
-    q.u1 = qd(c.m1);
-    q.u2 = qd(c.m2);
-    q.u3 = qd(c.m3);
-    q.e = recon_eps(q.d, c.E, q.u1, q.u2, q.u3, g.small_eps);
-    q.p = q.e * g.gm1;
-  } else {
-    const Cons c1 = r.c;
-    q.d = c1.d;
-    q.u1 = qd(c1.m1);
-    q.u2 = qd(c1.m2);
-    q.u3 = qd(c1.m3);
-    q.e = recon_eps(q.d, c1.E, q.u1, q.u2, q.u3, g.small_eps);
-    q.p = eos_pressure(q.d, c1.E, r.v1, r.v2, r.v3, g.gm1, g.small_eps);
+    // the sound speed enters only the lambdas of cells whose face states are built
+    q.c = need_c ? sqrt(qd(q.p * g.gam)) : 0.0;
+  } else if (!prim_fast<STAGE>(g, r.c, r.v1, r.v2, r.v3, nsrc, need_c, q)) {
+    q = prim_ieee<STAGE>(g.small_eps, g.gm1, g.gam, r.c, r.v1, r.v2, r.v3, nsrc, need_c);
   }
-  // the sound speed enters only the lambdas of cells whose face states are built
-  q.c = need_c ? sqrt(qd(q.p * g.gam)) : 0.0;
   if (q.d < kLowRho) flags |= kFlagLowRho;
   if (fabs(q.u1) > g.vlimit || fabs(q.u2) > g.vlimit || fabs(q.u3) > g.vlimit)
     flags |= kFlagVlimit;
@@ -305,6 +340,47 @@ __device__ __forceinline__ double warp_max(double v) {
 }
 
 }  // namespace
+
+// The end of stage 1 without a force, from the updated cell n: the velocity
+// after flux(1), then source(1)'s energy, state()'s pressure and the Courant
+// rate of the next step (courant.f90:20-22).  Every division is by n's density:
+// one correctly rounded reciprocal and the residual correction (exact) while
+// all numerators lie in the window, checked once; false sends the caller to
+// epi_ieee.
+template <bool POW2>
+__device__ __forceinline__ bool epi_fast(const Geom& g, const double n[5], double& u1, double& u2,
+                                         double& u3, double& r0) {
+  const double d = n[0];
+  const double kn = kHalf * (n[1] * n[1] + n[2] * n[2] + n[3] * n[3]);
+  bool ok = d >= 0x1p-450 && d <= 0x1p+450 && quot_fast_ok(n[1]) && quot_fast_ok(n[2]) &&
+            quot_fast_ok(n[3]) && quot_fast_ok(kn);
+  const double r = ok ? __drcp_rn(d) : 1.0;
+  u1 = quot_fast(n[1], d, r);
+  u2 = quot_fast(n[2], d, r);
+  u3 = quot_fast(n[3], d, r);
+  const double ek = quot_fast(kn, d, r);
+  const double E3 = fmax(n[4] - ek, g.small_eps) + ek;
+  const double pA = eos_pressure(d, E3, u1, u2, u3, g.gm1, g.small_eps);
+  const double pn = g.gam * pA;
+  ok = ok && quot_fast_ok(pn);
+  const double sound = sqrt(quot_fast(pn, d, r));
+  if (POW2)
+    r0 = (sound + fabs(u1)) * g.idx + (sound + fabs(u2)) * g.idy + (sound + fabs(u3)) * g.idz;
+  else
+    r0 = cdiv(sound + fabs(u1), g.dx, g.idx) + cdiv(sound + fabs(u2), g.dy, g.idy) +
+         cdiv(sound + fabs(u3), g.dz, g.idz);
+  return ok;
+}
+template <bool POW2>
+__device__ __forceinline__ void epi_ieee(const Geom& g, const double n[5], double& u1, double& u2,
+                                         double& u3, double& r0) {
+  u1 = n[1] / n[0];
+  u2 = n[2] / n[0];
+  u3 = n[3] / n[0];
+  const double E3 = source_energy(n[0], n[1], n[2], n[3], n[4], g.small_eps);
+  const double pA = eos_pressure(n[0], E3, u1, u2, u3, g.gm1, g.small_eps);
+  r0 = courant_rate<POW2>(n[0], pA, g.gam, u1, u2, u3, g.dx, g.dy, g.dz, g.idx, g.idy, g.idz);
+}
 
 // ------------------------------------------------------------------ stage kernel
 // One tile of one stage.  FULL: the tile is a whole TX x TY block of interior
@@ -548,9 +624,18 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
             isfinite(n[4])))
         flags |= kFlagNonFinite;
       if (STAGE == 1) {
-        // state/velocity after flux(1) and after source(1) (main.f90:372-380,490-515)
-        const SharedDiv qn(n[0]);
-        const double u1 = qn(n[1]), u2 = qn(n[2]), u3 = qn(n[3]);
+        // state/velocity after flux(1) and after source(1) (main.f90:372-380,490-515);
+        // without a force every division here is by the new density: one
+        // reciprocal and one window check for all of them (epi_fast)
+        double u1, u2, u3, r0 = 0.0;
+        if (GRAV) {
+          const SharedDiv qn(n[0]);
+          u1 = qn(n[1]);
+          u2 = qn(n[2]);
+          u3 = qn(n[3]);
+        } else if (!epi_fast<POW2>(g, n, u1, u2, u3, r0)) {
+          epi_ieee<POW2>(g, n, u1, u2, u3, r0);
+        }
         if (n[0] < kLowRho) flags |= kFlagLowRho;
         if (fabs(u1) > g.vlimit || fabs(u2) > g.vlimit || fabs(u3) > g.vlimit)
           flags |= kFlagVlimit;
@@ -576,11 +661,6 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
           rate = fmax(rate, r0);
           if (!(r0 >= 0.0)) flags |= kFlagNonFinite;
         } else {
-          // source(1) energy, then the Courant rate of the next step (courant.f90:20-22)
-          const double E3 = source_energy_q(qn, n[1], n[2], n[3], n[4], g.small_eps);
-          const double pA = eos_pressure(n[0], E3, u1, u2, u3, g.gm1, g.small_eps);
-          const double r0 = courant_rate_q<POW2>(qn, pA, g.gam, u1, u2, u3, g.dx, g.dy, g.dz,
-                                                 g.idx, g.idy, g.idz);
           rate = fmax(rate, r0);
           if (!(r0 >= 0.0)) flags |= kFlagNonFinite;
         }

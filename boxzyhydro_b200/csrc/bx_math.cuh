@@ -36,7 +36,18 @@ struct FaceState {
 BX_HD double slope3(double c0, double c1, double c2) {
   const double d1 = c1 - c0, d2 = c2 - c0, d3 = c2 - c1;
   const double x1 = kTheta * d1, x2 = kHalf * d2, x3 = kTheta * d3;
+#ifdef __CUDA_ARCH__
+  // the least magnitude on the bit images (with the sign cleared, non-negative
+  // doubles order like their 64-bit patterns; a NaN, whose pattern lies above
+  // infinity's, is passed over like fmin does)
+  const unsigned long long a1 = (unsigned long long)__double_as_longlong(x1) & 0x7fffffffffffffffull;
+  const unsigned long long a2 = (unsigned long long)__double_as_longlong(x2) & 0x7fffffffffffffffull;
+  const unsigned long long a3 = (unsigned long long)__double_as_longlong(x3) & 0x7fffffffffffffffull;
+  const unsigned long long am = a1 < a2 ? (a1 < a3 ? a1 : a3) : (a2 < a3 ? a2 : a3);
+  const double m = __longlong_as_double((long long)am);
+#else
   const double m = fmin(fabs(x1), fmin(fabs(x2), fabs(x3)));
+#endif
 #ifdef __CUDA_ARCH__
   // The same selection on the bit images, off the FP64 pipe: when d1 or d3 is
   // a zero, x1 or x3 is one and m = 0, the reference's +0; otherwise d1 and d3
@@ -199,6 +210,11 @@ __device__ __forceinline__ double quot_fast(double a, double d, double r) {
   return fma(e, r, q0);
 }
 
+// IEEE a/d out of line: the fallback of the shortened divisions below, taken
+// only outside their exponent window, so its code is not repeated at every
+// division of the stage kernels
+static __device__ __noinline__ double div_ieee(double a, double d) { return a / d; }
+
 // a/d for several numerators sharing one denominator d > 0.  With r the
 // correctly rounded reciprocal of d, q0 = RN(a*r) is within one ulp of a/d and
 // the residual a - d*q0 is exact under a fused multiply-add, so
@@ -218,7 +234,7 @@ struct SharedDiv {
   }
   __device__ __forceinline__ double operator()(double a) const {
     if (ok && quot_fast_ok(a)) return quot_fast(a, d, r);
-    return a / d;
+    return div_ieee(a, d);
   }
 };
 
@@ -307,8 +323,7 @@ BX_HD void hll_flux(const FaceState& L, const FaceState& R, double gam, double F
 #pragma unroll
     for (int i = 0; i < 5; ++i) F[i] = quot_fast(F[i], den, r);
   } else {
-#pragma unroll
-    for (int i = 0; i < 5; ++i) F[i] = F[i] / den;
+    for (int i = 0; i < 5; ++i) F[i] = div_ieee(F[i], den);
   }
 #else
   for (int i = 0; i < 5; ++i) F[i] = F[i] / den;
