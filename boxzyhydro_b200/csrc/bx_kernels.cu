@@ -154,11 +154,19 @@ struct Raw {
   double v1, v2, v3;
 };
 
+// STAGE 0 or 1: the stage is known at compile time; STAGE 2: it is the runtime
+// value rs (the persistent batched kernel runs both stages in one body)
+template <int STAGE>
+__device__ __forceinline__ bool stage_is0(int rs) {
+  return STAGE == 2 ? rs == 0 : STAGE == 0;
+}
+
 template <int STAGE, bool GRAV = false, bool CG = false>
-__device__ __forceinline__ Raw load_raw(const StageArgs& a, const Geom& g, int x, int y, int z) {
+__device__ __forceinline__ Raw load_raw(const StageArgs& a, const Geom& g, int x, int y, int z,
+                                        int rs = 0) {
   const long long PS = a.ncells_total;
   Raw r;
-  if (STAGE == 0) {
+  if (stage_is0<STAGE>(rs)) {
     r.c = load_cons<CG>(a.X, PS, g, x, y, z);
     if (GRAV) load_g(a.G, PS, g, x, y, z, r.v1, r.v2, r.v3);
   } else {
@@ -176,12 +184,13 @@ __device__ __forceinline__ Raw load_raw(const StageArgs& a, const Geom& g, int x
 // than a branch per division, and false sends the caller to prim_ieee.
 template <int STAGE>
 __device__ __forceinline__ bool prim_fast(const Geom& g, const Cons& c, double v1, double v2,
-                                          double v3, int nsrc, bool need_c, Prim& q) {
+                                          double v3, int nsrc, bool need_c, Prim& q, int rs = 0) {
+  const bool is0 = stage_is0<STAGE>(rs);
   const double d = c.d;
   bool ok = d >= 0x1p-450 && d <= 0x1p+450;
   const double r = ok ? __drcp_rn(d) : 1.0;
   double E = c.E;
-  if (STAGE == 0) {
+  if (is0) {
     // source(): E = max(E - K, eps) + K with K = half*|m|^2/rho, the same K each time
     const double kn = kHalf * (c.m1 * c.m1 + c.m2 * c.m2 + c.m3 * c.m3);
     ok = ok && quot_fast_ok(kn);
@@ -194,7 +203,7 @@ __device__ __forceinline__ bool prim_fast(const Geom& g, const Cons& c, double v
   q.u2 = quot_fast(c.m2, d, r);
   q.u3 = quot_fast(c.m3, d, r);
   q.e = recon_eps(d, E, q.u1, q.u2, q.u3, g.small_eps);
-  q.p = STAGE == 0 ? q.e * g.gm1 : eos_pressure(d, E, v1, v2, v3, g.gm1, g.small_eps);
+  q.p = is0 ? q.e * g.gm1 : eos_pressure(d, E, v1, v2, v3, g.gm1, g.small_eps);
   q.c = 0.0;
   if (need_c) {
     const double pn = q.p * g.gam;
@@ -207,22 +216,23 @@ __device__ __forceinline__ bool prim_fast(const Geom& g, const Cons& c, double v
 // the same with IEEE divisions (taken only outside the window)
 template <int STAGE>
 __device__ __forceinline__ Prim prim_ieee(double small_eps, double gm1, double gam, Cons c, double v1,
-                                       double v2, double v3, int nsrc, bool need_c) {
+                                       double v2, double v3, int nsrc, bool need_c, int rs = 0) {
   Prim q;
-  if (STAGE == 0) apply_sources(c, nsrc, small_eps);
+  const bool is0 = stage_is0<STAGE>(rs);
+  if (is0) apply_sources(c, nsrc, small_eps);
   q.d = c.d;
   q.u1 = c.m1 / c.d;
   q.u2 = c.m2 / c.d;
   q.u3 = c.m3 / c.d;
   q.e = recon_eps(q.d, c.E, q.u1, q.u2, q.u3, small_eps);
-  q.p = STAGE == 0 ? q.e * gm1 : eos_pressure(q.d, c.E, v1, v2, v3, gm1, small_eps);
+  q.p = is0 ? q.e * gm1 : eos_pressure(q.d, c.E, v1, v2, v3, gm1, small_eps);
   q.c = need_c ? sqrt(q.p * gam / q.d) : 0.0;
   return q;
 }
 
 template <int STAGE, bool GRAV = false>
 __device__ __forceinline__ Prim prim_of(const Geom& g, Raw r, unsigned& flags, int nsrc,
-                                        double dth, bool need_c = true) {
+                                        double dth, bool need_c = true, int rs = 0) {
   Prim q;
   if (STAGE == 0 && GRAV) {
     const SharedDiv qd(r.c.d);
@@ -238,8 +248,8 @@ __device__ __forceinline__ Prim prim_of(const Geom& g, Raw r, unsigned& flags, i
     q.p = eos_pressure(q.d, c.E, v1, v2, v3, g.gm1, g.small_eps);
     // the sound speed enters only the lambdas of cells whose face states are built
     q.c = need_c ? sqrt(qd(q.p * g.gam)) : 0.0;
-  } else if (!prim_fast<STAGE>(g, r.c, r.v1, r.v2, r.v3, nsrc, need_c, q)) {
-    q = prim_ieee<STAGE>(g.small_eps, g.gm1, g.gam, r.c, r.v1, r.v2, r.v3, nsrc, need_c);
+  } else if (!prim_fast<STAGE>(g, r.c, r.v1, r.v2, r.v3, nsrc, need_c, q, rs)) {
+    q = prim_ieee<STAGE>(g.small_eps, g.gm1, g.gam, r.c, r.v1, r.v2, r.v3, nsrc, need_c, rs);
   }
   if (q.d < kLowRho) flags |= kFlagLowRho;
   if (fabs(q.u1) > g.vlimit || fabs(q.u2) > g.vlimit || fabs(q.u3) > g.vlimit)
@@ -261,9 +271,9 @@ __device__ __forceinline__ Prim prim_of(const Geom& g, Raw r, unsigned& flags, i
 template <int STAGE, bool GRAV = false, bool CG = false>
 __device__ __forceinline__ Prim load_prim(const StageArgs& a, const Geom& g, int x, int y, int z,
                                           unsigned& flags, int nsrc, double dth,
-                                          bool need_c = true) {
-  return prim_of<STAGE, GRAV>(g, load_raw<STAGE, GRAV, CG>(a, g, x, y, z), flags, nsrc, dth,
-                              need_c);
+                                          bool need_c = true, int rs = 0) {
+  return prim_of<STAGE, GRAV>(g, load_raw<STAGE, GRAV, CG>(a, g, x, y, z, rs), flags, nsrc, dth,
+                              need_c, rs);
 }
 
 template <bool POW2>
@@ -391,7 +401,8 @@ __device__ __forceinline__ void epi_ieee(const Geom& g, const double n[5], doubl
 template <int STAGE, bool POW2, bool THREED, bool FULL, bool GRAV, bool CG = false>
 __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, const Geom& g,
                                            Ctrl* C, double dt, int nsrc, double* sm,
-                                           double* red_rate, unsigned* red_flags) {
+                                           double* red_rate, unsigned* red_flags, int rs = 0) {
+  const bool is0 = stage_is0<STAGE>(rs);
   double* SP = sm;                    // [7][TY+4][TX+4] primitives of the plane
   double* SX = sm + NR0;              // [12][TY][TX+2] x states (minus 0..5, plus 6..11)
   double* SY = SX + 12 * NSX;         // [12][TY+2][TX] y states
@@ -422,10 +433,10 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
 
   const int z0 = g.az0 + t.z0, z1 = g.az0 + t.z1;
   if (THREED && own) {
-    const Prim Pm2 = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z0 - 2, flags, nsrc, dth);
-    const Prim Pm1 = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z0 - 1, flags, nsrc, dth);
-    Pk = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z0, flags, nsrc, dth);
-    Pk1 = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z0 + 1, flags, nsrc, dth);
+    const Prim Pm2 = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z0 - 2, flags, nsrc, dth, true, rs);
+    const Prim Pm1 = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z0 - 1, flags, nsrc, dth, true, rs);
+    Pk = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z0, flags, nsrc, dth, true, rs);
+    Pk1 = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z0 + 1, flags, nsrc, dth, true, rs);
     FaceState mm, pm, m0;
     if (z0 - 1 < g.az0) {
       ghost_states(Pm1, mm, pm);
@@ -443,7 +454,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
 
   for (int z = (THREED ? z0 : g.az0 + t.z0); z < (THREED ? z1 : g.az0 + t.z1); ++z) {
     // ---- A: primitives of plane z (own from the pipeline, halo computed here)
-    if (STAGE == 1 && own) {
+    if (!is0 && own) {
       // the update at the end of this plane reads the step input of the own
       // cell, which nothing in this stage loaded before: start it towards L2
       const double* c = a.X + g.base + gx + (long long)gy * g.sy + (long long)z * g.sz;
@@ -462,12 +473,12 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
     FaceState mz1, pz1;
     if (own) {
       if (THREED) {
-        P2 = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z + 2, flags, nsrc, dth);
+        P2 = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z + 2, flags, nsrc, dth, true, rs);
       } else {
-        Pk = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z, flags, nsrc, dth);
+        Pk = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z, flags, nsrc, dth, true, rs);
       }
       put_prim(SP, (ty + 2) * PW + (tx + 2), Pk);
-      if (STAGE == 0) {
+      if (is0) {
         // sources change only E, so this is m/rho of the step input
         const long long o = g.base + gx + (long long)gy * g.sy + (long long)z * g.sz;
         a.U[o] = Pk.u1;
@@ -495,7 +506,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
       const int fx = bx0 + cx, fy = by0 + cy;
       const bool near = cx >= -1 && cx <= w && cy >= -1 && cy <= h;
       const bool inner = fx >= g.ax0 && fx < g.ax1 && fy >= g.ay0 && fy < g.ay1;
-      const Prim q = load_prim<STAGE, GRAV, CG>(a, g, fx, fy, z, flags, nsrc, dth, near && inner);
+      const Prim q = load_prim<STAGE, GRAV, CG>(a, g, fx, fy, z, flags, nsrc, dth, near && inner, rs);
       put_prim(SP, (cy + 2) * PW + (cx + 2), q);
     }
     if (THREED && own) {
@@ -605,7 +616,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
           c0.E = source_energy_q(q0, c0.m1, c0.m2, c0.m3, c0.E, g.small_eps);
       }
       double n[5];
-      if (STAGE == 0) {
+      if (is0) {
         n[0] = c0.d + ft[0];
         n[1] = c0.m1 + ft[1];
         n[2] = c0.m2 + ft[2];
@@ -623,7 +634,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
       if (!(isfinite(n[0]) && isfinite(n[1]) && isfinite(n[2]) && isfinite(n[3]) &&
             isfinite(n[4])))
         flags |= kFlagNonFinite;
-      if (STAGE == 1) {
+      if (!is0) {
         // state/velocity after flux(1) and after source(1) (main.f90:372-380,490-515);
         // without a force every division here is by the new density: one
         // reciprocal and one window check for all of them (epi_fast)
@@ -694,7 +705,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
       r = fmax(r, red_rate[k]);
     }
     if (f) atomicOr(&C->flags, f);
-    if (STAGE == 1) atomicMax(&C->rate_bits, (unsigned long long)__double_as_longlong(r));
+    if (!is0) atomicMax(&C->rate_bits, (unsigned long long)__double_as_longlong(r));
   }
 }
 
@@ -806,23 +817,16 @@ __device__ __forceinline__ void ctrl_store_cg(Ctrl* p, const Ctrl& c) {
 }
 }  // namespace
 
-// one tile of one stage in the persistent kernel; not inlined, so each stage
-// and tile kind gets a register allocation of its own
-template <int STAGE, int PM, bool THREED, bool FULL>
-__device__ __noinline__ void persistent_tile_k(const StageArgs& a, const Tile& t, const Geom& g,
-                                               Ctrl* C, double dt, int nsrc, double* sm,
-                                               double* red_rate, unsigned* red_flags) {
-  stage_tile<STAGE, PM == 1, THREED, FULL, false, true>(a, t, g, C, dt, nsrc, sm, red_rate,
-                                                        red_flags);
-}
-template <int STAGE, int PM, bool THREED>
-__device__ __forceinline__ void persistent_tile(const StageArgs& a, const Tile& t, const Geom& g,
-                                                Ctrl* C, double dt, int nsrc, double* sm,
-                                                double* red_rate, unsigned* red_flags) {
-  if ((t.x0 + TX <= g.ax1 - g.ax0) && (t.y0 + TY <= g.ay1 - g.ay0))
-    persistent_tile_k<STAGE, PM, THREED, true>(a, t, g, C, dt, nsrc, sm, red_rate, red_flags);
-  else
-    persistent_tile_k<STAGE, PM, THREED, false>(a, t, g, C, dt, nsrc, sm, red_rate, red_flags);
+// one tile of either stage in the persistent kernel: a single inlined body with
+// the stage as a runtime value (two bodies, or bodies called out of line, spill
+// registers) and the tile's extents at run time
+template <int PM, bool THREED>
+__device__ __forceinline__ void persistent_tile(int stage, const StageArgs& a, const Tile& t,
+                                                const Geom& g, Ctrl* C, double dt, int nsrc,
+                                                double* sm, double* red_rate,
+                                                unsigned* red_flags) {
+  stage_tile<2, PM == 1, THREED, false, false, true>(a, t, g, C, dt, nsrc, sm, red_rate,
+                                                     red_flags, stage);
 }
 
 template <int PM, bool THREED>
@@ -865,15 +869,9 @@ __global__ void __launch_bounds__(NT, 65536 / (NT * 128)) k_batch_persistent(Per
       const int X = (p.cur + 2 * step) % 3, Y = (X + 1) % 3, Z = (X + 2) % 3;
       StageArgs a = p.a;
       a.X = p.buf[X];
-      if (stage == 0) {
-        a.Y = nullptr;
-        a.out = p.buf[Y];
-        persistent_tile<0, PM, THREED>(a, t, sg, C, s_dt, s_nsrc, sm, red_rate, red_flags);
-      } else {
-        a.Y = p.buf[Y];
-        a.out = p.buf[Z];
-        persistent_tile<1, PM, THREED>(a, t, sg, C, s_dt, s_nsrc, sm, red_rate, red_flags);
-      }
+      a.Y = stage == 0 ? nullptr : p.buf[Y];
+      a.out = stage == 0 ? p.buf[Y] : p.buf[Z];
+      persistent_tile<PM, THREED>(stage, a, t, sg, C, s_dt, s_nsrc, sm, red_rate, red_flags);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
