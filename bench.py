@@ -400,8 +400,10 @@ def batched_measure(args, rank, world, local, init_dist=True):
             b.set_persistent(True)
         if not args.no_autotune:
             zc, tms = b.autotune(reps=2)
+            _, ttx, tty, _ = b.tile_shape
             tuned.append({"tile_depth": "whole box" if zc >= 1 << 30 else
                           ("default rule" if zc == 0 else zc), "trial_ms_per_step": tms,
+                          "tile_columns": f"{ttx}x{tty}",
                           "launch_form": "persistent" if b.persistent else "4 per step"})
         b.run(args.steps)
         inf = b.info()
@@ -426,11 +428,14 @@ def batched_measure(args, rank, world, local, init_dist=True):
     total_ms = max_over_ranks(total_ms, world, "cuda")
     value = weak_value(world, args.nbox, args.steps, total_ms)
 
-    # single-grid path looped over a stratified sample, extrapolated by size
+    # single-grid path looped over the whole ensemble (--loop-sample 0) or over a
+    # stratified sample, extrapolated by size
     sizes = sorted({s["side"] for s in spec})
     per_size_ms = {}
     for side in sizes:
-        sample = [s for s in spec if s["side"] == side][: args.loop_sample]
+        sample = [s for s in spec if s["side"] == side]
+        if args.loop_sample > 0:
+            sample = sample[: args.loop_sample]
         ms_list = []
         for s in sample:
             h = Hydro(ic.riemann_params(side, s["gamma"]))
@@ -447,6 +452,7 @@ def batched_measure(args, rank, world, local, init_dist=True):
             ms_list.append(e0.elapsed_time(e1))
             h.close()
         per_size_ms[side] = sum(ms_list) / len(ms_list)
+    # with the whole ensemble this sum is the measured loop time itself
     loop_ms = max_over_ranks(sum(per_size_ms[s["side"]] for s in spec), world, "cuda")
     loop_value = weak_value(world, args.nbox, args.steps, loop_ms)
     cells = sum(s["side"] ** 3 for s in spec)
@@ -463,7 +469,8 @@ def batched_measure(args, rank, world, local, init_dist=True):
                    "cell_updates_per_s": weak_value(world, cells, args.steps, total_ms)},
         "loop_single_grid": {"value": loop_value, "unit": "box-steps/s",
                              "ms_per_box_run_by_side": per_size_ms,
-                             "sample_per_side": args.loop_sample},
+                             "sample_per_side": args.loop_sample if args.loop_sample > 0
+                             else "all (every box of the ensemble run alone)"},
         "speedup_vs_loop": value / loop_value,
         "autotune": tuned or None,
         "parity": {"boxes_checked": checked, "max_rel_diff_cons": maxdiff,
@@ -483,6 +490,37 @@ def adjoint_arm(args, rank, world, local):
     line = adjoint_measure(args, local)
     print(json.dumps(line), flush=True)
     return 0
+
+
+def host_mem_available():
+    """MemAvailable of /proc/meminfo in bytes (0 if unreadable)."""
+    try:
+        with open("/proc/meminfo") as f:
+            for ln in f:
+                if ln.startswith("MemAvailable:"):
+                    return int(ln.split()[1]) * 1024
+    except OSError:
+        pass
+    return 0
+
+
+def auto_host_stride(steps, sets, set_bytes):
+    """Stride of the adjoint's host level for `sets` free device plane sets: a
+    segment of L steps takes L + 1 sets (two hold segment starts) and recomputes
+    L - 1 steps plus stage 0 of the steps the remaining sets (stage-0 cache
+    entries, at least 2) do not cover (about half a step each); the host keeps
+    (steps - 1) // L states in at most 45 % of its available memory and at
+    most 256 GiB (pinning takes time).  0 when no stride fits."""
+    cap = min(0.45 * host_mem_available(), float(256 << 30))
+    best, best_cost = 0, None
+    for L in range(2, max(2, sets - 4) + 1):
+        entries = sets - (L + 1)
+        if entries < 2 or ((steps - 1) // L) * set_bytes > cap:
+            continue
+        cost = ((L - 1) + 0.5 * max(1, L - entries)) / L
+        if best_cost is None or cost < best_cost - 1e-12:
+            best, best_cost = L, cost
+    return best
 
 
 def adjoint_measure(args, local):
@@ -533,6 +571,14 @@ def adjoint_measure(args, local):
         if args.stage0_cache <= 0 and not args.keep_stage0:
             entries = max(2, min(8, round(0.35 * sets)))
         snaps = int(max(1, min(args.steps, sets - entries)))
+        if args.host_stride < 0:
+            args.host_stride = auto_host_stride(args.steps, sets, 5 * plane)
+        if args.host_stride >= 2:
+            # host level: stride + 1 plane sets (two hold segment starts, the
+            # other stride - 1 take a segment's states), the rest cache entries
+            snaps = int(max(3, min(sets - 2, args.host_stride + 1)))
+            if args.stage0_cache <= 0 and not args.keep_stage0:
+                entries = int(max(2, sets - snaps))
     peak = [0]
 
     def used():
@@ -543,6 +589,12 @@ def adjoint_measure(args, local):
     eng.stage0_cache(entries)
     if args.keep_stage0:
         eng.keep_stage0(True)
+    host = None
+    if args.host_stride >= 2:
+        try:
+            host = {"stride": args.host_stride, "pinned_bytes": eng.host_level(args.host_stride)}
+        except Exception as e:  # refused (host memory): the device-only schedule runs
+            host = {"stride": args.host_stride, "refused": str(e)}
     stream = torch.cuda.Stream()
     eng.set_stream(stream.cuda_stream)
     used()
@@ -632,7 +684,7 @@ def adjoint_measure(args, local):
         "config": {"workload": f"discrete adjoint, {n}^3 interior, gamma=5/3, {ic_name}, "
                                f"{args.steps} steps, loss 0.5||rho(T)-rho_target||^2",
                    "snapshots": snaps, "keep_stage0": bool(args.keep_stage0),
-                   "stage0_cache_entries": entries},
+                   "stage0_cache_entries": entries, "host_level": host},
         "ms_forward": stats_fwd["ms_forward"], "ms_backward": stt["ms_backward"],
         "forward_cell_updates_per_s": hp.n_active() * args.steps / (stats_fwd["ms_forward"] * 1e-3),
         "recomputed_steps": stt["recomputed_steps"],
@@ -680,12 +732,17 @@ def main():
     ap.add_argument("--adj-ic", default="blob", choices=["blob", "turb"], dest="adj_ic")
     ap.add_argument("--keep-stage0", action="store_true", dest="keep_stage0")
     ap.add_argument("--stage0-cache", type=int, default=0, dest="stage0_cache")
+    ap.add_argument("--host-stride", type=int, default=0, dest="host_stride",
+                    help="adjoint: every stride-th state in pinned host memory (0: off; "
+                         "-1 with --snapshots 0: chosen from the free device and host memory)")
     ap.add_argument("--nbox", type=int, default=4096)
     ap.add_argument("--check-boxes", type=int, default=16, dest="check_boxes")
     ap.add_argument("--no-autotune", action="store_true", dest="no_autotune")
     ap.add_argument("--persistent", action="store_true",
                     help="batched: one persistent launch per run (the autotuner may still choose)")
-    ap.add_argument("--loop-sample", type=int, default=8, dest="loop_sample")
+    ap.add_argument("--loop-sample", type=int, default=8, dest="loop_sample",
+                    help="batched: boxes per side of the looped single-grid baseline "
+                         "(0: every box of the ensemble)")
     ap.add_argument("--parity-steps", type=int, default=3, dest="parity_steps",
                     help="steps of the full-size GPU-vs-oracle comparison (0: skip)")
     ap.add_argument("--no-extra", action="store_true", dest="no_extra",

@@ -113,6 +113,8 @@ def lib():
         "bx_batch_run": (C.c_int, [H, C.c_int64, C.c_double, C.c_int32]),
         "bx_batch_autotune": (C.c_int, [H, C.c_int32, i32p, dp]),
         "bx_batch_set_persistent": (C.c_int, [H, C.c_int32]),
+        "bx_batch_set_tile_shape": (C.c_int, [H, C.c_int32]),
+        "bx_batch_get_tile_shape": (C.c_int, [H, i32p, i32p, i32p, i32p]),
         "bx_batch_get_persistent": (C.c_int, [H, i32p]),
         "bx_batch_wait_selftest": (C.c_int, [C.c_int64, i32p, dp]),
         "bx_batch_download": (C.c_int, [H, C.c_int32, vp, vp, vp]),
@@ -123,6 +125,7 @@ def lib():
         "bx_adj_set_stream": (C.c_int, [H, vp]),
         "bx_adj_keep_stage0": (C.c_int, [H, C.c_int32]),
         "bx_adj_stage0_cache": (C.c_int, [H, C.c_int32]),
+        "bx_adj_host_level": (C.c_int, [H, C.c_int64, C.POINTER(C.c_int64)]),
         "bx_adj_forward": (C.c_int, [H, vp, vp, C.c_int32]),
         "bx_adj_forward_branches": (C.c_int, [H, vp, vp, vp, vp]),
         "bx_adj_backward": (C.c_int, [H, vp, vp]),

@@ -54,6 +54,14 @@ class AdjointEngine:
         """Entries of the backward pass's cache of stage-0 results (>= 2)."""
         self._c(lib().bx_adj_stage0_cache(self._h, int(entries)))
 
+    def host_level(self, stride):
+        """Copy every stride-th state of the next forward run to pinned host
+        memory and reverse the segments between them one by one (0: off).
+        Returns the pinned bytes."""
+        hb = C.c_int64()
+        self._c(lib().bx_adj_host_level(self._h, int(stride), C.byref(hb)))
+        return hb.value
+
     def set_stream(self, ptr):
         self._c(lib().bx_adj_set_stream(self._h, C.c_void_p(ptr) if ptr else None))
 

@@ -73,6 +73,17 @@ class Batch:
         launches per step; the same results."""
         self._c(lib().bx_batch_set_persistent(self._h, 1 if enable else 0))
 
+    def set_tile_shape(self, shape):
+        """0: 32 x 8 column tiles, 1: 16 x 16 (the same results)."""
+        self._c(lib().bx_batch_set_tile_shape(self._h, int(shape)))
+
+    @property
+    def tile_shape(self):
+        """(shape index, tx, ty, depth) of the stage kernels' tiles."""
+        v = [C.c_int32() for _ in range(4)]
+        self._c(lib().bx_batch_get_tile_shape(self._h, *[C.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
     @property
     def persistent(self):
         e = C.c_int32()
@@ -80,10 +91,11 @@ class Batch:
         return bool(e.value)
 
     def autotune(self, reps=2):
-        """Pick the ensemble's tile depth, then the launch form (four launches per
-        step or one persistent launch), by timing trial steps from the current
-        states (left unchanged): returns (depth, ms per step); depth 0 is the
-        default rule, >= 2**30 whole box depths; `persistent` tells the form."""
+        """Pick the ensemble's tile shape and depth, then the launch form (four
+        launches per step or one persistent launch), by timing trial steps from the
+        current states (left unchanged): returns (depth, ms per step); depth 0 is
+        the default rule, >= 2**30 whole box depths; `tile_shape` and `persistent`
+        tell the rest."""
         zc = C.c_int32()
         ms = C.c_double()
         self._c(lib().bx_batch_autotune(self._h, int(reps), C.byref(zc), C.byref(ms)))

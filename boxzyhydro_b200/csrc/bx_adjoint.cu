@@ -26,6 +26,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -1031,10 +1032,30 @@ struct bx_adj {
   // primitives and their adjoints (7 planes each); forward steps use the first
   // 3 planes of P for the stage-0 velocity
   double *P = nullptr, *PA = nullptr;
+  // optional host level of the schedule (bx_adj_host_level): the unfrozen
+  // forward copies the state of every hstride-th step into pinned host memory,
+  // and the backward reverses the segments between those steps one after
+  // another, last first, each with the device pool.  Pool slots snaps and
+  // snaps-1 hold segment starts: segment j's start in hold[j & 1] while the
+  // start of segment j-1 is copied into the other from the host.
+  long long hstride = 0;
+  std::vector<double*> hsnap;  // hsnap[j-1]: state of step j*hstride
+  size_t host_bytes = 0;
+  double* hold[2] = {nullptr, nullptr};
+  long long hold_step[2] = {-1, -1};  // step whose state hold[b] holds
+  cudaStream_t cstream = nullptr;     // host <-> device copies of the host level
+  cudaEvent_t cev[2] = {nullptr, nullptr};  // last copy into or out of hold[b] done
+  cudaEvent_t uev[2] = {nullptr, nullptr};  // the compute stream's use of hold[b] done
+  bool host_valid = false;
   double ms_fwd = 0.0, ms_bwd = 0.0;
   long long fwd_steps_in_bwd = 0;
   size_t bytes = 0;
   bool have_forward = false;
+  // the grid's two-sweep ghost plan leaves corner ghosts lagging (reflective
+  // 3-D boxes): they enter only the Courant maximum, so the fused stage
+  // arithmetic holds with the dt sequence of the per-phase kernels, which an
+  // unfrozen forward takes from a run of those first
+  bool dt_phase = false;
   int nsrc0 = 1;
   std::string err;
 };
@@ -1353,6 +1374,116 @@ static int reverse_range(bx_adj* A, const double* Xa, long long a, long long b, 
   return reverse_range(A, Xa, a, m, lam, false);
 }
 
+// The grids the adjoint takes: face ghosts on the stage kernels' donor rule
+// (the stencils read no others), fixed gamma, no flux_ang.  Their two-sweep
+// plan may leave corner ghosts lagging; those enter only the Courant maximum.
+static bool adjoint_grid(const bx_params& P, const GhostTable& T) {
+  return T.face_rule_ok && !(P.flags & BX_FLAG_PHASE_ONLY) && !P.fluxangmom && P.h2stat == -1;
+}
+
+// dt sequence of nsteps steps of the per-phase kernels (the reference data
+// flow, lagging corner ghosts included) from the planes X0, on a handle of its
+// own; into A->dts and A->d_dts
+static int phase_dts(bx_adj* A, const double* X0) {
+  bx_handle* h2 = nullptr;
+  if (int r = bx_create(&A->h->P, &h2)) return aerr(A, r, bx_last_error(nullptr));
+  struct Closer {
+    bx_handle* h;
+    ~Closer() { bx_destroy(h); }
+  } closer{h2};
+  if (int r = bx_set_stream(h2, A->h->stream)) return aerr(A, r, bx_last_error(h2));
+  if (int r = bx_handle_start_from_planes(h2, X0)) return aerr(A, r, bx_last_error(h2));
+  if (int r = bx_set_clock(h2, 0.0, 0.0, 0)) return aerr(A, r, bx_last_error(h2));
+  for (long long k = 0; k < A->nsteps; ++k) {
+    int32_t ran = 0;
+    if (int r = bx_step(h2, 1e300, &ran)) return aerr(A, r, bx_last_error(h2));
+    double t, dt, dtold;
+    int64_t step;
+    if (int r = bx_get_clock(h2, &t, &dt, &dtold, &step)) return aerr(A, r, bx_last_error(h2));
+    if (!ran) return aerr(A, BX_ERR_STATE, "the per-phase run stopped early");
+    A->dts[k] = dt;
+  }
+  uint32_t bits = 0;
+  int32_t path = 0;
+  bx_status(h2, &bits, &path);
+  if (bits & (kFlagVlimit | kFlagLowRho | kFlagNonFinite))
+    return aerr(A, BX_ERR_STATE,
+                "a guard fired in the forward run (velocity limiter, low density or non-finite "
+                "values); the adjoint of this run is not defined by the fused stages");
+  ACK(cudaMemcpyAsync(A->d_dts, A->dts.data(), A->nsteps * sizeof(double),
+                      cudaMemcpyHostToDevice, A->h->stream));
+  return BX_OK;
+}
+
+// ---- host level of the schedule
+
+static void free_host_level(bx_adj* A) {
+  if (A->cstream) cudaStreamSynchronize(A->cstream);
+  for (double* p : A->hsnap) cudaFreeHost(p);
+  A->hsnap.clear();
+  for (int b = 0; b < 2; ++b) {
+    if (A->cev[b]) cudaEventDestroy(A->cev[b]);
+    if (A->uev[b]) cudaEventDestroy(A->uev[b]);
+    A->cev[b] = A->uev[b] = nullptr;
+    A->hold[b] = nullptr;
+    A->hold_step[b] = -1;
+  }
+  if (A->cstream) cudaStreamDestroy(A->cstream);
+  A->cstream = nullptr;
+  A->hstride = 0;
+  A->host_bytes = 0;
+  A->host_valid = false;
+}
+
+// MemAvailable of /proc/meminfo in bytes, or 0 when it cannot be read
+static unsigned long long host_mem_available() {
+  FILE* f = std::fopen("/proc/meminfo", "r");
+  if (!f) return 0;
+  char line[256];
+  unsigned long long kb = 0;
+  while (std::fgets(line, sizeof line, f))
+    if (std::sscanf(line, "MemAvailable: %llu kB", &kb) == 1) break;
+  std::fclose(f);
+  return kb * 1024ull;
+}
+
+// copy the state of step `step` (host snapshot j-1, j = step / hstride) into
+// hold[b] on the copy stream, after the compute stream's work so far is done
+// with that buffer
+static int fetch_hold(bx_adj* A, int b, long long step) {
+  const size_t bytes = 5 * A->ng * sizeof(double);
+  ACK(cudaEventRecord(A->uev[b], A->h->stream));
+  ACK(cudaStreamWaitEvent(A->cstream, A->uev[b], 0));
+  ACK(cudaMemcpyAsync(A->hold[b], A->hsnap[step / A->hstride - 1], bytes, cudaMemcpyHostToDevice,
+                      A->cstream));
+  ACK(cudaEventRecord(A->cev[b], A->cstream));
+  A->hold_step[b] = step;
+  return BX_OK;
+}
+
+// reverse every step with the host level: segments [j L, (j+1) L) from the
+// last to the first, each by reverse_range over the device pool
+static int reverse_host_level(bx_adj* A, double* lam) {
+  const long long L = A->hstride;
+  const long long nseg = (A->nsteps + L - 1) / L;
+  for (long long j = nseg - 1; j >= 0; --j) {
+    const long long a = j * L, b = std::min(A->nsteps, a + L);
+    const double* Xa = A->pool[0];
+    if (j > 0) {
+      const int hb = (int)(j & 1);
+      if (A->hold_step[hb] != a)
+        if (int r = fetch_hold(A, hb, a)) return r;
+      ACK(cudaStreamWaitEvent(A->h->stream, A->cev[hb], 0));
+      Xa = A->hold[hb];
+    }
+    // the start of segment j-1 goes into the buffer segment j+1 used
+    if (j - 1 >= 1 && A->hold_step[(j - 1) & 1] != a - L)
+      if (int r = fetch_hold(A, (int)((j - 1) & 1), a - L)) return r;
+    if (int r = reverse_range(A, Xa, a, b, lam, false)) return r;
+  }
+  return BX_OK;
+}
+
 extern "C" {
 
 const char* bx_adj_last_error(bx_adj* A) { return A ? A->err.c_str() : g_adj_err.c_str(); }
@@ -1360,6 +1491,7 @@ const char* bx_adj_last_error(bx_adj* A) { return A ? A->err.c_str() : g_adj_err
 int bx_adj_destroy(bx_adj* A) {
   if (!A) return BX_OK;
   if (A->h && A->h->stream) cudaStreamSynchronize(A->h->stream);
+  free_host_level(A);
   for (double* p : A->pool) cudaFree(p);
   double* ps[] = {A->W0, A->W1, A->W2, A->XT, A->lamA, A->lamB, A->lamC1,
                   A->P,  A->PA, A->d_dts};
@@ -1380,12 +1512,13 @@ int bx_adj_create(const bx_params* params, int64_t nsteps, int32_t snapshots, bx
     delete A;
     return r;
   }
-  if (!A->h->eligible) {
+  if (!adjoint_grid(*params, A->h->T)) {
     bx_adj_destroy(A);
     return aerr(nullptr, BX_ERR_UNSUPPORTED,
-                "the adjoint follows the fused stage kernels, which this grid does not run "
-                "(ghost fill not resolved within two sweeps, or fluxangmom)");
+                "the adjoint follows the fused stage arithmetic, which this grid does not have "
+                "(face ghosts off the donor rule, fluxangmom or a tabulated EOS)");
   }
+  A->dt_phase = !A->h->T.resolved2;
   const long long n = A->h->g.ng;
   A->ng = n;
   A->nsteps = nsteps;
@@ -1462,6 +1595,52 @@ int bx_adj_stage0_cache(bx_adj* A, int32_t entries) {
   return BX_OK;
 }
 
+int bx_adj_host_level(bx_adj* A, int64_t stride, int64_t* host_bytes) {
+  if (!A || stride < 0 || stride == 1) return aerr(A, BX_ERR_ARG, "bad arguments");
+  if (A->h && A->h->stream) cudaStreamSynchronize(A->h->stream);
+  free_host_level(A);
+  if (host_bytes) *host_bytes = 0;
+  if (stride == 0 || stride >= A->nsteps) return BX_OK;
+  if (A->snaps < 3)
+    return aerr(A, BX_ERR_ARG, "the host level needs at least 3 snapshots (2 hold segment starts)");
+  const long long nhost = (A->nsteps - 1) / stride;  // steps stride, 2 stride, ... < nsteps
+  const size_t per = 5 * A->ng * sizeof(double);
+  const unsigned long long need = (unsigned long long)nhost * per;
+  const unsigned long long avail = host_mem_available();
+  // pinned pages cannot be swapped out: leave the system half of what it has
+  if (avail == 0 || need > avail / 2)
+    return aerr(A, BX_ERR_NOMEM,
+                "host level: " + std::to_string(need >> 20) + " MiB of pinned memory requested, " +
+                    std::to_string(avail >> 20) + " MiB available (at most half is taken)");
+  int rc = BX_OK;
+  auto fail = [&](int code) {
+    free_host_level(A);
+    return code;
+  };
+  ACK(cudaStreamCreateWithFlags(&A->cstream, cudaStreamNonBlocking));
+  for (int b = 0; b < 2; ++b) {
+    if ((rc = (cudaEventCreateWithFlags(&A->cev[b], cudaEventDisableTiming) == cudaSuccess &&
+               cudaEventCreateWithFlags(&A->uev[b], cudaEventDisableTiming) == cudaSuccess)
+                  ? BX_OK
+                  : BX_ERR_CUDA))
+      return fail(aerr(A, rc, "host level: event creation failed"));
+  }
+  A->hsnap.assign(nhost, nullptr);
+  for (long long j = 0; j < nhost; ++j)
+    if (cudaHostAlloc(&A->hsnap[j], per, cudaHostAllocDefault) != cudaSuccess) {
+      cudaGetLastError();
+      A->hsnap[j] = nullptr;
+      return fail(aerr(A, BX_ERR_NOMEM, "host level: pinned allocation failed"));
+    }
+  A->hold[0] = A->pool[A->snaps];
+  A->hold[1] = A->pool[A->snaps - 1];
+  A->hstride = stride;
+  A->host_bytes = need;
+  A->host_valid = false;  // filled by the next unfrozen forward run
+  if (host_bytes) *host_bytes = (int64_t)need;
+  return BX_OK;
+}
+
 int bx_adj_set_stream(bx_adj* A, void* s) {
   if (!A) return BX_ERR_ARG;
   return bx_set_stream(A->h, s);
@@ -1491,12 +1670,27 @@ int bx_adj_forward(bx_adj* A, const double* cons0, double* consT, int32_t frozen
   c.max_step = 1ll << 62;
   ACK(cudaMemcpyAsync(h->d_ctrl, &c, sizeof(Ctrl), cudaMemcpyHostToDevice, s));
   ACK(box_rate(g, X0, g.ng, h->d_ctrl, s));
+  // dt from the recorded sequence: frozen runs, and unfrozen ones on grids
+  // whose dt comes from the per-phase kernels (computed first)
+  const bool given_dt = frozen || A->dt_phase;
+  if (!frozen && A->dt_phase)
+    if (int r = phase_dts(A, X0)) return r;
   double* cur = X0;
   double* bufs[2] = {A->W0, A->W2};
   int nsrc = 1;
   for (long long k = 0; k < A->nsteps; ++k) {
     double* out = bufs[k & 1];
-    if (!frozen && A->chain_slot_of[k + 1] >= 0) out = A->pool[A->chain_slot_of[k + 1]];
+    int hb = -1;  // host level: the hold buffer this step's output goes to
+    if (!frozen && A->hstride) {
+      if ((k + 1) % A->hstride == 0 && k + 1 < A->nsteps) {
+        hb = (int)(((k + 1) / A->hstride) & 1);
+        // the copy out of this buffer two host snapshots ago must be done
+        ACK(cudaStreamWaitEvent(s, A->cev[hb], 0));
+        out = A->hold[hb];
+      }
+    } else if (!frozen && A->chain_slot_of[k + 1] >= 0) {
+      out = A->pool[A->chain_slot_of[k + 1]];
+    }
     StageArgs a{};
     a.ctrl = h->d_ctrl;
     a.geom = h->d_geom;
@@ -1504,7 +1698,7 @@ int bx_adj_forward(bx_adj* A, const double* cons0, double* consT, int32_t frozen
     a.ncells_total = g.ng;
     a.nsrc = nsrc;
     a.U = A->P;
-    if (frozen) {
+    if (given_dt) {
       k_set_clock<<<1, 1, 0, s>>>(h->d_ctrl, A->dts[k], 1);
     } else {
       ACK(launch_dt(h->d_ctrl, 1, s));
@@ -1516,10 +1710,23 @@ int bx_adj_forward(bx_adj* A, const double* cons0, double* consT, int32_t frozen
     a.Y = a.out;
     a.out = out;
     ACK(launch_stage(1, g.pow2 ? 1 : 0, g.threed != 0, a, h->ntiles, s));
-    if (!frozen) ACK(launch_end(h->d_ctrl, 1, s));
+    if (!given_dt) ACK(launch_end(h->d_ctrl, 1, s));
+    if (hb >= 0) {
+      ACK(cudaEventRecord(A->uev[hb], s));
+      ACK(cudaStreamWaitEvent(A->cstream, A->uev[hb], 0));
+      ACK(cudaMemcpyAsync(A->hsnap[(k + 1) / A->hstride - 1], out, n5 * sizeof(double),
+                          cudaMemcpyDeviceToHost, A->cstream));
+      ACK(cudaEventRecord(A->cev[hb], A->cstream));
+      A->hold_step[hb] = k + 1;
+    }
     A->step_nsrc[k] = nsrc;
     nsrc = 2;
     cur = out;
+  }
+  if (!frozen && A->hstride) {
+    // the forward's time includes its copies to the host
+    ACK(cudaStreamWaitEvent(s, A->cev[0], 0));
+    ACK(cudaStreamWaitEvent(s, A->cev[1], 0));
   }
   ACK(cudaEventRecord(ev.e1, s));
   ACK(cudaEventSynchronize(ev.e1));
@@ -1527,7 +1734,9 @@ int bx_adj_forward(bx_adj* A, const double* cons0, double* consT, int32_t frozen
   cudaEventElapsedTime(&ms, ev.e0, ev.e1);
   if (!frozen) {
     A->ms_fwd = ms;
-    ACK(cudaMemcpy(A->dts.data(), A->d_dts, A->nsteps * sizeof(double), cudaMemcpyDeviceToHost));
+    if (!A->dt_phase)
+      ACK(cudaMemcpy(A->dts.data(), A->d_dts, A->nsteps * sizeof(double),
+                     cudaMemcpyDeviceToHost));
   }
   Ctrl hc;
   ACK(cudaMemcpy(&hc, h->d_ctrl, sizeof(Ctrl), cudaMemcpyDeviceToHost));
@@ -1541,7 +1750,8 @@ int bx_adj_forward(bx_adj* A, const double* cons0, double* consT, int32_t frozen
   ACK(cudaStreamSynchronize(s));
   if (!frozen) {
     A->have_forward = true;
-    A->chain_valid = true;
+    A->chain_valid = A->hstride == 0;
+    A->host_valid = A->hstride != 0;
     A->c1_valid = A->c1pool != nullptr;
   }
   return BX_OK;
@@ -1564,8 +1774,11 @@ int bx_adj_backward(bx_adj* A, const double* lamT, double* lam0) {
   A->c1_hits = 0;
   A->rev_done = A->nsteps;
   A->pool_free.clear();
-  const bool chain = A->chain_valid;
-  for (int k = A->snaps; k >= 1; --k)
+  if (A->hstride && !A->host_valid)
+    return aerr(A, BX_ERR_STATE, "the host level was set after the forward run: run it again");
+  const bool chain = A->chain_valid && !A->hstride;
+  // with the host level the two top slots hold segment starts
+  for (int k = A->hstride ? A->snaps - 2 : A->snaps; k >= 1; --k)
     if (!chain || k > (int)A->chain.size()) A->pool_free.push_back(k);
   A->chain_left = chain ? (int)A->chain.size() : 0;
   double* lam = lam0;
@@ -1575,7 +1788,11 @@ int bx_adj_backward(bx_adj* A, const double* lamT, double* lam0) {
   // the chain snapshots are overwritten while reversing: a later backward
   // without a new forward rebuilds them
   A->chain_valid = false;
-  if (int r = reverse_range(A, A->pool[0], 0, A->nsteps, lam, chain)) return r;
+  if (A->hstride) {
+    if (int r = reverse_host_level(A, lam)) return r;
+  } else if (int r = reverse_range(A, A->pool[0], 0, A->nsteps, lam, chain)) {
+    return r;
+  }
   ACK(cudaEventRecord(ev.e1, s));
   ACK(cudaEventSynchronize(ev.e1));
   float ms = 0.f;
@@ -1619,15 +1836,14 @@ int bx_adj_device_bytes(const bx_params* params, int64_t nsteps, int32_t snapsho
     return aerr(nullptr, BX_ERR_ARG, "bad arguments");
   if ((long long)params->nx * params->ny * params->nz >= (1ll << 31))
     return aerr(nullptr, BX_ERR_ARG, "grid exceeds 2^31 cells");
-  // the grids bx_adj_create takes: those the fused stage kernels run
+  // the grids bx_adj_create takes
   {
     GhostTable T;
     build_ghost_tables(*params, T);
-    if (!(T.resolved2 && T.face_rule_ok && !(params->flags & BX_FLAG_PHASE_ONLY) &&
-          !params->fluxangmom && params->h2stat == -1))
+    if (!adjoint_grid(*params, T))
       return aerr(nullptr, BX_ERR_UNSUPPORTED,
-                  "the adjoint follows the fused stage kernels, which this grid does not run "
-                  "(ghost fill not resolved within two sweeps, fluxangmom or a tabulated EOS)");
+                  "the adjoint follows the fused stage arithmetic, which this grid does not have "
+                  "(face ghosts off the donor rule, fluxangmom or a tabulated EOS)");
   }
   const __int128 n = (__int128)params->nx * params->ny * params->nz;
   const __int128 snaps = std::min<long long>(snapshots, nsteps);

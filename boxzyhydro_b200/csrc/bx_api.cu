@@ -22,10 +22,6 @@
 
 using namespace bx;
 
-namespace bx {
-size_t stage_smem_bytes();
-int stage_blocks_per_sm(int stage, int pm, bool threed);
-}  // namespace bx
 
 #include "bx_handle.h"
 
@@ -1064,6 +1060,20 @@ int bx_profile_read(bx_handle* h, double* ms_stage0, double* ms_stage1, int64_t*
 }
 
 }  // extern "C"
+
+int bx_handle_start_from_planes(bx_handle* h, const double* planes) {
+  CHECK_H();
+  if (!planes || !h->pa.cons) return set_err(h, BX_ERR_ARG, "no planes or no reference arrays");
+  const long long n = h->g.ng;
+  cudaStream_t s = h->stream;
+  CK(cudaMemcpyAsync(h->pa.cons, planes, 5 * n * sizeof(double), cudaMemcpyDeviceToDevice, s));
+  for (int k = 0; k < 4; ++k)
+    if (int r = ghost1(h)) return r;
+  CK(prims_from_cons(h->g, h->pa, s));
+  h->launches += 5;
+  h->mode = 0;
+  return bx_adindx_fill(h);
+}
 
 int bx_handle_adopt_fused(bx_handle* h, const double* planes, long long ps, int nsrc,
                           const Ctrl& clock) {

@@ -28,9 +28,6 @@
 
 using namespace bx;
 
-namespace bx {
-int stage_blocks_per_sm(int stage, int pm, bool threed);
-}
 
 namespace {
 
@@ -60,6 +57,7 @@ struct bx_batch {
   Tile* d_tiles = nullptr;
   int ntiles = 0;
   int zc = 0;  // tile depth policy of the tile list (set_tiles)
+  int shape = 0;  // tile shape of the stage kernels (Shape0: 32 x 8, Shape1: 16 x 16)
   bool pow2 = true, threed = true;
   int pm = 1;  // 1: all boxes have power-of-two spacings; 0: otherwise (cdiv, exact for any)
   PhaseArrays scratch{};  // reference arrays of the largest box (downloads)
@@ -126,7 +124,8 @@ const char* bx_batch_last_error(bx_batch* b) { return b ? b->err.c_str() : g_bat
 // tile marches through the whole box depth when the ensemble has enough
 // columns to fill the GPU many times over (no z warm-up repeated per chunk),
 // else depths are cut into chunks of 32 planes.
-static std::vector<Tile> batch_tiles(const bx_batch* b, int zc_req) {
+static std::vector<Tile> batch_tiles(const bx_batch* b, int zc_req, int shape) {
+  const int TX = shape_tx(shape), TY = shape_ty(shape);
   int dev = 0, sms = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -135,7 +134,8 @@ static std::vector<Tile> batch_tiles(const bx_batch* b, int zc_req) {
     const Geom& g = b->G[i];
     ncol += (long long)((g.ax1 - g.ax0 + TX - 1) / TX) * ((g.ay1 - g.ay0 + TY - 1) / TY);
   }
-  const bool whole = ncol >= 16ll * sms * std::max(1, stage_blocks_per_sm(1, b->pm, b->threed));
+  const bool whole =
+      ncol >= 16ll * sms * std::max(1, stage_blocks_per_sm(1, b->pm, b->threed, shape));
   std::vector<std::pair<long long, Tile>> tl;
   for (int i = 0; i < b->nbox; ++i) {
     const Geom& g = b->G[i];
@@ -159,8 +159,8 @@ static std::vector<Tile> batch_tiles(const bx_batch* b, int zc_req) {
 }
 
 // (re)build the device tile list; a captured run graph holds the old one
-static int set_tiles(bx_batch* b, int zc_req) {
-  const std::vector<Tile> tiles = batch_tiles(b, zc_req);
+static int set_tiles(bx_batch* b, int zc_req, int shape) {
+  const std::vector<Tile> tiles = batch_tiles(b, zc_req, shape);
   if (b->graph) {
     cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
@@ -177,6 +177,7 @@ static int set_tiles(bx_batch* b, int zc_req) {
   BCK(cudaMemcpy(b->d_tiles_of_box, per_box.data(), b->nbox * sizeof(int),
                  cudaMemcpyHostToDevice));
   b->zc = zc_req;
+  b->shape = shape;
   return BX_OK;
 }
 
@@ -274,7 +275,7 @@ int bx_batch_create(int32_t nbox, const bx_params* params, bx_batch** out) {
     b->h_ctrl[i].nsrc = 1;
   }
   BCKC(cudaMemcpy(b->d_ctrl, b->h_ctrl, nbox * sizeof(Ctrl), cudaMemcpyHostToDevice));
-  if (int r = set_tiles(b, 0)) return fail(r);
+  if (int r = set_tiles(b, 0, 0)) return fail(r);
   // reference arrays for downloads, sized for the largest box
   const long long m = b->max_ng;
   BCKC(cudaMalloc(&b->scratch.cons, 5 * m * sizeof(double)));
@@ -289,8 +290,10 @@ int bx_batch_create(int32_t nbox, const bx_params* params, bx_batch** out) {
   BCKC(cudaMalloc(&b->d_ready, nbox * sizeof(unsigned)));
   BCKC(cudaMalloc(&b->d_head, sizeof(unsigned long long)));
   BCKC(cudaMalloc(&b->d_pstatus, sizeof(int)));
-  stage_blocks_per_sm(0, b->pm, b->threed);  // sets the shared-memory attribute
-  stage_blocks_per_sm(1, b->pm, b->threed);
+  for (int sh = 0; sh < kNumShapes; ++sh) {  // sets the shared-memory attributes
+    stage_blocks_per_sm(0, b->pm, b->threed, sh);
+    stage_blocks_per_sm(1, b->pm, b->threed, sh);
+  }
 #undef BCKC
   *out = b;
   return BX_OK;
@@ -437,7 +440,7 @@ static int enqueue_steps(bx_batch* b, int nsteps) {
     p.head = b->d_head;
     p.status = b->d_pstatus;
     p.poll_limit = b->poll_limit;
-    BCK(launch_batch_persistent(p, b->pm, b->threed, b->nbox, b->stream, nullptr));
+    BCK(launch_batch_persistent(p, b->pm, b->threed, b->nbox, b->stream, nullptr, b->shape));
     return BX_OK;
   }
   for (int k = 0; k < nsteps; ++k) {
@@ -447,10 +450,10 @@ static int enqueue_steps(bx_batch* b, int nsteps) {
     a.X = b->buf[X];
     a.Y = nullptr;
     a.out = b->buf[Y];
-    BCK(launch_stage(0, b->pm, b->threed, a, b->ntiles, b->stream));
+    BCK(launch_stage(0, b->pm, b->threed, a, b->ntiles, b->stream, b->shape));
     a.Y = b->buf[Y];
     a.out = b->buf[Z];
-    BCK(launch_stage(1, b->pm, b->threed, a, b->ntiles, b->stream));
+    BCK(launch_stage(1, b->pm, b->threed, a, b->ntiles, b->stream, b->shape));
     BCK(launch_end_batch(b->d_ctrl, b->nbox, b->stream));
     c = Z;
   }
@@ -553,16 +556,17 @@ int bx_batch_run(bx_batch* b, int64_t nsteps, double endtime, int32_t use_graph)
 }
 
 // Run configuration of the ensemble picked by measurement.  Each candidate tile
-// depth (the default rule, whole box depths, and 64, 32, 16 and 8 planes) runs
-// `reps` trial steps from the boxes' current states -- a step reads the input
-// plane set and writes the other two, and the clocks are put back after every
-// trial, so the ensemble is left as it was -- with four launches per step; at
-// the fastest depth the persistent launch is timed the same way, and the faster
-// of the two launch forms stays.  The tile's x-y extent is the stage kernel's
-// (32 x 8: its shared-memory layout is fixed at compile time) and the halo is
-// the stencil's two cells (a deeper halo would fuse the two stages at the cost
-// of recomputing stage 0 on a two-cell ring around every tile, more FP64 work
-// for a kernel that is bound by FP64 issue, not by memory traffic).
+// shape (32 x 8 and 16 x 16 columns, both in 256-thread blocks; each has its own
+// compiled shared-memory layout) and tile depth (the default rule, whole box
+// depths, and 64, 32, 16 and 8 planes) runs `reps` trial steps from the boxes'
+// current states -- a step reads the input plane set and writes the other two,
+// and the clocks are put back after every trial, so the ensemble is left as it
+// was -- with four launches per step; at the fastest shape and depth the
+// persistent launch is timed the same way, and the faster of the two launch
+// forms stays.  The halo is the stencil's two cells (a deeper halo would fuse
+// the two stages at the cost of recomputing stage 0 on a two-cell ring around
+// every tile, more FP64 work for a kernel that is bound by FP64 issue, not by
+// memory traffic).
 static int trial_ms(bx_batch* b, const std::vector<Ctrl>& saved, int reps, double* ms_out) {
   double ms_min = 1e300;
   for (int r = 0; r < reps; ++r) {
@@ -595,21 +599,24 @@ int bx_batch_autotune(bx_batch* b, int32_t reps, int32_t* zc_out, double* ms_out
   if (int r = pull_ctrl(b)) return r;
   const std::vector<Ctrl> saved(b->h_ctrl, b->h_ctrl + b->nbox);
   const int cand[] = {0, -1, 64, 32, 16, 8};
-  int best = 0;
+  int best = 0, best_shape = 0;
   double best_ms = 1e300;
   b->persistent = false;
-  for (int zc : cand) {
-    // whole depths: a chunk no box exceeds
-    const int zreq = zc < 0 ? (1 << 30) : zc;
-    if (int r = set_tiles(b, zreq)) return r;
-    double ms = 0.0;
-    if (int r = trial_ms(b, saved, reps, &ms)) return r;
-    if (ms < best_ms) {
-      best_ms = ms;
-      best = zreq;
+  for (int sh = 0; sh < kNumShapes; ++sh) {
+    for (int zc : cand) {
+      // whole depths: a chunk no box exceeds
+      const int zreq = zc < 0 ? (1 << 30) : zc;
+      if (int r = set_tiles(b, zreq, sh)) return r;
+      double ms = 0.0;
+      if (int r = trial_ms(b, saved, reps, &ms)) return r;
+      if (ms < best_ms) {
+        best_ms = ms;
+        best = zreq;
+        best_shape = sh;
+      }
     }
   }
-  if (int r = set_tiles(b, best)) return r;
+  if (int r = set_tiles(b, best, best_shape)) return r;
   b->persistent = true;
   double pms = 0.0;
   if (int r = trial_ms(b, saved, reps, &pms)) return r;
@@ -619,6 +626,21 @@ int bx_batch_autotune(bx_batch* b, int32_t reps, int32_t* zc_out, double* ms_out
   if (int r = push_ctrl(b)) return r;
   if (zc_out) *zc_out = best;
   if (ms_out) *ms_out = best_ms;
+  return BX_OK;
+}
+
+int bx_batch_set_tile_shape(bx_batch* b, int32_t shape) {
+  if (!b || shape < 0 || shape >= kNumShapes) return berr(b, BX_ERR_ARG, "bad arguments");
+  return set_tiles(b, b->zc, shape);
+}
+
+int bx_batch_get_tile_shape(bx_batch* b, int32_t* shape, int32_t* tx, int32_t* ty,
+                            int32_t* depth) {
+  if (!b) return BX_ERR_ARG;
+  if (shape) *shape = b->shape;
+  if (tx) *tx = shape_tx(b->shape);
+  if (ty) *ty = shape_ty(b->shape);
+  if (depth) *depth = b->zc;
   return BX_OK;
 }
 

@@ -270,8 +270,10 @@ void build_ghost_tables(const bx_params& P, GhostTable& T) {
   T.resolved2 = resolved;
   // face ghosts (one coordinate in the ghost band) must follow the donor rule
   // used by the stage kernels: outflow -> first interior cell, reflective ->
-  // mirror image across the wall with that axis' momentum negated.
-  bool ok = resolved;
+  // mirror image across the wall with that axis' momentum negated.  Checked on
+  // unresolved plans too: there the stencils still read face ghosts only, and
+  // the lagging edge and corner ghosts enter nothing but the Courant maximum.
+  bool ok = true;
   const int nx = P.nx, ny = P.ny, nz = P.nz;
   const bool threed = nz >= 6;
   auto donor = [&](int c, int a0, int a1, int wl, int wr, uint8_t bit, uint8_t& sg) {

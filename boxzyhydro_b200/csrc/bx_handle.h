@@ -78,3 +78,9 @@ int bx_create_lean(const bx_params* params, bx_handle** out);
 // a box on a handle of its own.
 int bx_handle_adopt_fused(bx_handle* h, const double* planes, long long ps, int nsrc,
                           const bx::Ctrl& clock);
+// Start the reference arrays of h from the five conserved planes (plane stride
+// ngrid) on the device: two calls of the ghost fill (four sweeps, so every
+// ghost the sweeps reach is set from the interior, whatever the planes held
+// there), u = m/rho and state()'s pressure; the handle's next step then runs on
+// the per-phase kernels unless the grid takes the fused ones.
+int bx_handle_start_from_planes(bx_handle* h, const double* planes);

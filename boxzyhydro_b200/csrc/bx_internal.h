@@ -95,6 +95,38 @@ constexpr int TY = BX_TY;
 constexpr int NT = BX_NT;
 static_assert(TX * TY <= NT && NT % 32 == 0, "tile larger than the block");
 
+// The stage kernels' tile shapes: TX_ x TY_ interior columns in a block of NT
+// threads, and the shared-memory layout that follows from them (per z plane:
+// primitives of the tile plus a two-cell halo, aliased with the x/y face
+// fluxes; x and y face states; per-thread z-pipeline slots).  Shape 0 is the
+// single-grid path's (TX x TY); the batched path's autotuner may pick shape 1.
+template <int TX_, int TY_>
+struct TileShape {
+  static constexpr int TX = TX_, TY = TY_;
+  static constexpr int NT = BX_NT;
+  static constexpr int PW = TX + 4;          // prim plane width (x halo 2)
+  static constexpr int NP = (TY + 4) * PW;   // prim plane cells
+  static constexpr int NSX = TY * (TX + 2);  // x-state cells
+  static constexpr int NSY = (TY + 2) * TX;  // y-state cells
+  static constexpr int NFX = TY * (TX + 1);  // x faces
+  static constexpr int NFY = (TY + 1) * TX;  // y faces
+  // per-thread z-pipeline slots (3-D): the z flux below and above the own cell
+  // (5 + 5) and the plus z-state carried to the next plane (6), kept in shared
+  // memory so the x/y phases have the registers
+  static constexpr int NZS = 16;
+  // the face fluxes of the face and update phases alias the primitives
+  static constexpr int NR0 = (7 * NP > 5 * (NFX + NFY)) ? 7 * NP : 5 * (NFX + NFY);
+  static constexpr int SMEM_DOUBLES = NR0 + 12 * NSX + 12 * NSY + NZS * NT;
+  static_assert(TX * TY <= NT && NT % 32 == 0, "tile larger than the block");
+  static_assert(4 * (TX + TY) <= NT, "one halo cell per thread and plane at most");
+};
+using Shape0 = TileShape<TX, TY>;
+using Shape1 = TileShape<16, 16>;
+constexpr int kNumShapes = 2;
+// the x and y extents of tile shape `shape`
+inline int shape_tx(int shape) { return shape == 1 ? Shape1::TX : Shape0::TX; }
+inline int shape_ty(int shape) { return shape == 1 ? Shape1::TY : Shape0::TY; }
+
 // ghost-fill tables: per ghost (index order), destination cell, source cell and
 // momentum sign mask (bit0: m1, bit1: m2, bit2: m3 negated).
 struct GhostTable {
@@ -134,9 +166,14 @@ struct StageArgs {
 // host threads may launch the same kernel.
 cudaError_t ensure_dyn_smem(const void* fn, size_t bytes);
 
+// dynamic shared memory of the stage kernels of a tile shape, and their resident
+// blocks per SM (sets the shared-memory attribute on the current device)
+size_t stage_smem_bytes(int shape = 0);
+int stage_blocks_per_sm(int stage, int pm, bool threed, int shape = 0);
+
 // pm: 1 = every box has power-of-two spacings, 0 = otherwise
 cudaError_t launch_stage(int stage, int pm, bool threed, const StageArgs& a, int ntiles,
-                         cudaStream_t s);
+                         cudaStream_t s, int shape = 0);
 cudaError_t launch_dt(Ctrl* ctrl, int nbox, cudaStream_t s);
 cudaError_t launch_end(Ctrl* ctrl, int nbox, cudaStream_t s);
 
@@ -214,7 +251,7 @@ struct PersistArgs {
 // the launch of a run (after launch_dt_batch for its first step); blocks_out:
 // the blocks launched (resident blocks per SM x SMs)
 cudaError_t launch_batch_persistent(const PersistArgs& p, int pm, bool threed, int nbox,
-                                    cudaStream_t s, int* blocks_out);
+                                    cudaStream_t s, int* blocks_out, int shape = 0);
 // a wait of the persistent kernel on a counter nothing advances, with the given
 // poll limit: *gave_up = 1 when it returned without the counter (the check of
 // the bounded wait)

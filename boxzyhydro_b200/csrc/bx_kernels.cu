@@ -289,22 +289,7 @@ __device__ __forceinline__ void dir_states(const Prim& m, const Prim& c, const P
   muscl_states<POW2>(c, ud, sd, s1, s2, s3, sp, se, dt, ds, ids, mi, pl);
 }
 
-// shared-memory geometry of the stage kernel
-constexpr int PW = TX + 4;            // prim plane width (x halo 2)
-constexpr int NP = (TY + 4) * PW;     // prim plane cells
-constexpr int NSX = TY * (TX + 2);    // x-state cells
-constexpr int NSY = (TY + 2) * TX;    // y-state cells
-constexpr int NFX = TY * (TX + 1);    // x faces
-constexpr int NFY = (TY + 1) * TX;    // y faces
-// per-thread z-pipeline slots (3-D): the z flux below and above the own cell
-// (5 + 5) and the plus z-state carried to the next plane (6), kept in shared
-// memory so the x/y phases have the registers
-constexpr int NZS = 16;
-// the face fluxes of phases C/D alias the primitives of phases A/B
-constexpr int NR0 = (7 * NP > 5 * (NFX + NFY)) ? 7 * NP : 5 * (NFX + NFY);
-constexpr int SMEM_DOUBLES = NR0 + 12 * NSX + 12 * NSY + NZS * NT;
-static_assert(4 * (TX + TY) <= NT, "one halo cell per thread and plane at most");
-
+template <int NP>
 __device__ __forceinline__ void put_prim(double* SP, int i, const Prim& q) {
   SP[0 * NP + i] = q.d;
   SP[1 * NP + i] = q.u1;
@@ -314,6 +299,7 @@ __device__ __forceinline__ void put_prim(double* SP, int i, const Prim& q) {
   SP[5 * NP + i] = q.e;
   SP[6 * NP + i] = q.c;
 }
+template <int NP>
 __device__ __forceinline__ Prim get_prim(const double* SP, int i) {
   Prim q;
   q.d = SP[0 * NP + i];
@@ -398,11 +384,13 @@ __device__ __forceinline__ void epi_ieee(const Geom& g, const double n[5], doubl
 // dt: the step's full dt; nsrc: the sources the stage input is short of (both
 // read from the box's control block by the caller).  CG: inputs through L2 (the
 // persistent batched kernel).
-template <int STAGE, bool POW2, bool THREED, bool FULL, bool GRAV, bool CG = false>
+template <class S, int STAGE, bool POW2, bool THREED, bool FULL, bool GRAV, bool CG = false>
 __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, const Geom& g,
                                            Ctrl* C, double dt, int nsrc, double* sm,
                                            double* red_rate, unsigned* red_flags, int rs = 0) {
   const bool is0 = stage_is0<STAGE>(rs);
+  constexpr int TX = S::TX, TY = S::TY, NT = S::NT, PW = S::PW, NP = S::NP;
+  constexpr int NSX = S::NSX, NSY = S::NSY, NFX = S::NFX, NFY = S::NFY, NR0 = S::NR0;
   double* SP = sm;                    // [7][TY+4][TX+4] primitives of the plane
   double* SX = sm + NR0;              // [12][TY][TX+2] x states (minus 0..5, plus 6..11)
   double* SY = SX + 12 * NSX;         // [12][TY+2][TX] y states
@@ -477,7 +465,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
       } else {
         Pk = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z, flags, nsrc, dth, true, rs);
       }
-      put_prim(SP, (ty + 2) * PW + (tx + 2), Pk);
+      put_prim<NP>(SP, (ty + 2) * PW + (tx + 2), Pk);
       if (is0) {
         // sources change only E, so this is m/rho of the step input
         const long long o = g.base + gx + (long long)gy * g.sy + (long long)z * g.sz;
@@ -507,7 +495,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
       const bool near = cx >= -1 && cx <= w && cy >= -1 && cy <= h;
       const bool inner = fx >= g.ax0 && fx < g.ax1 && fy >= g.ay0 && fy < g.ay1;
       const Prim q = load_prim<STAGE, GRAV, CG>(a, g, fx, fy, z, flags, nsrc, dth, near && inner, rs);
-      put_prim(SP, (cy + 2) * PW + (cx + 2), q);
+      put_prim<NP>(SP, (cy + 2) * PW + (cx + 2), q);
     }
     if (THREED && own) {
       if (z + 1 >= g.az1) {
@@ -534,12 +522,12 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         if (i >= nxs) continue;
         const int cy = i / (w + 2), cx = i % (w + 2) - 1;
         const int c = (cy + 2) * PW + (cx + 2);
-        const Prim q = get_prim(SP, c);
+        const Prim q = get_prim<NP>(SP, c);
         const int fx = bx0 + cx;
         if (fx < g.ax0 || fx >= g.ax1) {
           ghost_states(q, mi, pl);
         } else {
-          dir_states<POW2>(get_prim(SP, c - 1), q, get_prim(SP, c + 1), q.u1, dt, g.dx, g.idx, mi,
+          dir_states<POW2>(get_prim<NP>(SP, c - 1), q, get_prim<NP>(SP, c + 1), q.u1, dt, g.dx, g.idx, mi,
                            pl);
         }
         const int o = cy * (TX + 2) + (cx + 1);
@@ -549,12 +537,12 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         const int k = i - nxs_w;
         const int cy = k / w - 1, cx = k % w;
         const int c = (cy + 2) * PW + (cx + 2);
-        const Prim q = get_prim(SP, c);
+        const Prim q = get_prim<NP>(SP, c);
         const int fy = by0 + cy;
         if (fy < g.ay0 || fy >= g.ay1) {
           ghost_states(q, mi, pl);
         } else {
-          dir_states<POW2>(get_prim(SP, c - PW), q, get_prim(SP, c + PW), q.u2, dt, g.dy, g.idy,
+          dir_states<POW2>(get_prim<NP>(SP, c - PW), q, get_prim<NP>(SP, c + PW), q.u2, dt, g.dy, g.idy,
                            mi, pl);
         }
         const int o = (cy + 1) * TX + cx;
@@ -709,11 +697,21 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
   }
 }
 
+template <int SH>
+struct ShapeSel {
+  using type = Shape0;
+};
+template <>
+struct ShapeSel<1> {
+  using type = Shape1;
+};
+
 // PM: 1 = every box of the launch has power-of-two spacings (divisions by the
 // cell sizes are multiplications by exact reciprocals), 0 = otherwise (cdiv,
-// exact for any spacing)
-template <int STAGE, int PM, bool THREED, bool GRAV = false>
+// exact for any spacing).  SH: the tile shape (Shape0 or Shape1).
+template <int STAGE, int PM, bool THREED, bool GRAV = false, int SH = 0>
 __global__ void __launch_bounds__(NT, 65536 / (NT * 128)) k_stage(StageArgs a) {
+  using S = typename ShapeSel<SH>::type;
   extern __shared__ double sm[];
   __shared__ Geom sg;
   __shared__ double red_rate[NT / 32];
@@ -725,19 +723,12 @@ __global__ void __launch_bounds__(NT, 65536 / (NT * 128)) k_stage(StageArgs a) {
   if (!C->active) return;
   const double dt = C->dt;
   const int nsrc = a.nsrc > 0 ? a.nsrc : C->nsrc;
-  const bool full = (t.x0 + TX <= sg.ax1 - sg.ax0) && (t.y0 + TY <= sg.ay1 - sg.ay0);
-  if (PM == 1) {
-    if (full)
-      stage_tile<STAGE, true, THREED, true, GRAV>(a, t, sg, C, dt, nsrc, sm, red_rate, red_flags);
-    else
-      stage_tile<STAGE, true, THREED, false, GRAV>(a, t, sg, C, dt, nsrc, sm, red_rate, red_flags);
-  } else {
-    if (full)
-      stage_tile<STAGE, false, THREED, true, GRAV>(a, t, sg, C, dt, nsrc, sm, red_rate, red_flags);
-    else
-      stage_tile<STAGE, false, THREED, false, GRAV>(a, t, sg, C, dt, nsrc, sm, red_rate,
-                                                    red_flags);
-  }
+  const bool full = (t.x0 + S::TX <= sg.ax1 - sg.ax0) && (t.y0 + S::TY <= sg.ay1 - sg.ay0);
+  constexpr bool P2 = PM == 1;
+  if (full)
+    stage_tile<S, STAGE, P2, THREED, true, GRAV>(a, t, sg, C, dt, nsrc, sm, red_rate, red_flags);
+  else
+    stage_tile<S, STAGE, P2, THREED, false, GRAV>(a, t, sg, C, dt, nsrc, sm, red_rate, red_flags);
 }
 
 // A batched box's clock at the start of a step (dt control of main.f90:266-281
@@ -820,17 +811,18 @@ __device__ __forceinline__ void ctrl_store_cg(Ctrl* p, const Ctrl& c) {
 // one tile of either stage in the persistent kernel: a single inlined body with
 // the stage as a runtime value (two bodies, or bodies called out of line, spill
 // registers) and the tile's extents at run time
-template <int PM, bool THREED>
+template <class S, int PM, bool THREED>
 __device__ __forceinline__ void persistent_tile(int stage, const StageArgs& a, const Tile& t,
                                                 const Geom& g, Ctrl* C, double dt, int nsrc,
                                                 double* sm, double* red_rate,
                                                 unsigned* red_flags) {
-  stage_tile<2, PM == 1, THREED, false, false, true>(a, t, g, C, dt, nsrc, sm, red_rate,
-                                                     red_flags, stage);
+  stage_tile<S, 2, PM == 1, THREED, false, false, true>(a, t, g, C, dt, nsrc, sm, red_rate,
+                                                        red_flags, stage);
 }
 
-template <int PM, bool THREED>
+template <int PM, bool THREED, int SH>
 __global__ void __launch_bounds__(NT, 65536 / (NT * 128)) k_batch_persistent(PersistArgs p) {
+  using S = typename ShapeSel<SH>::type;
   extern __shared__ double sm[];
   __shared__ Geom sg;
   __shared__ double red_rate[NT / 32];
@@ -871,7 +863,7 @@ __global__ void __launch_bounds__(NT, 65536 / (NT * 128)) k_batch_persistent(Per
       a.X = p.buf[X];
       a.Y = stage == 0 ? nullptr : p.buf[Y];
       a.out = stage == 0 ? p.buf[Y] : p.buf[Z];
-      persistent_tile<PM, THREED>(stage, a, t, sg, C, s_dt, s_nsrc, sm, red_rate, red_flags);
+      persistent_tile<S, PM, THREED>(stage, a, t, sg, C, s_dt, s_nsrc, sm, red_rate, red_flags);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -911,11 +903,11 @@ __global__ void k_wait_selftest(unsigned* never, long long limit, int* status) {
   if (!wait_at_least(never, 1u, limit)) atomicOr(status, 1);
 }
 
-template <int PM, bool THREED>
+template <int PM, bool THREED, int SH>
 static cudaError_t launch_persistent_t(const PersistArgs& p, int nbox, cudaStream_t s,
                                        int* blocks_out) {
-  const size_t smem = SMEM_DOUBLES * sizeof(double);
-  const void* fn = (const void*)k_batch_persistent<PM, THREED>;
+  const size_t smem = ShapeSel<SH>::type::SMEM_DOUBLES * sizeof(double);
+  const void* fn = (const void*)k_batch_persistent<PM, THREED, SH>;
   cudaError_t e = ensure_dyn_smem(fn, smem);
   if (e != cudaSuccess) return e;
   int dev = 0, sms = 0, per_sm = 0;
@@ -926,18 +918,25 @@ static cudaError_t launch_persistent_t(const PersistArgs& p, int nbox, cudaStrea
     return e;
   const int blocks = std::max(1, per_sm) * sms;
   k_persist_init<<<(nbox + 127) / 128, 128, 0, s>>>(p, nbox);
-  k_batch_persistent<PM, THREED><<<blocks, NT, smem, s>>>(p);
+  k_batch_persistent<PM, THREED, SH><<<blocks, NT, smem, s>>>(p);
   if (blocks_out) *blocks_out = blocks;
   return cudaGetLastError();
 }
 
-cudaError_t launch_batch_persistent(const PersistArgs& p, int pm, bool threed, int nbox,
-                                    cudaStream_t s, int* blocks_out) {
+template <int SH>
+static cudaError_t launch_persistent_s(const PersistArgs& p, int pm, bool threed, int nbox,
+                                       cudaStream_t s, int* blocks_out) {
   if (pm == 1)
-    return threed ? launch_persistent_t<1, true>(p, nbox, s, blocks_out)
-                  : launch_persistent_t<1, false>(p, nbox, s, blocks_out);
-  return threed ? launch_persistent_t<0, true>(p, nbox, s, blocks_out)
-                : launch_persistent_t<0, false>(p, nbox, s, blocks_out);
+    return threed ? launch_persistent_t<1, true, SH>(p, nbox, s, blocks_out)
+                  : launch_persistent_t<1, false, SH>(p, nbox, s, blocks_out);
+  return threed ? launch_persistent_t<0, true, SH>(p, nbox, s, blocks_out)
+                : launch_persistent_t<0, false, SH>(p, nbox, s, blocks_out);
+}
+
+cudaError_t launch_batch_persistent(const PersistArgs& p, int pm, bool threed, int nbox,
+                                    cudaStream_t s, int* blocks_out, int shape) {
+  return shape == 1 ? launch_persistent_s<1>(p, pm, threed, nbox, s, blocks_out)
+                    : launch_persistent_s<0>(p, pm, threed, nbox, s, blocks_out);
 }
 
 cudaError_t persistent_wait_selftest(long long poll_limit, int* gave_up, float* ms) {
@@ -969,41 +968,45 @@ cudaError_t persistent_wait_selftest(long long poll_limit, int* gave_up, float* 
   return e;
 }
 
-template <int STAGE, int PM, bool THREED, bool GRAV>
+template <int STAGE, int PM, bool THREED, bool GRAV, int SH>
 static cudaError_t launch_stage_t(const StageArgs& a, int ntiles, cudaStream_t s) {
-  const size_t smem = SMEM_DOUBLES * sizeof(double);
-  cudaError_t e = ensure_dyn_smem((const void*)k_stage<STAGE, PM, THREED, GRAV>, smem);
+  const size_t smem = ShapeSel<SH>::type::SMEM_DOUBLES * sizeof(double);
+  cudaError_t e = ensure_dyn_smem((const void*)k_stage<STAGE, PM, THREED, GRAV, SH>, smem);
   if (e != cudaSuccess) return e;
   if (ntiles <= 0) return cudaSuccess;
-  k_stage<STAGE, PM, THREED, GRAV><<<ntiles, NT, smem, s>>>(a);
+  k_stage<STAGE, PM, THREED, GRAV, SH><<<ntiles, NT, smem, s>>>(a);
   return cudaGetLastError();
 }
 
-template <int STAGE, bool GRAV>
+template <int STAGE, bool GRAV, int SH>
 static cudaError_t launch_stage_g(int pm, bool threed, const StageArgs& a, int ntiles,
                                   cudaStream_t s) {
-  if (pm == 1) return threed ? launch_stage_t<STAGE, 1, true, GRAV>(a, ntiles, s)
-                             : launch_stage_t<STAGE, 1, false, GRAV>(a, ntiles, s);
-  return threed ? launch_stage_t<STAGE, 0, true, GRAV>(a, ntiles, s)
-                : launch_stage_t<STAGE, 0, false, GRAV>(a, ntiles, s);
+  if (pm == 1) return threed ? launch_stage_t<STAGE, 1, true, GRAV, SH>(a, ntiles, s)
+                             : launch_stage_t<STAGE, 1, false, GRAV, SH>(a, ntiles, s);
+  return threed ? launch_stage_t<STAGE, 0, true, GRAV, SH>(a, ntiles, s)
+                : launch_stage_t<STAGE, 0, false, GRAV, SH>(a, ntiles, s);
 }
 
-// a.G set: the step has a gravitational force (instances with the force terms)
+// a.G set: the step has a gravitational force (instances with the force terms,
+// tile shape 0 only: the batched path, the one that tunes the shape, has no force)
 template <int STAGE>
 static cudaError_t launch_stage_s(int pm, bool threed, const StageArgs& a, int ntiles,
-                                  cudaStream_t s) {
-  return a.G ? launch_stage_g<STAGE, true>(pm, threed, a, ntiles, s)
-             : launch_stage_g<STAGE, false>(pm, threed, a, ntiles, s);
+                                  cudaStream_t s, int shape) {
+  if (a.G) return launch_stage_g<STAGE, true, 0>(pm, threed, a, ntiles, s);
+  return shape == 1 ? launch_stage_g<STAGE, false, 1>(pm, threed, a, ntiles, s)
+                    : launch_stage_g<STAGE, false, 0>(pm, threed, a, ntiles, s);
 }
 
 // pm: 1 every box has power-of-two spacings, 0 otherwise
 cudaError_t launch_stage(int stage, int pm, bool threed, const StageArgs& a, int ntiles,
-                         cudaStream_t s) {
-  return stage == 0 ? launch_stage_s<0>(pm, threed, a, ntiles, s)
-                    : launch_stage_s<1>(pm, threed, a, ntiles, s);
+                         cudaStream_t s, int shape) {
+  return stage == 0 ? launch_stage_s<0>(pm, threed, a, ntiles, s, shape)
+                    : launch_stage_s<1>(pm, threed, a, ntiles, s, shape);
 }
 
-size_t stage_smem_bytes() { return SMEM_DOUBLES * sizeof(double); }
+size_t stage_smem_bytes(int shape) {
+  return (shape == 1 ? Shape1::SMEM_DOUBLES : Shape0::SMEM_DOUBLES) * sizeof(double);
+}
 
 // ------------------------------------------------------------------ clock kernels
 // dt control of main.f90:266-281 and 342, per box
@@ -1950,16 +1953,29 @@ cudaError_t soa_to_aos(const double* soa, double* aos, long long n, int k, cudaS
 }  // namespace bx
 
 namespace bx {
-int stage_blocks_per_sm(int stage, int pm, bool threed) {
+int stage_blocks_per_sm(int stage, int pm, bool threed, int shape) {
   int nb = 0;
-  const size_t smem = stage_smem_bytes();
+  const size_t smem = stage_smem_bytes(shape);
   const void* fn;
-  if (stage == 0)
-    fn = pm == 1 ? (threed ? (const void*)k_stage<0, 1, true> : (const void*)k_stage<0, 1, false>)
-                 : (threed ? (const void*)k_stage<0, 0, true> : (const void*)k_stage<0, 0, false>);
-  else
-    fn = pm == 1 ? (threed ? (const void*)k_stage<1, 1, true> : (const void*)k_stage<1, 1, false>)
-                 : (threed ? (const void*)k_stage<1, 0, true> : (const void*)k_stage<1, 0, false>);
+  if (shape == 1) {
+    if (stage == 0)
+      fn = pm == 1 ? (threed ? (const void*)k_stage<0, 1, true, false, 1>
+                             : (const void*)k_stage<0, 1, false, false, 1>)
+                   : (threed ? (const void*)k_stage<0, 0, true, false, 1>
+                             : (const void*)k_stage<0, 0, false, false, 1>);
+    else
+      fn = pm == 1 ? (threed ? (const void*)k_stage<1, 1, true, false, 1>
+                             : (const void*)k_stage<1, 1, false, false, 1>)
+                   : (threed ? (const void*)k_stage<1, 0, true, false, 1>
+                             : (const void*)k_stage<1, 0, false, false, 1>);
+  } else {
+    if (stage == 0)
+      fn = pm == 1 ? (threed ? (const void*)k_stage<0, 1, true> : (const void*)k_stage<0, 1, false>)
+                   : (threed ? (const void*)k_stage<0, 0, true> : (const void*)k_stage<0, 0, false>);
+    else
+      fn = pm == 1 ? (threed ? (const void*)k_stage<1, 1, true> : (const void*)k_stage<1, 1, false>)
+                   : (threed ? (const void*)k_stage<1, 0, true> : (const void*)k_stage<1, 0, false>);
+  }
   if (ensure_dyn_smem(fn, smem) != cudaSuccess ||
       cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, fn, NT, smem) != cudaSuccess) {
     cudaGetLastError();

@@ -37,28 +37,18 @@ BX_HD double slope3(double c0, double c1, double c2) {
   const double d1 = c1 - c0, d2 = c2 - c0, d3 = c2 - c1;
   const double x1 = kTheta * d1, x2 = kHalf * d2, x3 = kTheta * d3;
 #ifdef __CUDA_ARCH__
-  // the least magnitude on the bit images (with the sign cleared, non-negative
-  // doubles order like their 64-bit patterns; a NaN, whose pattern lies above
-  // infinity's, is passed over like fmin does)
-  const unsigned long long a1 = (unsigned long long)__double_as_longlong(x1) & 0x7fffffffffffffffull;
-  const unsigned long long a2 = (unsigned long long)__double_as_longlong(x2) & 0x7fffffffffffffffull;
-  const unsigned long long a3 = (unsigned long long)__double_as_longlong(x3) & 0x7fffffffffffffffull;
-  const unsigned long long am = a1 < a2 ? (a1 < a3 ? a1 : a3) : (a2 < a3 ? a2 : a3);
-  const double m = __longlong_as_double((long long)am);
+  // The argument of least magnitude, with its own sign, by two compares of
+  // magnitudes (a NaN compares false; the guards flag it).  When d1 and d3
+  // share a strict sign (their sign bits agree and neither is zero, so m is
+  // not zero), all three arguments carry it and the result is m; anything else
+  // gives the reference's +0.  Ties of magnitude pick arguments of equal value.
+  const double t = fabs(x1) < fabs(x2) ? x1 : x2;
+  const double m = fabs(t) < fabs(x3) ? t : x3;
+  const int h1 = __double2hiint(d1), h3 = __double2hiint(d3);
+  const bool take = ((h1 ^ h3) >= 0) && (m != 0.0);
+  return take ? m : 0.0;
 #else
   const double m = fmin(fabs(x1), fmin(fabs(x2), fabs(x3)));
-#endif
-#ifdef __CUDA_ARCH__
-  // The same selection on the bit images, off the FP64 pipe: when d1 or d3 is
-  // a zero, x1 or x3 is one and m = 0, the reference's +0; otherwise d1 and d3
-  // share a strict sign exactly when their sign bits agree, and the result is
-  // m with that sign.  So: m != 0 and equal sign bits give m with d1's sign bit,
-  // anything else +0 (NaN inputs, which the guards flag, aside).
-  const int h1 = __double2hiint(d1), h3 = __double2hiint(d3);
-  const int hm = __double2hiint(m), lm = __double2loint(m);
-  const bool take = ((h1 ^ h3) >= 0) && ((hm | lm) != 0);
-  return take ? __hiloint2double(hm | (h1 & (int)0x80000000), lm) : 0.0;
-#else
   const bool pos = (d1 > 0.0) && (d3 > 0.0);
   const bool neg = (d1 < 0.0) && (d3 < 0.0);
   return pos ? m : (neg ? -m : 0.0);
@@ -190,12 +180,11 @@ BX_HD void ghost_states(const Prim& q, FaceState& mi, FaceState& pl) {
 }
 
 // The shared-denominator quotient below is exact for a numerator a when a = +-0
-// or |a| lies in [2^-450, 2^451): an integer test on the exponent field of its
-// bit image (biased exponents 573..1473), so it costs no FP64 instruction.
+// or |a| lies in [2^-450, 2^451) (NaN and infinities fail): three compares,
+// which the compiler chains on one predicate.
 __device__ __forceinline__ bool quot_fast_ok(double a) {
-  const unsigned hi = (unsigned)__double2hiint(a), lo = (unsigned)__double2loint(a);
-  const unsigned e = (hi >> 20) & 0x7ffu;
-  return (e - 573u <= 900u) || (((hi << 1) | lo) == 0u);
+  const double m = fabs(a);
+  return (m >= 0x1p-450 && m < 0x1p+451) || a == 0.0;
 }
 
 // q = a/d for five numerators over one denominator d, given r = RN(1/d) with d

@@ -258,18 +258,25 @@ int bx_batch_get_clock(bx_batch *b, int32_t box, double *time, double *dt, doubl
  * if one gave up).  Both forms give the same results bit for bit. */
 int bx_batch_run(bx_batch *b, int64_t nsteps, double endtime, int32_t use_graph);
 int bx_batch_set_persistent(bx_batch *b, int32_t enable);
+/* Tile shape of the stage kernels for the ensemble: 0 = 32 x 8 columns, 1 = 16 x 16
+ * (both in 256-thread blocks); bx_batch_autotune picks it.  The getter also gives the
+ * shape's extents and the tile depth (as bx_batch_autotune's zc). */
+int bx_batch_set_tile_shape(bx_batch *b, int32_t shape);
+int bx_batch_get_tile_shape(bx_batch *b, int32_t *shape, int32_t *tx, int32_t *ty,
+                            int32_t *depth);
 int bx_batch_get_persistent(bx_batch *b, int32_t *enabled);
 /* The bounded wait of the persistent launch, run on a counter that nothing advances
  * with the given poll limit: *gave_up = 1 when the wait ended without it (the limit
  * ran out), *ms its device time.  A check of the limit that needs no fault. */
 int bx_batch_wait_selftest(int64_t poll_limit, int32_t *gave_up, double *ms);
-/* Run configuration of the ensemble picked by measurement: every candidate tile depth
- * (the default rule, whole box depths, 64, 32, 16, 8 planes) runs reps trial steps
- * from the boxes' current states, which the trials leave unchanged (inputs are
- * not overwritten; clocks are restored), and the fastest is kept for the following
- * runs; at that depth the persistent launch is timed too and kept if faster
- * (bx_batch_get_persistent).  *zc = the chosen depth (0 = default rule, >= 2^30 =
- * whole depths), *ms = its trial step time.  Results do not depend on either. */
+/* Run configuration of the ensemble picked by measurement: every candidate tile shape
+ * (32 x 8, 16 x 16) and tile depth (the default rule, whole box depths, 64, 32, 16, 8
+ * planes) runs reps trial steps from the boxes' current states, which the trials leave
+ * unchanged (inputs are not overwritten; clocks are restored), and the fastest is kept
+ * for the following runs; with it the persistent launch is timed too and kept if
+ * faster (bx_batch_get_persistent, bx_batch_get_tile_shape).  *zc = the chosen depth
+ * (0 = default rule, >= 2^30 = whole depths), *ms = its trial step time.  Results do
+ * not depend on any of them. */
 int bx_batch_autotune(bx_batch *b, int32_t reps, int32_t *zc, double *ms);
 int bx_batch_download(bx_batch *b, int32_t box, double *cons, double *u, double *p);
 /* device time of the last run (ms), kernels it launched, boxes running on their own
@@ -279,12 +286,18 @@ int bx_batch_info(bx_batch *b, double *last_run_ms, int64_t *launches, int32_t *
 const char *bx_batch_last_error(bx_batch *b);
 
 /* ---- Discrete adjoint.  No counterpart in the reference.  Reverse-mode derivative
- * of an nsteps-step run of the fused stage kernels (the step of bx_step on grids whose
- * ghost plan resolves), with the dt sequence of the forward run held fixed and every
- * limiter/max/min branch taken as in the forward.  Device arrays are SoA planes
- * (5 x ngrid doubles, rho, m1, m2, m3, E) of the reference cons; ghost entries of
- * the inputs are ignored and those of gradients are zero.  Snapshots follow a
- * binomial schedule in `snapshots` plane sets. */
+ * of an nsteps-step run of the fused stage arithmetic (the step of bx_step), with the
+ * dt sequence of the forward run held fixed and every limiter/max/min branch taken as
+ * in the forward.  Grids: fixed gamma, no flux_ang, face ghosts on the donor rule of
+ * the stage kernels.  Where the two-sweep ghost plan leaves corner ghosts lagging
+ * (reflective 3-D boxes), which enter only the Courant maximum, an unfrozen forward
+ * first runs the per-phase kernels from cons0 to take their dt sequence (its time is
+ * part of the forward's).  Device arrays are SoA planes (5 x ngrid doubles, rho, m1,
+ * m2, m3, E) of the reference cons; ghost entries of the inputs are ignored (the run
+ * starts with the ghosts two calls of the fill give) and those of gradients are zero.
+ * The forward refuses runs in which the velocity limiter or the low-density branch
+ * fires (BX_ERR_STATE).  Snapshots follow a binomial schedule in `snapshots` plane
+ * sets. */
 typedef struct bx_adj bx_adj;
 int bx_adj_create(const bx_params *params, int64_t nsteps, int32_t snapshots, bx_adj **out);
 int bx_adj_destroy(bx_adj *a);
@@ -298,6 +311,19 @@ int bx_adj_keep_stage0(bx_adj *a, int32_t enable);
  * so the reverse of that step skips its stage-0 recompute; more entries keep
  * results for longer.  BX_ERR_NOMEM if they do not fit. */
 int bx_adj_stage0_cache(bx_adj *a, int32_t entries);
+/* Host level of the checkpoint schedule.  stride >= 2: the next unfrozen forward
+ * copies the state of steps stride, 2 stride, ... (below nsteps) into pinned host
+ * memory, on a copy stream beside the step kernels (the forward's time includes
+ * the copies), and backward passes reverse the segments between those steps from
+ * the last to the first, each with the device snapshots; the start of the next
+ * segment is copied back while the current one is reversed.  Two of the
+ * `snapshots` plane sets hold segment starts, so snapshots >= 3.  A segment of
+ * stride steps with at least stride - 1 free plane sets recomputes each of its
+ * states once.  stride = 0 (or >= nsteps) turns the level off and frees the host
+ * memory.  *host_bytes (may be NULL) receives the pinned bytes.  BX_ERR_NOMEM
+ * when they exceed half of the host's available memory (/proc/meminfo) or the
+ * allocation fails.  No reference counterpart (the reference has no adjoint). */
+int bx_adj_host_level(bx_adj *a, int64_t stride, int64_t *host_bytes);
 /* frozen=0: dt by the CFL rule (main.f90:266-281) and recorded; frozen=1: the recorded
  * dt sequence (for finite differences).  BX_ERR_STATE if a guard fired. */
 int bx_adj_forward(bx_adj *a, const double *cons0, double *consT, int32_t frozen);

@@ -84,6 +84,46 @@ def test_dot_product(walls, dims, dx):
     eng.close()
 
 
+def test_reflective_3d_box_takes_the_per_phase_dt_sequence():
+    """A reflective 3-D box: its two-sweep ghost plan leaves corner ghosts
+    lagging, which enter only the Courant maximum, so the engine takes the dt
+    sequence of the per-phase kernels and runs the fused stage arithmetic with
+    it.  The forward equals the oracle's run of the reference loop bit for bit
+    (dt sequence included), and the dot-product test holds to 1e-12."""
+    from boxzyhydro_b200.hydro import apply_ghost_plan, ghost_plan
+    walls, dims = (1,) * 6, (14, 12, 11)
+    st, eng = setup(walls, dims, nsteps=6, snaps=3)
+    hp = st.params
+    pl = ghost_plan(hp)
+    assert not pl["fused_ok"]
+    consT = fwd(eng, st.cons, frozen=False)
+    dts = eng.dts()
+    # the oracle from the state the engine starts from: two calls of the fill
+    c = st.cons.copy()
+    for _ in range(2):
+        c = apply_ghost_plan(c, pl["src2"], pl["sgn2"], pl["dst"])
+    o = O.Oracle(hp)
+    o.set_state(c, c[:, 1:4] / c[:, :1], np.ones(hp.ngrid), np.full(hp.ngrid, hp.gammafix))
+    odts = []
+    for _ in range(6):
+        assert o.step()
+        odts.append(o.clock()["dt"])
+    m = interior_mask(hp)
+    assert np.array_equal(np.array(odts), dts)
+    assert np.array_equal(o.get_state()[0][m], consT[m])
+    o.close()
+    rng = np.random.default_rng(9)
+    v = rand_dir(hp, rng, np.array([1.0, 0.3, 0.3, 0.3, 2.0]))
+    cT, dT = TLM.run(hp, st.cons, v, dts)
+    assert np.allclose(cT[m], consT[m], rtol=1e-13, atol=0), "TLM forward differs from GPU"
+    lamT = rand_dir(hp, rng, np.ones(5))
+    lam0 = bwd(eng, lamT)
+    d1 = float(np.sum(lamT[m] * dT[m]))
+    d2 = float(np.sum(lam0[m] * v[m]))
+    assert abs(d1 - d2) <= 1e-12 * abs(d1), (d1, d2)
+    eng.close()
+
+
 def test_dot_product_32cubed_twenty_steps():
     """The dot-product test on a 32^3-interior box over 20 steps with 5 snapshots
     (the checkpoint schedule recomputes), 1e-12 relative."""
@@ -251,6 +291,46 @@ def test_stage0_cache_sizes_give_the_same_gradient():
         fwd(eng, st.cons, frozen=False)
         assert np.array_equal(bwd(eng, lamT), ref), entries
     eng.close()
+
+
+def test_host_level_gives_the_same_gradient():
+    """States every `stride` steps in pinned host memory, the segments between
+    them reversed one by one: the same gradient bit for bit as the device-only
+    schedule, each state recomputed once when a segment fits the free plane sets,
+    and a second backward of the same run (segment starts fetched again) equal
+    to the first."""
+    from boxzyhydro_b200._lib import BoxzyError
+    st, eng = setup(nsteps=23, snaps=8)
+    hp = st.params
+    fwd(eng, st.cons, frozen=False)
+    rng = np.random.default_rng(8)
+    lamT = rand_dir(hp, rng, np.ones(5))
+    ref = bwd(eng, lamT)
+    for stride, entries in ((7, 2), (5, 8), (2, 2)):
+        eng.stage0_cache(entries)
+        nbytes = eng.host_level(stride)
+        assert nbytes == ((23 - 1) // stride) * 5 * hp.ngrid * 8
+        fwd(eng, st.cons, frozen=False)
+        got = bwd(eng, lamT)
+        assert np.array_equal(got, ref), stride
+        # six free plane sets: every segment reversed with each state computed once
+        nseg = (23 + stride - 1) // stride
+        assert eng.stats()["recomputed_steps"] == 23 - nseg, stride
+        assert np.array_equal(bwd(eng, lamT), ref), stride
+    # the level set after the forward run: refused until the forward runs again
+    eng.host_level(4)
+    with pytest.raises(BoxzyError):
+        bwd(eng, lamT)
+    eng.host_level(0)
+    fwd(eng, st.cons, frozen=False)
+    assert np.array_equal(bwd(eng, lamT), ref)
+    with pytest.raises(BoxzyError):
+        eng.host_level(1)
+    eng.close()
+    _, small = setup(nsteps=10, snaps=2)
+    with pytest.raises(BoxzyError):
+        small.host_level(3)
+    small.close()
 
 
 def test_torch_autograd_function():

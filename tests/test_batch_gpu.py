@@ -70,6 +70,29 @@ def test_persistent_launch_matches_single_grid_runs(graph):
     b.close()
 
 
+@pytest.mark.parametrize("persistent", [False, True])
+def test_16x16_tiles_match_single_grid_runs(persistent):
+    """The second tile shape (16 x 16 columns) in both launch forms: every box as
+    it would run alone, bit for bit."""
+    boxes = ensemble(10, seed=33, sides=(8, 12, 20, 13, 40, 18))
+    b = Batch([st.params for st in boxes])
+    b.set_tile_shape(1)
+    assert b.tile_shape[:3] == (1, 16, 16)
+    b.set_persistent(persistent)
+    for i, st in enumerate(boxes):
+        b.upload(i, st.cons)
+    b.run(4)
+    b.run(3)
+    for i, st in enumerate(boxes):
+        (c0, u0, p0), clk0 = alone(st, 7)
+        c1, u1, p1 = b.download(i)
+        assert np.array_equal(c0, c1) and np.array_equal(u0, u1) and np.array_equal(p0, p1), i
+        clk1 = b.clock(i)
+        for k in ("time", "dt", "dtold", "step"):
+            assert clk0[k] == clk1[k], (i, k)
+    b.close()
+
+
 def test_persistent_launch_with_a_box_leaving_the_fused_path():
     boxes = ensemble(6, seed=9)
     boxes[2].params.vlimit = 0.6
@@ -135,6 +158,7 @@ def test_autotune_leaves_the_ensemble_as_it_was():
     solo = b.info()["solo_boxes"]
     zc, ms = b.autotune(reps=2)
     assert ms > 0 and (zc in (0, 8, 16, 32, 64) or zc >= 1 << 30)
+    assert b.tile_shape[0] in (0, 1) and b.tile_shape[3] == zc
     assert b.info()["solo_boxes"] == solo
     for i in range(len(boxes)):
         assert b.clock(i)["step"] == 3
