@@ -631,6 +631,7 @@ def adjoint_measure(args, local):
     stt = eng.stats()
     del lamT
     ratio = stt["ms_backward"] / stats_fwd["ms_forward"]
+    grad_norm2 = float(torch.sum(grad * grad))
     # finite differences with the frozen dt sequence
     gen = torch.Generator(device=dev)
     gen.manual_seed(args.seed + 99)
@@ -692,6 +693,7 @@ def adjoint_measure(args, local):
         "engine_device_bytes": stt["device_bytes"],
         "peak_device_bytes_in_use": peak[0],
         "loss": loss,
+        "grad_norm2": grad_norm2,
         "fd_check": {"directions": args.fd_dirs, "h": h, "max_rel_diff": max(rel) if rel else None,
                      "median_rel_diff": float(np.median(rel)) if rel else None,
                      "per_direction": rel},
