@@ -563,10 +563,12 @@ def adjoint_measure(args, local):
         entries = 2
     if snaps <= 0:
         # engine: 7 state sets + 14 scratch planes + cache entries + (snaps + 1)
-        # state sets; this arm, beside c0: gradient, direction, perturbed state,
-        # output and one density plane (21 planes)
+        # state sets; this arm, beside c0, while the runs are timed: the forward's
+        # output (the loss adjoint), the gradient and one density plane.  The
+        # finite differences afterwards take their planes from the stage-0 cache,
+        # which is cut to two entries first.
         free = torch.cuda.mem_get_info(dev)[0]
-        fixed = (7 * 5 + 14 + 5 + 21) * plane + (6 << 30)
+        fixed = (7 * 5 + 14 + 5 + 11) * plane + (4 << 30)
         sets = int(max(3, (free - fixed) // (5 * plane)))
         if args.stage0_cache <= 0 and not args.keep_stage0:
             entries = max(2, min(8, round(0.35 * sets)))
@@ -632,6 +634,8 @@ def adjoint_measure(args, local):
     del lamT
     ratio = stt["ms_backward"] / stats_fwd["ms_forward"]
     grad_norm2 = float(torch.sum(grad * grad))
+    if (args.fd_dirs > 0 or args.fd_frozen_dirs > 0) and entries > 2:
+        eng.stage0_cache(2)  # room for the difference runs' planes
     # finite differences with the frozen dt sequence
     gen = torch.Generator(device=dev)
     gen.manual_seed(args.seed + 99)

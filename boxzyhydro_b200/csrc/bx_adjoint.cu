@@ -95,14 +95,17 @@ __global__ void k_r1_prims(Geom g, int stage, const double* A, const double* B, 
   const long long i = x + (long long)y * g.sy + (long long)z * g.sz;
   const long long n = g.ng;
   const C5 a = aload(A, n, g, x, y, z);
-  const double u1 = a.m1 / a.d, u2 = a.m2 / a.d, u3 = a.m3 / a.d;
+  // the forward's quotients, bit for bit: one exact reciprocal per density
+  const SharedDiv qa(a.d);
+  const double u1 = qa(a.m1), u2 = qa(a.m2), u3 = qa(a.m3);
   const double e = recon_eps(a.d, a.E, u1, u2, u3, g.small_eps);
   double p;
   if (stage == 0) {
     p = e * g.gm1;
   } else {
     const C5 b = aload(B, n, g, x, y, z);
-    const double s1 = b.m1 / b.d, s2 = b.m2 / b.d, s3 = b.m3 / b.d;
+    const SharedDiv qb(b.d);
+    const double s1 = qb(b.m1), s2 = qb(b.m2), s3 = qb(b.m3);
     p = eos_pressure(a.d, a.E, s1, s2, s3, g.gm1, g.small_eps);
   }
   P[i] = a.d;
@@ -111,7 +114,7 @@ __global__ void k_r1_prims(Geom g, int stage, const double* A, const double* B, 
   P[3 * n + i] = u3;
   P[4 * n + i] = p;
   P[5 * n + i] = e;
-  P[6 * n + i] = sqrt(p * g.gam / a.d);
+  P[6 * n + i] = sqrt(qa(p * g.gam));
 }
 
 // ---- conserved-variable VJP at cell (x,y,z) of a stage: gq holds the adjoints
@@ -130,13 +133,14 @@ __device__ __forceinline__ void cons_vjp_v(const Geom& g, int stage, const CvIn&
                                            const double gq[7], double gA[5], double gB[5]) {
   const double rho = v.rho, u[3] = {v.u[0], v.u[1], v.u[2]};
   const double p = v.p, e = v.e, cs = v.cs;
-  const double ir = 1.0 / rho;
+  // reciprocals of the derivative terms (not of values a branch depends on)
+  const double ir = rcp_deriv(rho);
   for (int q = 0; q < 5; ++q) gA[q] = gB[q] = 0.0;
   double grho = gq[0], gu[3] = {gq[1], gq[2], gq[3]}, gp = gq[4], ge = gq[5];
   if (cs > 0.0) {
     // c = sqrt(gam p / rho)
     const double h = kHalf * gq[6] * cs;
-    gp += h / p;
+    gp += h * rcp_deriv(p);
     grho -= h * ir;
   }
   if (stage == 0) {
@@ -146,7 +150,7 @@ __device__ __forceinline__ void cons_vjp_v(const Geom& g, int stage, const CvIn&
     const double us[3] = {v.bm[0] / v.bd, v.bm[1] / v.bd, v.bm[2] / v.bd};
     const double Ks = us[0] * us[0] + us[1] * us[1] + us[2] * us[2];
     if (v.aE - rho * kHalf * Ks > g.small_eps) {
-      const double gpg = gp * g.gm1, ib = 1.0 / v.bd;
+      const double gpg = gp * g.gm1, ib = rcp_deriv(v.bd);
       gA[4] += gpg;
       grho = fma(gpg, -kHalf * Ks, grho);
       for (int j = 0; j < 3; ++j) {
@@ -255,6 +259,16 @@ k_rdir(Geom g, const double* P, const double* lamL, double lscale, double dt, do
        RShape sh) {
   const int NL = sh.NL, W = sh.W, NQ = sh.NQ, NS = sh.NS, NF = sh.NF, ND = sh.ND;
   extern __shared__ double sm[];
+  // d slope(c+o) / d q(c) by the selected argument sq of genminmod (1:
+  // theta*(c1-c0), 2: half*(c2-c0), 3: theta*(c2-c1), 0: none): row o+1, column
+  // sq; c is the slope's c0 (o = +1), c1 (o = 0) or c2 (o = -1)
+  __shared__ double kk_tab[12];
+  if (threadIdx.x < 12) {
+    const int o = (int)threadIdx.x / 4 - 1, sq = (int)threadIdx.x % 4;
+    kk_tab[threadIdx.x] = o == 1 ? (sq == 1 ? -kTheta : (sq == 2 ? -kHalf : 0.0))
+                        : o == 0 ? (sq == 1 ? kTheta : (sq == 3 ? -kTheta : 0.0))
+                                 : (sq == 2 ? kHalf : (sq == 3 ? kTheta : 0.0));
+  }
   double* r1 = sm;
   double* r2 = sm + sh.r1;
   double* r3 = r2 + sh.r2;
@@ -285,27 +299,41 @@ k_rdir(Geom g, const double* P, const double* lamL, double lscale, double dt, do
   };
   auto valid = [&](int c) { return c >= lo - 1 && c <= hi; };
   auto inner = [&](int c) { return c >= lo && c < hi; };
+  // Each thread keeps one line l of the block and the positions j0, j0 + TPL,
+  // ... along it in every phase (x lines: consecutive threads take consecutive
+  // cells of a line; y/z lines: consecutive threads take adjacent lines), so the
+  // item decomposition and the line's offset are computed once, not per item.
+  const int TPL = blockDim.x / NL;
+  const int l = DIR == 0 ? (int)threadIdx.x / TPL : (int)threadIdx.x % NL;
+  const int j0 = DIR == 0 ? (int)threadIdx.x % TPL : (int)threadIdx.x / NL;
+  const bool lane = l < NL;
+  bool lok;
+  const long long lb = lane ? line_base(l, lok) : 0;
+  lok = lok && lane;
 
-  // P0: start fetching PA of the segment's cells (used in P5)
-  for (int t = threadIdx.x; t < NL * W; t += blockDim.x) {
-    const int l = DIR == 0 ? t / W : t % NL, j = DIR == 0 ? t % W : t / NL;
-    const int c = s0 + j;
-    bool ok;
-    const long long b = line_base(l, ok);
-    if (!(ok && valid(c))) continue;
-    const long long i = b + c * st;
-    for (int q = 0; q < 7; ++q) cp_async8(pa_s + q * NL * W + t, PA + q * n + i);
+  // PA is written, not accumulated, where no earlier direction reached: by the
+  // x lines everywhere (they run first and hold every interior cell and the
+  // x-face ghosts), by y and z lines at their own face ghosts (lo-1 and hi),
+  // which lie on no line of another direction.  So PA needs no clearing.
+  auto first = [&](int c) { return DIR == 0 || c == lo - 1 || c == hi; };
+  // P0: start fetching PA of the segment's other cells (used in P5)
+  if (DIR != 0) {
+    for (int j = j0; j < W && lok; j += TPL) {
+      const int c = s0 + j;
+      if (!valid(c) || first(c)) continue;
+      const long long i = lb + c * st;
+      const int kp = rsx<DIR>(l, j, W, NL);
+      for (int q = 0; q < 7; ++q) cp_async8(pa_s + q * NL * W + kp, PA + q * n + i);
+    }
+    cp_async_commit();
   }
-  cp_async_commit();
 
   // P1: primitives
-  for (int t = threadIdx.x; t < NL * NQ; t += blockDim.x) {
-    const int l = DIR == 0 ? t / NQ : t % NL, j = DIR == 0 ? t % NQ : t / NL;
+  for (int j = j0; j < NQ && lane; j += TPL) {
     const int c = s0 - 3 + j;
-    bool ok;
-    const long long b = line_base(l, ok);
+    const bool ok = lok;
     const int k = rsx<DIR>(l, j, NQ, NL);
-    const long long i = b + c * st;
+    const long long i = lb + c * st;
     if (ok && valid(c)) {
       for (int q = 0; q < 7; ++q) r1[q * NL * NQ + k] = P[q * n + i];
     } else {
@@ -320,8 +348,7 @@ k_rdir(Geom g, const double* P, const double* lamL, double lscale, double dt, do
   }
   __syncthreads();
   // P2: face states, slopes, selections
-  for (int t = threadIdx.x; t < NL * NS; t += blockDim.x) {
-    const int l = DIR == 0 ? t / NS : t % NL, j = DIR == 0 ? t % NS : t / NL;
+  for (int j = j0; j < NS && lane; j += TPL) {
     const int c = s0 - 2 + j;
     const int k = rsx<DIR>(l, j, NS, NL);
     auto qv = [&](int jj) {
@@ -372,11 +399,9 @@ k_rdir(Geom g, const double* P, const double* lamL, double lscale, double dt, do
   }
   __syncthreads();
   // P3: HLL derivative per face (high cell c = s0-1+j)
-  for (int t = threadIdx.x; t < NL * NF; t += blockDim.x) {
-    const int l = DIR == 0 ? t / NF : t % NL, j = DIR == 0 ? t % NF : t / NL;
+  for (int j = j0; j < NF && lane; j += TPL) {
     const int c = s0 - 1 + j;
-    bool ok;
-    const long long b = line_base(l, ok);
+    const bool ok = lok;
     const int k = rsx<DIR>(l, j, NF, NL);
     const int M3 = NL * NF;
     if (!(ok && c >= lo && c <= hi)) {
@@ -401,8 +426,7 @@ k_rdir(Geom g, const double* P, const double* lamL, double lscale, double dt, do
   }
   __syncthreads();
   // P4: MUSCL adjoint per cell c = s0-1+j (into r1: DQ planes 0-6, LS planes 7-12)
-  for (int t = threadIdx.x; t < NL * ND; t += blockDim.x) {
-    const int l = DIR == 0 ? t / ND : t % NL, j = DIR == 0 ? t % ND : t / NL;
+  for (int j = j0; j < ND && lane; j += TPL) {
     const int c = s0 - 1 + j;
     const int k = rsx<DIR>(l, j, ND, NL);
     const int M1 = NL * ND, M = NL * NS, M3 = NL * NF;
@@ -440,14 +464,15 @@ k_rdir(Geom g, const double* P, const double* lamL, double lscale, double dt, do
   }
   __syncthreads();
   // P5: gather and accumulate
-  cp_async_wait_all();
-  __syncthreads();
-  for (int t = threadIdx.x; t < NL * W; t += blockDim.x) {
-    const int l = DIR == 0 ? t / W : t % NL, j = DIR == 0 ? t % W : t / NL;
+  if (DIR != 0) {
+    cp_async_wait_all();
+    __syncthreads();
+  }
+  for (int j = j0; j < W && lok; j += TPL) {
     const int c = s0 + j;
-    bool ok;
-    const long long b = line_base(l, ok);
-    if (!(ok && valid(c))) continue;
+    if (!valid(c)) continue;
+    const long long b = lb;
+    const int kp = rsx<DIR>(l, j, W, NL);
     const int M1 = NL * ND;
     const int kc = rsx<DIR>(l, j + 1, ND, NL);
     double acc[7];
@@ -459,18 +484,17 @@ k_rdir(Geom g, const double* P, const double* lamL, double lscale, double dt, do
       const int sel = sel_s[rsx<DIR>(l, j + 2 + o, NS, NL)];
       const int kn = rsx<DIR>(l, j + 1 + o, ND, NL);
 #pragma unroll
-      for (int q = 0; q < 6; ++q) {
-        // d slope(c+o) / d q(c): c is the slope's c0 (o = +1), c1 (o = 0) or c2 (o = -1)
-        const int sq = (sel >> (2 * q)) & 3;
-        const double kk = o == 1 ? (sq == 1 ? -kTheta : (sq == 2 ? -kHalf : 0.0))
-                        : o == 0 ? (sq == 1 ? kTheta : (sq == 3 ? -kTheta : 0.0))
-                                 : (sq == 2 ? kHalf : (sq == 3 ? kTheta : 0.0));
-        acc[q] += kk * r1[(7 + q) * M1 + kn];
-      }
+      for (int q = 0; q < 6; ++q)
+        acc[q] += kk_tab[(o + 1) * 4 + ((sel >> (2 * q)) & 3)] * r1[(7 + q) * M1 + kn];
     }
     const long long i = b + c * st;
+    if (first(c)) {
 #pragma unroll
-    for (int q = 0; q < 7; ++q) PA[q * n + i] = pa_s[q * NL * W + t] + acc[q];
+      for (int q = 0; q < 7; ++q) PA[q * n + i] = acc[q];
+    } else {
+#pragma unroll
+      for (int q = 0; q < 7; ++q) PA[q * n + i] = pa_s[q * NL * W + kp] + acc[q];
+    }
   }
 }
 
@@ -588,10 +612,10 @@ __global__ void k_rcell(Geom g, const double* SA, const double* SB, const double
       for (int k = 1; k >= 0; --k) {
         // E' = max(E - K, eps) + K
         if (k < nsrc && !((k == 0 ? E0 : E1) - K > g.small_eps)) {
-          const double gE = l[4];
+          const double gE = l[4], id = rcp_deriv(d);
           l[4] = 0.0;
-          for (int j = 0; j < 3; ++j) l[1 + j] += gE * m[j] / d;
-          l[0] += gE * (-K / d);
+          for (int j = 0; j < 3; ++j) l[1 + j] += gE * m[j] * id;
+          l[0] += gE * (-K * id);
         }
       }
     }
@@ -634,10 +658,10 @@ __global__ void k_adj_src_vjp(Geom g, const double* X, int nsrc, double* lam) {
   for (int k = nsrc - 1; k >= 0; --k) {
     // E' = max(E - K, eps) + K
     if (!(Es[k] - K > g.small_eps)) {
-      const double gE = l[4];
+      const double gE = l[4], id = rcp_deriv(d);
       l[4] = 0.0;
-      for (int j = 0; j < 3; ++j) l[1 + j] += gE * m[j] / d;
-      l[0] += gE * (-K / d);
+      for (int j = 0; j < 3; ++j) l[1 + j] += gE * m[j] * id;
+      l[0] += gE * (-K * id);
     }
   }
   for (int q = 0; q < 5; ++q) lam[q * n + i] = l[q];
@@ -1156,7 +1180,6 @@ static int rev_stage(bx_adj* A, int stage, const double* SA, const double* SB, c
   bx_handle* h = A->h;
   const Geom& g = h->g;
   cudaStream_t s = h->stream;
-  const long long n = g.ng;
   // primitives of every cell: one block row per (y, z)
   const int tp = std::min(512, ((g.nx + 31) / 32) * 32);
   const dim3 pgrid((unsigned)((g.nx + tp - 1) / tp), (unsigned)g.ny, (unsigned)g.nz);
@@ -1167,7 +1190,6 @@ static int rev_stage(bx_adj* A, int stage, const double* SA, const double* SB, c
                    (unsigned)(g.threed ? g.az1 - g.az0 : g.nz));
   const long long nedge = 2ll * cgrid.y * cgrid.z;
   const dim3 egrid((unsigned)((nedge + 127) / 128));
-  ACK(cudaMemsetAsync(A->PA, 0, 7 * n * sizeof(double), s));
   ACK(launch_rdir<0>(g, A->P, lamL, lscale, dt, A->PA, s));
   ACK(launch_rdir<1>(g, A->P, lamL, lscale, dt, A->PA, s));
   if (g.threed) ACK(launch_rdir<2>(g, A->P, lamL, lscale, dt, A->PA, s));
