@@ -99,6 +99,8 @@ def lib():
         "bx_ghost_plan": (C.c_int, [C.POINTER(BxParams), i64p, vp, vp, vp, vp, vp, i32p]),
         "bx_profile": (C.c_int, [H, C.c_int32]),
         "bx_profile_read": (C.c_int, [H, dp, dp, i64p, i64p]),
+        "bx_step_host_profile": (C.c_int, [H, C.c_int32]),
+        "bx_step_host_timeline": (C.c_int, [H, C.POINTER(C.c_int32), dp]),
         "bx_fp64_peak": (C.c_int, [dp, dp]),
         "bx_check_shared_division": (C.c_int, [C.c_ulonglong, C.c_ulonglong, C.c_int,
                                                C.POINTER(C.c_ulonglong), dp, dp]),

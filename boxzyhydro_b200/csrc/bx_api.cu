@@ -210,6 +210,7 @@ int bx_destroy(bx_handle* h) {
   for (cudaStream_t x : h->hs)
     if (x) cudaStreamDestroy(x);
   for (cudaEvent_t e : h->hev) cudaEventDestroy(e);
+  for (cudaEvent_t e : h->io_tev) cudaEventDestroy(e);
   cudaFree(h->d_io_tiles);
   cudaFree(h->d_dst);
   cudaFree(h->d_src1);
@@ -890,11 +891,15 @@ static int host_io_enqueue(bx_handle* h, const double* cons_in, double* cons_out
   // the step has a force, else it is one force-free source short
   const int nsrc_out = h->gforce_set ? 1 : 2;
   int st1 = 0;  // stage-1 launches so far (alternating streams)
+  const bool tp = h->io_prof && !h->io_tev.empty();
+  auto tev = [&](int slab, int what) { return h->io_tev[1 + (size_t)kIoEv * slab + what]; };
   for (int k = 0; k < ns; ++k) {
     const bx_handle::Slab& sk = h->slabs[k];
     if (cons_in) {
+      if (tp) CK(cudaEventRecord(tev(k, 0), up));
       CK(cudaMemcpyAsync(aos + 5 * sk.i0, cons_in + 5 * sk.i0, (sk.i1 - sk.i0) * cell,
                          cudaMemcpyHostToDevice, up));
+      if (tp) CK(cudaEventRecord(tev(k, 1), up));
       CK(cudaEventRecord(ev_in[k], up));
       CK(cudaStreamWaitEvent(s, ev_in[k], 0));
       CK(slab_in(aos, X, n, sk.i0, sk.i1, s));
@@ -912,6 +917,7 @@ static int host_io_enqueue(bx_handle* h, const double* cons_in, double* cons_out
       h->launches += 1;
     }
     CK(cudaEventRecord(ev_s0[k], s));
+    if (tp) CK(cudaEventRecord(tev(k, 2), s));
     for (int j = 0; j < ns; ++j) {
       const bx_handle::Slab& sl = h->slabs[j];
       if (sl.s1_after != k) continue;
@@ -923,13 +929,17 @@ static int host_io_enqueue(bx_handle* h, const double* cons_in, double* cons_out
       aj.out = h->buf[Zi];
       CK(launch_stage(1, p2, t3, aj, sl.nt, sj));
       CK(cudaEventRecord(ev_st1[j], sj));
+      if (tp) CK(cudaEventRecord(tev(j, 3), sj));
       CK(cudaStreamWaitEvent(cs, ev_st1[j], 0));
       CK(slab_out(g, h->buf[Zi], n, nsrc_out, aos, sl.i0, sl.i1, h->d_dst, h->d_src2, h->d_sgn2,
                   sl.g0, sl.g1, cs));
       CK(cudaEventRecord(ev_cv[j], cs));
+      if (tp) CK(cudaEventRecord(tev(j, 4), cs));
       CK(cudaStreamWaitEvent(down, ev_cv[j], 0));
+      if (tp) CK(cudaEventRecord(tev(j, 5), down));
       CK(cudaMemcpyAsync(cons_out + 5 * sl.i0, aos + 5 * sl.i0, (sl.i1 - sl.i0) * cell,
                          cudaMemcpyDeviceToHost, down));
+      if (tp) CK(cudaEventRecord(tev(j, 6), down));
       h->launches += 3;
     }
   }
@@ -979,6 +989,13 @@ int bx_step_host(bx_handle* h, const double* cons_in, double* cons_out, double e
   h->clock.rate_bits0 = 0;
   if (int r = push_clock(h)) return r;
   const Ctrl before = h->clock;  // rate_bits: the rate dt is taken from if spec
+  if (h->io_prof) {
+    if (h->io_tev.empty()) {
+      h->io_tev.assign(1 + (size_t)kIoEv * h->slabs.size(), nullptr);
+      for (cudaEvent_t& e : h->io_tev) CK(cudaEventCreate(&e));
+    }
+    CK(cudaEventRecord(h->io_tev[0], s));
+  }
   CK(cudaEventRecord(ev_start, s));
   for (cudaStream_t x : h->hs) CK(cudaStreamWaitEvent(x, ev_start, 0));
   if (spec) CK(launch_dt(h->d_ctrl, 1, s));
@@ -1046,6 +1063,34 @@ int bx_profile(bx_handle* h, int32_t enable) {
   h->ms_stage[0] = h->ms_stage[1] = 0.0;
   h->n_stage = 0;
   h->launches = 0;
+  return BX_OK;
+}
+
+int bx_step_host_profile(bx_handle* h, int32_t enable) {
+  CHECK_H();
+  h->io_prof = enable != 0;
+  return BX_OK;
+}
+
+int bx_step_host_timeline(bx_handle* h, int32_t* nslabs, double* ms) {
+  CHECK_H();
+  if (!nslabs) return set_err(h, BX_ERR_ARG, "nslabs is required");
+  const int ns = (int)h->slabs.size();
+  if (!ms) {
+    *nslabs = ns;
+    return BX_OK;
+  }
+  if (*nslabs < ns || h->io_tev.empty())
+    return set_err(h, BX_ERR_STATE, "no profiled bx_step_host, or ms too short");
+  *nslabs = ns;
+  for (int k = 0; k < ns; ++k)
+    for (int w = 0; w < kIoEv; ++w) {
+      float t = 0.f;
+      const cudaError_t e =
+          cudaEventElapsedTime(&t, h->io_tev[0], h->io_tev[1 + (size_t)kIoEv * k + w]);
+      ms[(size_t)kIoEv * k + w] = e == cudaSuccess ? t : -1.0;
+      if (e != cudaSuccess) cudaGetLastError();
+    }
   return BX_OK;
 }
 

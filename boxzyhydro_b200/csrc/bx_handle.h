@@ -7,6 +7,11 @@
 
 #include "bx_internal.h"
 
+// timing events per slab of a profiled bx_step_host: upload start, upload end,
+// stage 0 enqueued after that upload, the slab's stage 1 end, its conversion end,
+// download start, download end
+constexpr int kIoEv = 7;
+
 struct bx_handle {
   bx_params P{};
   bx::Geom g{};
@@ -63,6 +68,11 @@ struct bx_handle {
   // upload copies, download copies, conversions, second stage-1 stream
   cudaStream_t hs[4] = {nullptr, nullptr, nullptr, nullptr};
   std::vector<cudaEvent_t> hev;  // start, join, then per slab: in, stage 0, stage 1, converted
+  // bx_step_host_profile: timing events, the start and per slab the upload's
+  // start and end, stage 0 enqueued after it, the slab's stage 1, conversion and
+  // the download's start and end (kIoEv each)
+  bool io_prof = false;
+  std::vector<cudaEvent_t> io_tev;
   // bx_run: CUDA graphs of a whole chunk of force-free steps, per input plane
   // set (3) and pending sources (1 or 2)
   cudaGraphExec_t run_graph[6] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};

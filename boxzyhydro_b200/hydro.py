@@ -230,6 +230,21 @@ class Hydro:
         self._c(lib().bx_profile_read(self._h, C.byref(a), C.byref(b), C.byref(n), C.byref(k)))
         return dict(ms_stage0=a.value, ms_stage1=b.value, fused_steps=n.value, launches=k.value)
 
+    def step_host_profile(self, enable=True):
+        """Record CUDA events per slab in the following step_host calls."""
+        self._c(lib().bx_step_host_profile(self._h, 1 if enable else 0))
+
+    def step_host_timeline(self):
+        """The last profiled step_host call, per slab (rows): milliseconds from
+        its start to upload start, upload end, stage 0 enqueued after that
+        upload, stage 1 end, conversion end, download start, download end."""
+        ns = C.c_int32()
+        self._c(lib().bx_step_host_timeline(self._h, C.byref(ns), None))
+        ms = np.empty((ns.value, 7), dtype=np.float64)
+        self._c(lib().bx_step_host_timeline(self._h, C.byref(ns),
+                                            ms.ctypes.data_as(C.POINTER(C.c_double))))
+        return ms
+
     def status(self):
         bits = C.c_uint32()
         path = C.c_int32()

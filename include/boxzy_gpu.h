@@ -220,6 +220,15 @@ int bx_device_cons(bx_handle *h, double **cons_soa, int64_t *ngrid);
 int bx_profile(bx_handle *h, int32_t enable);
 int bx_profile_read(bx_handle *h, double *ms_stage0, double *ms_stage1, int64_t *fused_steps,
                     int64_t *launches);
+/* Timeline of bx_step_host (a measurement aid): with enable != 0, each call records
+ * CUDA events per slab of its pipeline.  bx_step_host_timeline with ms == NULL sets
+ * *nslabs to the slab count; with ms of at least 7 x *nslabs doubles it fills, per
+ * slab k, ms[7k..7k+6] = milliseconds from the call's start to: upload start,
+ * upload end, the end of the stage-0 launches enqueued after that upload, the
+ * slab's stage-1 end, its conversion to the host layout, download start, download
+ * end (-1 where the last call recorded no such event). */
+int bx_step_host_profile(bx_handle *h, int32_t enable);
+int bx_step_host_timeline(bx_handle *h, int32_t *nslabs, double *ms);
 
 /* Host-only query (no GPU needed): the ghost-fill plan bx_create builds for a grid.
  * For each ghost cell in index order: dst = cell, src1/sgn1 = source cell and

@@ -168,3 +168,27 @@ def test_end_time_reached():
     st = ic.turbulent_box(n=32, seed=6)
     ga, gb = run_pair(st, 2, pinned=True, in_place=False, endtime=0.0)
     assert ga.clock()["step"] == 0
+
+
+def test_profiled_call_gives_a_timeline_and_the_same_state():
+    """With the timeline on, a call records its per-slab events (ordered as the
+    pipeline orders them) and gives the same state as without it."""
+    st = ic.turbulent_box(n=64, seed=6)
+    ga, gb = Hydro(st.params), Hydro(st.params)
+    c = pinned_copy(np.ascontiguousarray(st.cons))
+    ref = c.copy()
+    ga.step_host(c, c)
+    gb.step_host(ref, ref)
+    ga.step_host_profile(True)
+    ga.step_host(c, c)
+    gb.step_host(ref, ref)
+    assert np.array_equal(c, ref)
+    tl = ga.step_host_timeline()
+    assert tl.shape[0] > 4 and tl.shape[1] == 7
+    assert np.all(tl >= 0.0)
+    up0, up1, s0, s1, cv, dn0, dn1 = tl.T
+    assert np.all(up1 >= up0) and np.all(cv >= s1) and np.all(dn0 >= cv) and np.all(dn1 >= dn0)
+    assert np.all(np.diff(up1) >= 0.0)  # the uploads run in order on one stream
+    ga.step_host_profile(False)
+    ga.close()
+    gb.close()
