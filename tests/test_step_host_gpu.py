@@ -187,7 +187,12 @@ def test_profiled_call_gives_a_timeline_and_the_same_state():
     assert tl.shape[0] > 4 and tl.shape[1] == 7
     assert np.all(tl >= 0.0)
     up0, up1, s0, s1, cv, dn0, dn1 = tl.T
-    assert np.all(up1 >= up0) and np.all(cv >= s1) and np.all(dn0 >= cv) and np.all(dn1 >= dn0)
+    # events on one stream are ordered; across streams (a wait on another
+    # stream's event, then an event here) the two timestamps may differ by the
+    # few microseconds between the waited-on event and the one recorded beside it
+    tol = 0.05
+    assert np.all(up1 >= up0) and np.all(dn1 >= dn0)
+    assert np.all(cv >= s1 - tol) and np.all(dn0 >= cv - tol)
     assert np.all(np.diff(up1) >= 0.0)  # the uploads run in order on one stream
     ga.step_host_profile(False)
     ga.close()
