@@ -525,22 +525,31 @@ def host_mem_available():
     return 0
 
 
-def auto_host_stride(steps, sets, set_bytes):
-    """Stride of the adjoint's host level for `sets` free device plane sets: a
-    segment of L steps takes L + 1 sets (two hold segment starts) and recomputes
-    L - 1 steps plus stage 0 of the steps the remaining sets (stage-0 cache
-    entries, at least 2) do not cover (about half a step each); the host keeps
-    (steps - 1) // L states in at most 45 % of its available memory and at
-    most 256 GiB (pinning takes time).  0 when no stride fits."""
+def auto_host_plan(steps, sets, set_bytes, entries=4):
+    """Host level of the adjoint's schedule for `sets` free device plane sets:
+    the stride L and the device snapshots that recompute the fewest steps,
+    (L, snapshots) or (0, None) when the device pool alone does better.  The
+    host keeps (steps - 1) // L states in at most 45 % of its available memory
+    and at most 256 GiB (pinning takes time; the library refuses more than half);
+    two device sets hold segment starts and `entries` are stage-0 cache entries,
+    the rest reverse each segment (the schedule's own count, bx_adj_plan)."""
+    from boxzyhydro_b200.adjoint import plan
     cap = min(0.45 * host_mem_available(), float(256 << 30))
-    best, best_cost = 0, None
-    for L in range(2, max(2, sets - 4) + 1):
-        entries = sets - (L + 1)
-        if entries < 2 or ((steps - 1) // L) * set_bytes > cap:
+    snaps_dev = max(1, min(steps, sets - entries))
+    best_cost, best = plan(steps, snaps_dev)["recomputed_first"], (0, None)
+    snaps = sets - entries
+    if snaps < 3:
+        return best
+    for L in range(2, steps):
+        if ((steps - 1) // L) * set_bytes > cap:
             continue
-        cost = ((L - 1) + 0.5 * max(1, L - entries)) / L
-        if best_cost is None or cost < best_cost - 1e-12:
-            best, best_cost = L, cost
+        cost = 0
+        for a in range(0, steps, L):
+            seg = min(L, steps - a)
+            if seg > 1:
+                cost += plan(seg, snaps - 2)["recomputed_again"]
+        if cost < best_cost:
+            best_cost, best = cost, (L, snaps)
     return best
 
 
@@ -595,8 +604,10 @@ def adjoint_measure(args, local):
             entries = max(2, min(8, round(0.35 * sets)))
         snaps = int(max(1, min(args.steps, sets - entries)))
         if args.host_stride < 0:
-            args.host_stride = auto_host_stride(args.steps, sets, 5 * plane)
-        if args.host_stride >= 2:
+            args.host_stride, hs = auto_host_plan(args.steps, sets, 5 * plane)
+            if args.host_stride >= 2:
+                snaps, entries = hs, sets - hs
+        elif args.host_stride >= 2:
             # host level: stride + 1 plane sets (two hold segment starts, the
             # other stride - 1 take a segment's states), the rest cache entries
             snaps = int(max(3, min(sets - 2, args.host_stride + 1)))
