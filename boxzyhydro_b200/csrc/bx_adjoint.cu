@@ -219,6 +219,9 @@ __device__ __forceinline__ void cons_vjp(const Geom& g, int stage, const double*
 // a segment cell moves 64 contiguous bytes (measured at 128^3: 6.5 % less
 // backward time than 4 lines in 128-thread blocks; 11 or 16 lines with shorter
 // segments were slower).
+// first x of the y and z lines of the direction kernels (see k_rdir)
+__host__ __device__ inline int rdir_x0(const Geom& g) { return g.ax0 & ~3; }
+
 struct RShape {
   int NL, W, NQ, NS, NF, ND, nseg, threads;
   size_t r1, r2, r3, r4, smem;  // region sizes in doubles; smem in bytes
@@ -277,7 +280,11 @@ k_rdir(Geom g, const double* P, const double* lamL, double lscale, double dt, do
   double* lm_s = r1 + 7 * NL * NQ;  // lives in r1 beside the primitives until P4
   const long long n = g.ng;
   const int zlo = g.threed ? g.az0 : 0, zhi = g.threed ? g.az1 : g.nz;
-  const int nxi = g.ax1 - g.ax0, nyi = g.ay1 - g.ay0, nzi = zhi - zlo;
+  const int nyi = g.ay1 - g.ay0, nzi = zhi - zlo;
+  // y and z lines: x from the interior start rounded down to 4 cells (32
+  // bytes), so each 8-line group reads whole 32-byte sectors of a row; the
+  // lines left of the interior are idle
+  const int xs = rdir_x0(g), nxi = g.ax1 - xs;
   const int lo = DIR == 0 ? g.ax0 : DIR == 1 ? g.ay0 : g.az0;
   const int hi = DIR == 0 ? g.ax1 : DIR == 1 ? g.ay1 : g.az1;
   const long long st = DIR == 0 ? 1 : DIR == 1 ? g.sy : g.sz;
@@ -294,8 +301,10 @@ k_rdir(Geom g, const double* P, const double* lamL, double lscale, double dt, do
     ok = L < nlines;
     if (!ok) return 0;
     if (DIR == 0) return (g.ay0 + L % nyi) * g.sy + (zlo + L / nyi) * g.sz;
-    if (DIR == 1) return (g.ax0 + L % nxi) + (zlo + L / nxi) * g.sz;
-    return (g.ax0 + L % nxi) + (g.ay0 + L / nxi) * g.sy;
+    const int x = xs + (int)(L % nxi);
+    ok = x >= g.ax0;
+    if (DIR == 1) return x + (zlo + L / nxi) * g.sz;
+    return x + (g.ay0 + L / nxi) * g.sy;
   };
   auto valid = [&](int c) { return c >= lo - 1 && c <= hi; };
   auto inner = [&](int c) { return c >= lo && c < hi; };
@@ -1151,7 +1160,7 @@ template <int DIR, bool POW2>
 static cudaError_t launch_rdir(const Geom& g, const double* P, const double* lamL, double lscale,
                                double dt, double* PA, cudaStream_t s) {
   const long long nzi = g.threed ? g.az1 - g.az0 : g.nz;
-  const long long nxi = g.ax1 - g.ax0, nyi = g.ay1 - g.ay0;
+  const long long nxi = g.ax1 - rdir_x0(g), nyi = g.ay1 - g.ay0;
   const long long nlines = DIR == 0 ? nyi * nzi : DIR == 1 ? nxi * nzi : nxi * nyi;
   const int lo = DIR == 0 ? g.ax0 : DIR == 1 ? g.ay0 : g.az0;
   const int hi = DIR == 0 ? g.ax1 : DIR == 1 ? g.ay1 : g.az1;
