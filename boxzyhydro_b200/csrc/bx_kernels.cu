@@ -457,6 +457,12 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         for (int q = 0; q < 3; ++q) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.U + o3 + q * PS));
       }
     }
+    if (is0 && own && THREED && z + 3 < g.az1) {
+      // stage 0: the own column's step input of the next plane iteration
+      const long long o3 = g.base + gx + (long long)gy * g.sy + (long long)(z + 3) * g.sz;
+#pragma unroll
+      for (int q = 0; q < 5; ++q) asm volatile("prefetch.global.L2 [%0];" ::"l"(a.X + o3 + q * PS));
+    }
     Prim P2;
     FaceState mz1, pz1;
     if (own) {
