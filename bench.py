@@ -189,9 +189,10 @@ def physics_arm(args, rank, world, local):
     synthetic ideal-gas tables of the eos module's layout) and the gravity
     coupling (a softened point-mass potential handed over from page-locked host
     memory before every step, its upload and calc_gforce inside the timed
-    region).  All three run on the
-    per-phase kernels.  Device-timed steps and the oracle with the same physics
-    on a bounded sample of the host cores."""
+    region).  flux_ang runs on the per-phase kernels, the tabulated EOS and the
+    gravity coupling on the fused stage kernels (the line gives each variant's
+    path).  Device-timed steps and the oracle with the same physics on a
+    bounded sample of the host cores."""
     import dataclasses
 
     import numpy as np

@@ -54,7 +54,9 @@ static cudaError_t dalloc(void** p, size_t bytes) {
 }
 
 // ---- tiles: TX x TY column tiles times z chunks sized so the launch fills the GPU
-static std::vector<Tile> make_tiles(const Geom& g, int box, int slots, int zc_force = 0) {
+static std::vector<Tile> make_tiles(const Geom& g, int box, int slots, int zc_force = 0,
+                                    int shape = 0) {
+  const int TX = shape_tx(shape), TY = shape_ty(shape);
   const int NAx = g.ax1 - g.ax0, NAy = g.ay1 - g.ay0, NAz = g.az1 - g.az0;
   const int tx = (NAx + TX - 1) / TX, ty = (NAy + TY - 1) / TY;
   const long long cols = (long long)tx * ty;
@@ -122,9 +124,14 @@ static int create_handle(const bx_params* params, bx_handle** out, bool lean) {
   h->P = P;
   fill_geom(P, h->g);
   build_ghost_tables(P, h->T);
-  // flux_ang runs on the per-phase kernels only
-  h->eligible = h->T.resolved2 && h->T.face_rule_ok && !(P.flags & BX_FLAG_PHASE_ONLY) &&
-                !P.fluxangmom && P.h2stat == -1;
+  // flux_ang runs on the per-phase kernels only; the tabulated EOS takes the
+  // fused kernels (tile shape 2) once its tables are set, except with nz == 1,
+  // whose scale-height branch reads the previous gamma
+  const bool fusable = h->T.resolved2 && h->T.face_rule_ok &&
+                       !(P.flags & BX_FLAG_PHASE_ONLY) && !P.fluxangmom;
+  h->eligible = fusable && P.h2stat == -1;
+  h->tab_fusable = fusable && P.h2stat >= 0 && P.nz != 1;
+  h->shape = P.h2stat >= 0 ? 2 : 0;
   const long long ng = h->g.ng;
   h->nghost = (int)h->T.dst.size();
   auto fail = [&](int code) {
@@ -172,8 +179,8 @@ static int create_handle(const bx_params* params, bx_handle** out, bool lean) {
   int dev = 0, sms = 148;
   CKC(cudaGetDevice(&dev));
   CKC(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-  const int per_sm = std::max(1, stage_blocks_per_sm(1, h->g.pow2, h->g.threed));
-  std::vector<Tile> tiles = make_tiles(h->g, 0, sms * per_sm);
+  const int per_sm = std::max(1, stage_blocks_per_sm(1, h->g.pow2, h->g.threed, h->shape));
+  std::vector<Tile> tiles = make_tiles(h->g, 0, sms * per_sm, 0, h->shape);
   h->ntiles = (int)tiles.size();
   CKC(dalloc((void**)&h->d_tiles, tiles.size() * sizeof(Tile)));
   CKC(cudaMemcpy(h->d_tiles, tiles.data(), tiles.size() * sizeof(Tile), cudaMemcpyHostToDevice));
@@ -275,7 +282,12 @@ static int fused_arrays(bx_handle* h) {
   CK(fused_to_phase(h->g, h->buf[h->cur], h->nsrc, h->pa, h->nghost, h->d_dst, h->d_src2,
                     h->d_sgn2, h->stream));
   h->launches += 3;
-  if (h->p_saved) {
+  if (h->g.tab) {
+    // state() with the tables: p, gamma and mu from the conserved variables and
+    // u = m/rho (the velocity array at a step boundary of the fused path)
+    CK(phase_state(h->g, h->pa, h->d_ctrl, h->stream));
+    h->launches += 1;
+  } else if (h->p_saved) {
     // no fused step since the planes took the reference arrays: their p stands
     CK(cudaMemcpyAsync(h->pa.p, h->pa.cons_old + 3 * h->g.ng, h->g.ng * sizeof(double),
                        cudaMemcpyDeviceToDevice, h->stream));
@@ -512,9 +524,25 @@ int bx_save_cons_old(bx_handle* h) {
   return BX_OK;
 }
 
+// a grid with the tabulated EOS takes the fused kernels only without a force
+// (their force instances have the fixed-gamma tile shape): the state goes to
+// the reference arrays when a force is set, and back with the next clean step
+// once it is cleared
+static int tab_force_switch(bx_handle* h, bool force) {
+  if (!h->g.tab) return BX_OK;
+  if (force) {
+    if (int r = to_phase(h)) return r;
+    h->eligible = false;
+  } else {
+    h->eligible = h->tab_fusable && h->d_eos != nullptr;
+  }
+  return BX_OK;
+}
+
 int bx_set_gforce(bx_handle* h, const double* gforce) {
   CHECK_H();
   const long long n = h->g.ng;
+  if (int r = tab_force_switch(h, gforce != nullptr)) return r;
   if (!gforce) {
     h->gforce_set = false;
     CK(cudaStreamSynchronize(h->stream));
@@ -566,12 +594,15 @@ int bx_set_eos_table(bx_handle* h, const bx_eos_table* t) {
   e.tk2 = h->d_eos + 3 * n2;
   e.rho = h->d_eos + 4 * n2;
   e.deng = h->d_eos + 4 * n2 + nr;
+  // the fused kernels read the tables from here on (not while a force is set)
+  h->eligible = h->tab_fusable && !h->gforce_set;
   return BX_OK;
 }
 
 int bx_set_phi(bx_handle* h, const double* phi) {
   CHECK_H();
   if (!phi) return bx_set_gforce(h, nullptr);
+  if (int r = tab_force_switch(h, true)) return r;
   const long long n = h->g.ng;
   if (!h->pa.gforce) CK(dalloc((void**)&h->pa.gforce, 3 * n * sizeof(double)));
   double* tmp = staging(h);
@@ -650,6 +681,7 @@ static int fused_launch(bx_handle* h) {
   a.geom = h->d_geom;
   a.tiles = h->d_tiles;
   a.ncells_total = h->g.ng;
+  a.eos = h->pa.eos;
   a.nsrc = h->nsrc;
   // the velocity array is stale while the state lives in the planes (to_phase
   // rebuilds it), so it holds the stage-0 velocity here; cons_old likewise
@@ -663,11 +695,11 @@ static int fused_launch(bx_handle* h) {
   a.Y = nullptr;
   a.out = h->buf[Y];
   if (h->prof) CK(cudaEventRecord(h->ev[0], h->stream));
-  CK(launch_stage(0, p2, t3, a, h->ntiles, h->stream));
+  CK(launch_stage(0, p2, t3, a, h->ntiles, h->stream, h->shape));
   if (h->prof) CK(cudaEventRecord(h->ev[1], h->stream));
   a.Y = h->buf[Y];
   a.out = h->buf[Z];
-  CK(launch_stage(1, p2, t3, a, h->ntiles, h->stream));
+  CK(launch_stage(1, p2, t3, a, h->ntiles, h->stream, h->shape));
   if (h->prof) CK(cudaEventRecord(h->ev[2], h->stream));
   CK(launch_end(h->d_ctrl, 1, h->stream));
   h->launches += 4;
@@ -1191,6 +1223,7 @@ static int fused_run(bx_handle* h, double endtime, int64_t nsteps, int64_t* take
   a.geom = h->d_geom;
   a.tiles = h->d_tiles;
   a.ncells_total = g.ng;
+  a.eos = h->pa.eos;
   a.U = h->pa.u;
   a.G = h->gforce_set ? h->pa.gforce : nullptr;
   a.UC = h->pa.cons_old;
@@ -1203,10 +1236,10 @@ static int fused_run(bx_handle* h, double endtime, int64_t nsteps, int64_t* take
       a.X = h->buf[cur];
       a.Y = nullptr;
       a.out = h->buf[(cur + 1) % 3];
-      if (e == cudaSuccess) e = launch_stage(0, p2, t3, a, h->ntiles, s);
+      if (e == cudaSuccess) e = launch_stage(0, p2, t3, a, h->ntiles, s, h->shape);
       a.Y = h->buf[(cur + 1) % 3];
       a.out = h->buf[(cur + 2) % 3];
-      if (e == cudaSuccess) e = launch_stage(1, p2, t3, a, h->ntiles, s);
+      if (e == cudaSuccess) e = launch_stage(1, p2, t3, a, h->ntiles, s, h->shape);
       if (e == cudaSuccess) e = launch_end_batch(h->d_ctrl, 1, s);
       if (e != cudaSuccess) return e;
       cur = (cur + 2) % 3;

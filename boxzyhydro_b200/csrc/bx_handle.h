@@ -39,6 +39,10 @@ struct bx_handle {
   // (kept in pa.cons_old's fourth plane) is the one to give back
   bool p_saved = false;
   bool eligible = false;
+  // the grid would take the fused kernels with the tabulated EOS (tile shape
+  // 2): eligible turns on once the tables are set, and off while a force is set
+  bool tab_fusable = false;
+  int shape = 0;  // stage-kernel tile shape of the single-grid launches
   bool gforce_set = false;
   uint32_t status = 0;
   int last_path = 0;

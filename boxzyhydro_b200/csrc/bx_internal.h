@@ -100,10 +100,15 @@ static_assert(TX * TY <= NT && NT % 32 == 0, "tile larger than the block");
 // primitives of the tile plus a two-cell halo, aliased with the x/y face
 // fluxes; x and y face states; per-thread z-pipeline slots).  Shape 0 is the
 // single-grid path's (TX x TY); the batched path's autotuner may pick shape 1.
-template <int TX_, int TY_>
+template <int TX_, int TY_, bool TAB_ = false>
 struct TileShape {
   static constexpr int TX = TX_, TY = TY_;
   static constexpr int NT = BX_NT;
+  // TAB: the tabulated EOS, whose gamma is a reconstructed primitive (eight
+  // primitive fields, seven per face state)
+  static constexpr bool TAB = TAB_;
+  static constexpr int NPF = TAB ? 8 : 7;    // primitive fields
+  static constexpr int NSF = TAB ? 7 : 6;    // face-state fields
   static constexpr int PW = TX + 4;          // prim plane width (x halo 2)
   static constexpr int NP = (TY + 4) * PW;   // prim plane cells
   static constexpr int NSX = TY * (TX + 2);  // x-state cells
@@ -111,21 +116,28 @@ struct TileShape {
   static constexpr int NFX = TY * (TX + 1);  // x faces
   static constexpr int NFY = (TY + 1) * TX;  // y faces
   // per-thread z-pipeline slots (3-D): the z flux below and above the own cell
-  // (5 + 5) and the plus z-state carried to the next plane (6), kept in shared
-  // memory so the x/y phases have the registers
-  static constexpr int NZS = 16;
+  // (5 + 5) and the plus z-state carried to the next plane (NSF), kept in
+  // shared memory so the x/y phases have the registers
+  static constexpr int NZS = 10 + NSF;
   // the face fluxes of the face and update phases alias the primitives
-  static constexpr int NR0 = (7 * NP > 5 * (NFX + NFY)) ? 7 * NP : 5 * (NFX + NFY);
-  static constexpr int SMEM_DOUBLES = NR0 + 12 * NSX + 12 * NSY + NZS * NT;
+  static constexpr int NR0 = (NPF * NP > 5 * (NFX + NFY)) ? NPF * NP : 5 * (NFX + NFY);
+  static constexpr int SMEM_DOUBLES = NR0 + 2 * NSF * NSX + 2 * NSF * NSY + NZS * NT;
   static_assert(TX * TY <= NT && NT % 32 == 0, "tile larger than the block");
   static_assert(4 * (TX + TY) <= NT, "one halo cell per thread and plane at most");
 };
 using Shape0 = TileShape<TX, TY>;
 using Shape1 = TileShape<16, 16>;
-constexpr int kNumShapes = 2;
+// the tabulated EOS (single grids only): 32 x 6 columns, so the larger
+// primitive and face-state sets still fit two blocks per SM
+using Shape2 = TileShape<32, 6, true>;
+constexpr int kNumShapes = 2;  // the shapes the batched autotuner chooses among
 // the x and y extents of tile shape `shape`
-inline int shape_tx(int shape) { return shape == 1 ? Shape1::TX : Shape0::TX; }
-inline int shape_ty(int shape) { return shape == 1 ? Shape1::TY : Shape0::TY; }
+inline int shape_tx(int shape) {
+  return shape == 2 ? Shape2::TX : shape == 1 ? Shape1::TX : Shape0::TX;
+}
+inline int shape_ty(int shape) {
+  return shape == 2 ? Shape2::TY : shape == 1 ? Shape1::TY : Shape0::TY;
+}
 
 // ghost-fill tables: per ghost (index order), destination cell, source cell and
 // momentum sign mask (bit0: m1, bit1: m2, bit2: m3 negated).
@@ -143,6 +155,14 @@ void build_ghost_tables(const bx_params& P, GhostTable& T);
 void fill_geom(const bx_params& P, Geom& g);
 bool is_pow2(double x);
 
+// tabulated EOS on the device (H2STAT >= 0): tables of the eos module
+struct EosDev {
+  int neos, neos_rho;
+  double log_rho_low, drho, density_unit, tk_bgrnd;
+  const double *eng2, *gam2, *muc2, *tk2;  // (neos, neos_rho), neos fastest
+  const double *rho, *deng;                // (neos_rho)
+};
+
 // ---- kernels (bx_kernels.cu)
 struct StageArgs {
   const double* X;   // step input planes (C2 if nsrc==2, C3 if nsrc==1)
@@ -158,6 +178,7 @@ struct StageArgs {
   const Tile* tiles;
   long long ncells_total;  // plane stride of the pooled buffers
   int nsrc;                // > 0: sources the input is short of; 0: per box (Ctrl::nsrc)
+  EosDev eos;              // the tables of the tabulated EOS (tile shape 2 only)
 };
 
 // Raises the dynamic shared-memory limit of kernel `fn` on the current device
@@ -178,14 +199,6 @@ cudaError_t launch_dt(Ctrl* ctrl, int nbox, cudaStream_t s);
 cudaError_t launch_end(Ctrl* ctrl, int nbox, cudaStream_t s);
 
 // phase kernels (one reference subroutine each, full arrays)
-// tabulated EOS on the device (H2STAT >= 0): tables of the eos module
-struct EosDev {
-  int neos, neos_rho;
-  double log_rho_low, drho, density_unit, tk_bgrnd;
-  const double *eng2, *gam2, *muc2, *tk2;  // (neos, neos_rho), neos fastest
-  const double *rho, *deng;                // (neos_rho)
-};
-
 struct PhaseArrays {
   double* cons;     // 5*ng SoA
   double* cons_old; // 5*ng

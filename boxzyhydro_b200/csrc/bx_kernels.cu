@@ -47,6 +47,47 @@ cudaError_t ensure_dyn_smem(const void* fn, size_t bytes) {
 
 namespace {
 
+// get_gamma2 (eos.f90:653-699): gamma, mu and T from the tables by the specific
+// internal energy eng = eps/rho, linear in eng within the density row irho, then
+// linear in rho towards row irho+1.  eps is clamped like the reference's.
+__device__ void get_gamma2(const EosDev& e, double& eps, double rho, double& tk, double& m,
+                           double& gam) {
+  int irho = min((int)((log10(rho * e.density_unit) - e.log_rho_low) / e.drho) + 1, e.neos_rho);
+  if (irho < 1) irho = 1;
+  int irhop = irho + 1;
+  if (irhop > e.neos_rho) irhop = irho;
+  const long long ne = e.neos;
+  auto at = [&](const double* t, int ie, int ir) { return t[(ie - 1) + (ir - 1) * ne]; };
+  double eng = eps / rho;
+  int ientry = (int)((log10(eng) - log10(at(e.eng2, 1, irho))) / e.deng[irho - 1]) + 1;
+  if (ientry > e.neos - 1) {
+    ientry = e.neos - 1;
+    eng = at(e.eng2, e.neos, irho);
+    eps = eng * rho;
+  }
+  if (ientry < 1 || eng < at(e.eng2, 1, irho)) {
+    ientry = 1;
+    eng = at(e.eng2, 1, irho);
+    eps = eng * rho;
+  }
+  auto lin = [&](const double* t, int ir) {
+    return at(t, ientry, ir) + (at(t, ientry + 1, ir) - at(t, ientry, ir)) /
+                                   (at(e.eng2, ientry + 1, ir) - at(e.eng2, ientry, ir)) *
+                                   (eng - at(e.eng2, ientry, ir));
+  };
+  gam = lin(e.gam2, irho);
+  m = lin(e.muc2, irho);
+  tk = lin(e.tk2, irho);
+  if (!(e.rho[irho - 1] == e.rho[irhop - 1])) {
+    const double gamp = lin(e.gam2, irhop), mp = lin(e.muc2, irhop), tkp = lin(e.tk2, irhop);
+    const double slope = 1.0 / (e.rho[irhop - 1] - e.rho[irho - 1]) * (rho - e.rho[irho - 1]);
+    gam = gam + (gamp - gam) * slope;
+    m = m + (mp - m) * slope;
+    tk = tk + (tkp - tk) * slope;
+  }
+}
+
+
 // Loads of the stage inputs: through the read-only path when the planes stay
 // unchanged for the whole launch (one launch per stage), from L2 (cg) in the
 // persistent batched kernel, whose other blocks write planes that this block
@@ -218,6 +259,7 @@ template <int STAGE>
 __device__ __forceinline__ Prim prim_ieee(double small_eps, double gm1, double gam, Cons c, double v1,
                                        double v2, double v3, int nsrc, bool need_c, int rs = 0) {
   Prim q;
+  q.g = gam;
   const bool is0 = stage_is0<STAGE>(rs);
   if (is0) apply_sources(c, nsrc, small_eps);
   q.d = c.d;
@@ -230,10 +272,12 @@ __device__ __forceinline__ Prim prim_ieee(double small_eps, double gm1, double g
   return q;
 }
 
-template <int STAGE, bool GRAV = false>
+template <int STAGE, bool GRAV = false, bool TAB = false>
 __device__ __forceinline__ Prim prim_of(const Geom& g, Raw r, unsigned& flags, int nsrc,
-                                        double dth, bool need_c = true, int rs = 0) {
+                                        double dth, bool need_c = true, int rs = 0,
+                                        const EosDev* eos = nullptr) {
   Prim q;
+  q.g = g.gam;
   if (STAGE == 0 && GRAV) {
     const SharedDiv qd(r.c.d);
     Cons c = r.c;
@@ -248,8 +292,22 @@ __device__ __forceinline__ Prim prim_of(const Geom& g, Raw r, unsigned& flags, i
     q.p = eos_pressure(q.d, c.E, v1, v2, v3, g.gm1, g.small_eps);
     // the sound speed enters only the lambdas of cells whose face states are built
     q.c = need_c ? sqrt(qd(q.p * g.gam)) : 0.0;
-  } else if (!prim_fast<STAGE>(g, r.c, r.v1, r.v2, r.v3, nsrc, need_c, q, rs)) {
-    q = prim_ieee<STAGE>(g.small_eps, g.gm1, g.gam, r.c, r.v1, r.v2, r.v3, nsrc, need_c, rs);
+  } else if (!prim_fast<STAGE>(g, r.c, r.v1, r.v2, r.v3, nsrc, need_c && !TAB, q, rs)) {
+    q = prim_ieee<STAGE>(g.small_eps, g.gm1, g.gam, r.c, r.v1, r.v2, r.v3, nsrc,
+                         need_c && !TAB, rs);
+  }
+  if (TAB) {
+    // state() with the tables (state.f90:60-79): eps from the energy and the
+    // velocity array state() reads (stage 0: m/rho, so the reconstruction's
+    // eps; stage 1: the stage-0 velocity), then p and gamma by get_gamma2
+    double eps = stage_is0<STAGE>(rs)
+                     ? q.e
+                     : fmax(r.c.E - kin_rho_u(q.d, r.v1, r.v2, r.v3), g.small_eps);
+    double tk, m, gam;
+    get_gamma2(*eos, eps, q.d, tk, m, gam);
+    q.p = (q.d * tk * g.rgas / m);
+    q.g = gam;
+    q.c = need_c ? sqrt(q.p * gam / q.d) : 0.0;
   }
   if (q.d < kLowRho) flags |= kFlagLowRho;
   if (fabs(q.u1) > g.vlimit || fabs(q.u2) > g.vlimit || fabs(q.u3) > g.vlimit)
@@ -268,15 +326,15 @@ __device__ __forceinline__ Prim prim_of(const Geom& g, Raw r, unsigned& flags, i
 //           sources still pending, then source(0) with the force, which kicks
 //           the momenta; state() then reads the velocity array of before the
 //           kick (main.f90:318-319 call state() before velocity()).
-template <int STAGE, bool GRAV = false, bool CG = false>
+template <int STAGE, bool GRAV = false, bool CG = false, bool TAB = false>
 __device__ __forceinline__ Prim load_prim(const StageArgs& a, const Geom& g, int x, int y, int z,
                                           unsigned& flags, int nsrc, double dth,
                                           bool need_c = true, int rs = 0) {
-  return prim_of<STAGE, GRAV>(g, load_raw<STAGE, GRAV, CG>(a, g, x, y, z, rs), flags, nsrc, dth,
-                              need_c, rs);
+  return prim_of<STAGE, GRAV, TAB>(g, load_raw<STAGE, GRAV, CG>(a, g, x, y, z, rs), flags, nsrc,
+                                   dth, need_c, rs, &a.eos);
 }
 
-template <bool POW2>
+template <bool POW2, bool TAB = false>
 __device__ __forceinline__ void dir_states(const Prim& m, const Prim& c, const Prim& p, double ud,
                                            double dt, double ds, double ids, FaceState& mi,
                                            FaceState& pl) {
@@ -286,10 +344,12 @@ __device__ __forceinline__ void dir_states(const Prim& m, const Prim& c, const P
   const double s3 = slope3(m.u3, c.u3, p.u3);
   const double sp = slope3(m.p, c.p, p.p);
   const double se = slope3(m.e, c.e, p.e);
-  muscl_states<POW2>(c, ud, sd, s1, s2, s3, sp, se, dt, ds, ids, mi, pl);
+  // the tabulated EOS's gamma (adindx), reconstructed like the others (flux.f90:293,350)
+  const double sg = TAB ? slope3(m.g, c.g, p.g) : 0.0;
+  muscl_states<POW2, TAB>(c, ud, sd, s1, s2, s3, sp, se, dt, ds, ids, mi, pl, sg);
 }
 
-template <int NP>
+template <int NP, int NPF = 7>
 __device__ __forceinline__ void put_prim(double* SP, int i, const Prim& q) {
   SP[0 * NP + i] = q.d;
   SP[1 * NP + i] = q.u1;
@@ -298,8 +358,9 @@ __device__ __forceinline__ void put_prim(double* SP, int i, const Prim& q) {
   SP[4 * NP + i] = q.p;
   SP[5 * NP + i] = q.e;
   SP[6 * NP + i] = q.c;
+  if (NPF == 8) SP[7 * NP + i] = q.g;
 }
-template <int NP>
+template <int NP, int NPF = 7>
 __device__ __forceinline__ Prim get_prim(const double* SP, int i) {
   Prim q;
   q.d = SP[0 * NP + i];
@@ -309,8 +370,10 @@ __device__ __forceinline__ Prim get_prim(const double* SP, int i) {
   q.p = SP[4 * NP + i];
   q.e = SP[5 * NP + i];
   q.c = SP[6 * NP + i];
+  if (NPF == 8) q.g = SP[7 * NP + i];
   return q;
 }
+template <int NSF = 6>
 __device__ __forceinline__ void put_fs(double* S, int n, int i, const FaceState& f) {
   S[0 * n + i] = f.d;
   S[1 * n + i] = f.u1;
@@ -318,7 +381,9 @@ __device__ __forceinline__ void put_fs(double* S, int n, int i, const FaceState&
   S[3 * n + i] = f.u3;
   S[4 * n + i] = f.p;
   S[5 * n + i] = f.e;
+  if (NSF == 7) S[6 * n + i] = f.g;
 }
+template <int NSF = 6>
 __device__ __forceinline__ FaceState get_fs(const double* S, int n, int i) {
   FaceState f;
   f.d = S[0 * n + i];
@@ -327,6 +392,7 @@ __device__ __forceinline__ FaceState get_fs(const double* S, int n, int i) {
   f.u3 = S[3 * n + i];
   f.p = S[4 * n + i];
   f.e = S[5 * n + i];
+  if (NSF == 7) f.g = S[6 * n + i];
   return f;
 }
 
@@ -334,6 +400,7 @@ __device__ __forceinline__ double warp_max(double v) {
   for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
   return v;
 }
+
 
 }  // namespace
 
@@ -378,6 +445,23 @@ __device__ __forceinline__ void epi_ieee(const Geom& g, const double n[5], doubl
   r0 = courant_rate<POW2>(n[0], pA, g.gam, u1, u2, u3, g.dx, g.dy, g.dz, g.idx, g.idy, g.idz);
 }
 
+// The same end of stage 1 with the tabulated EOS: the next step's state()
+// takes p and gamma from the tables (state.f90:60-79) with the velocity after
+// source(1), m/rho of the new cell, and courant.f90:20-21 uses that gamma.
+template <bool POW2>
+__device__ __forceinline__ void epi_tab(const Geom& g, const EosDev& eos, const double n[5],
+                                        double& u1, double& u2, double& u3, double& r0) {
+  u1 = n[1] / n[0];
+  u2 = n[2] / n[0];
+  u3 = n[3] / n[0];
+  const double E3 = source_energy(n[0], n[1], n[2], n[3], n[4], g.small_eps);
+  double eps = fmax(E3 - kin_rho_u(n[0], u1, u2, u3), g.small_eps);
+  double tk, m, gam;
+  get_gamma2(eos, eps, n[0], tk, m, gam);
+  const double p = (n[0] * tk * g.rgas / m);
+  r0 = courant_rate<POW2>(n[0], p, gam, u1, u2, u3, g.dx, g.dy, g.dz, g.idx, g.idy, g.idz);
+}
+
 // ------------------------------------------------------------------ stage kernel
 // One tile of one stage.  FULL: the tile is a whole TX x TY block of interior
 // columns, so its extents are compile-time constants.
@@ -390,13 +474,15 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
                                            double* red_rate, unsigned* red_flags, int rs = 0) {
   const bool is0 = stage_is0<STAGE>(rs);
   constexpr int TX = S::TX, TY = S::TY, NT = S::NT, PW = S::PW, NP = S::NP;
+  constexpr bool TAB = S::TAB;
+  constexpr int NPF = S::NPF, NSF = S::NSF;
   constexpr int NSX = S::NSX, NSY = S::NSY, NFX = S::NFX, NFY = S::NFY, NR0 = S::NR0;
-  double* SP = sm;                    // [7][TY+4][TX+4] primitives of the plane
-  double* SX = sm + NR0;              // [12][TY][TX+2] x states (minus 0..5, plus 6..11)
-  double* SY = SX + 12 * NSX;         // [12][TY+2][TX] y states
+  double* SP = sm;                    // [NPF][TY+4][TX+4] primitives of the plane
+  double* SX = sm + NR0;              // [2 NSF][TY][TX+2] x states (minus, then plus)
+  double* SY = SX + 2 * NSF * NSX;    // [2 NSF][TY+2][TX] y states
   double* FX = sm;                    // [5][TY][TX+1] x face fluxes (aliases SP)
   double* FY = sm + 5 * NFX;          // [5][TY+1][TX] y face fluxes
-  double* ZS = SY + 12 * NSY;         // [16][NT]: Fzm 0-4, Fzp 5-9, plus state 10-15
+  double* ZS = SY + 2 * NSF * NSY;    // [10 + NSF][NT]: Fzm 0-4, Fzp 5-9, plus state 10-
   const double dth = dt * kHalf;  // the sources' half step (main.f90:282,471)
 
   const int tid = threadIdx.x;
@@ -421,23 +507,24 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
 
   const int z0 = g.az0 + t.z0, z1 = g.az0 + t.z1;
   if (THREED && own) {
-    const Prim Pm2 = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z0 - 2, flags, nsrc, dth, true, rs);
-    const Prim Pm1 = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z0 - 1, flags, nsrc, dth, true, rs);
-    Pk = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z0, flags, nsrc, dth, true, rs);
-    Pk1 = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z0 + 1, flags, nsrc, dth, true, rs);
+    const Prim Pm2 = load_prim<STAGE, GRAV, CG, TAB>(a, g, gx, gy, z0 - 2, flags, nsrc, dth, true, rs);
+    const Prim Pm1 = load_prim<STAGE, GRAV, CG, TAB>(a, g, gx, gy, z0 - 1, flags, nsrc, dth, true, rs);
+    Pk = load_prim<STAGE, GRAV, CG, TAB>(a, g, gx, gy, z0, flags, nsrc, dth, true, rs);
+    Pk1 = load_prim<STAGE, GRAV, CG, TAB>(a, g, gx, gy, z0 + 1, flags, nsrc, dth, true, rs);
     FaceState mm, pm, m0;
     if (z0 - 1 < g.az0) {
       ghost_states(Pm1, mm, pm);
     } else {
-      dir_states<POW2>(Pm2, Pm1, Pk, Pm1.u3, dt, g.dz, idz, mm, pm);
+      dir_states<POW2, TAB>(Pm2, Pm1, Pk, Pm1.u3, dt, g.dz, idz, mm, pm);
     }
     FaceState plusk;
     double Fzm[5];
-    dir_states<POW2>(Pm1, Pk, Pk1, Pk.u3, dt, g.dz, idz, m0, plusk);
-    hll_flux<2>(pm, m0, g.gam, Fzm);
+    dir_states<POW2, TAB>(Pm1, Pk, Pk1, Pk.u3, dt, g.dz, idz, m0, plusk);
+    hll_flux<2, TAB>(pm, m0, g.gam, Fzm);
     for (int q = 0; q < 5; ++q) zs(q) = Fzm[q];
     zs(10) = plusk.d; zs(11) = plusk.u1; zs(12) = plusk.u2; zs(13) = plusk.u3;
     zs(14) = plusk.p; zs(15) = plusk.e;
+    if (TAB) zs(16) = plusk.g;
   }
 
   for (int z = (THREED ? z0 : g.az0 + t.z0); z < (THREED ? z1 : g.az0 + t.z1); ++z) {
@@ -467,11 +554,11 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
     FaceState mz1, pz1;
     if (own) {
       if (THREED) {
-        P2 = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z + 2, flags, nsrc, dth, true, rs);
+        P2 = load_prim<STAGE, GRAV, CG, TAB>(a, g, gx, gy, z + 2, flags, nsrc, dth, true, rs);
       } else {
-        Pk = load_prim<STAGE, GRAV, CG>(a, g, gx, gy, z, flags, nsrc, dth, true, rs);
+        Pk = load_prim<STAGE, GRAV, CG, TAB>(a, g, gx, gy, z, flags, nsrc, dth, true, rs);
       }
-      put_prim<NP>(SP, (ty + 2) * PW + (tx + 2), Pk);
+      put_prim<NP, NPF>(SP, (ty + 2) * PW + (tx + 2), Pk);
       if (is0) {
         // sources change only E, so this is m/rho of the step input
         const long long o = g.base + gx + (long long)gy * g.sy + (long long)z * g.sz;
@@ -500,21 +587,23 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
       const int fx = bx0 + cx, fy = by0 + cy;
       const bool near = cx >= -1 && cx <= w && cy >= -1 && cy <= h;
       const bool inner = fx >= g.ax0 && fx < g.ax1 && fy >= g.ay0 && fy < g.ay1;
-      const Prim q = load_prim<STAGE, GRAV, CG>(a, g, fx, fy, z, flags, nsrc, dth, near && inner, rs);
-      put_prim<NP>(SP, (cy + 2) * PW + (cx + 2), q);
+      const Prim q = load_prim<STAGE, GRAV, CG, TAB>(a, g, fx, fy, z, flags, nsrc, dth, near && inner, rs);
+      put_prim<NP, NPF>(SP, (cy + 2) * PW + (cx + 2), q);
     }
     if (THREED && own) {
       if (z + 1 >= g.az1) {
         ghost_states(Pk1, mz1, pz1);
       } else {
-        dir_states<POW2>(Pk, Pk1, P2, Pk1.u3, dt, g.dz, idz, mz1, pz1);
+        dir_states<POW2, TAB>(Pk, Pk1, P2, Pk1.u3, dt, g.dz, idz, mz1, pz1);
       }
-      const FaceState plusk{zs(10), zs(11), zs(12), zs(13), zs(14), zs(15)};
+      const FaceState plusk{zs(10), zs(11), zs(12), zs(13), zs(14), zs(15),
+                            TAB ? zs(16) : 0.0};
       double Fzp[5];
-      hll_flux<2>(plusk, mz1, g.gam, Fzp);
+      hll_flux<2, TAB>(plusk, mz1, g.gam, Fzp);
       for (int q = 0; q < 5; ++q) zs(5 + q) = Fzp[q];
       zs(10) = pz1.d; zs(11) = pz1.u1; zs(12) = pz1.u2; zs(13) = pz1.u3;
       zs(14) = pz1.p; zs(15) = pz1.e;
+      if (TAB) zs(16) = pz1.g;
     }
     __syncthreads();
 
@@ -528,32 +617,32 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         if (i >= nxs) continue;
         const int cy = i / (w + 2), cx = i % (w + 2) - 1;
         const int c = (cy + 2) * PW + (cx + 2);
-        const Prim q = get_prim<NP>(SP, c);
+        const Prim q = get_prim<NP, NPF>(SP, c);
         const int fx = bx0 + cx;
         if (fx < g.ax0 || fx >= g.ax1) {
           ghost_states(q, mi, pl);
         } else {
-          dir_states<POW2>(get_prim<NP>(SP, c - 1), q, get_prim<NP>(SP, c + 1), q.u1, dt, g.dx, g.idx, mi,
+          dir_states<POW2, TAB>(get_prim<NP, NPF>(SP, c - 1), q, get_prim<NP, NPF>(SP, c + 1), q.u1, dt, g.dx, g.idx, mi,
                            pl);
         }
         const int o = cy * (TX + 2) + (cx + 1);
-        put_fs(SX, NSX, o, mi);
-        put_fs(SX + 6 * NSX, NSX, o, pl);
+        put_fs<NSF>(SX, NSX, o, mi);
+        put_fs<NSF>(SX + NSF * NSX, NSX, o, pl);
       } else {
         const int k = i - nxs_w;
         const int cy = k / w - 1, cx = k % w;
         const int c = (cy + 2) * PW + (cx + 2);
-        const Prim q = get_prim<NP>(SP, c);
+        const Prim q = get_prim<NP, NPF>(SP, c);
         const int fy = by0 + cy;
         if (fy < g.ay0 || fy >= g.ay1) {
           ghost_states(q, mi, pl);
         } else {
-          dir_states<POW2>(get_prim<NP>(SP, c - PW), q, get_prim<NP>(SP, c + PW), q.u2, dt, g.dy, g.idy,
+          dir_states<POW2, TAB>(get_prim<NP, NPF>(SP, c - PW), q, get_prim<NP, NPF>(SP, c + PW), q.u2, dt, g.dy, g.idy,
                            mi, pl);
         }
         const int o = (cy + 1) * TX + cx;
-        put_fs(SY, NSY, o, mi);
-        put_fs(SY + 6 * NSY, NSY, o, pl);
+        put_fs<NSF>(SY, NSY, o, mi);
+        put_fs<NSF>(SY + NSF * NSY, NSY, o, pl);
       }
     }
     __syncthreads();
@@ -567,18 +656,18 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         if (i >= nxf) continue;
         const int cy = i / (w + 1), f = i % (w + 1);
         const int base = cy * (TX + 2);
-        const FaceState L = get_fs(SX + 6 * NSX, NSX, base + f);  // plus state of cell f-1
-        const FaceState R = get_fs(SX, NSX, base + f + 1);        // minus state of cell f
-        hll_flux<0>(L, R, g.gam, F);
+        const FaceState L = get_fs<NSF>(SX + NSF * NSX, NSX, base + f);  // plus state of cell f-1
+        const FaceState R = get_fs<NSF>(SX, NSX, base + f + 1);        // minus state of cell f
+        hll_flux<0, TAB>(L, R, g.gam, F);
         const int o = cy * (TX + 1) + f;
 #pragma unroll
         for (int q = 0; q < 5; ++q) FX[q * NFX + o] = F[q];
       } else {
         const int k = i - nxf_w;
         const int f = k / w, cx = k % w;
-        const FaceState L = get_fs(SY + 6 * NSY, NSY, f * TX + cx);
-        const FaceState R = get_fs(SY, NSY, (f + 1) * TX + cx);
-        hll_flux<1>(L, R, g.gam, F);
+        const FaceState L = get_fs<NSF>(SY + NSF * NSY, NSY, f * TX + cx);
+        const FaceState R = get_fs<NSF>(SY, NSY, (f + 1) * TX + cx);
+        hll_flux<1, TAB>(L, R, g.gam, F);
         const int o = f * TX + cx;
 #pragma unroll
         for (int q = 0; q < 5; ++q) FY[q * NFY + o] = F[q];
@@ -638,6 +727,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
           u1 = qn(n[1]);
           u2 = qn(n[2]);
           u3 = qn(n[3]);
+        } else if (TAB) {
+          epi_tab<POW2>(g, a.eos, n, u1, u2, u3, r0);
         } else if (!epi_fast<POW2>(g, n, u1, u2, u3, r0)) {
           epi_ieee<POW2>(g, n, u1, u2, u3, r0);
         }
@@ -711,10 +802,15 @@ template <>
 struct ShapeSel<1> {
   using type = Shape1;
 };
+template <>
+struct ShapeSel<2> {
+  using type = Shape2;
+};
 
 // PM: 1 = every box of the launch has power-of-two spacings (divisions by the
 // cell sizes are multiplications by exact reciprocals), 0 = otherwise (cdiv,
-// exact for any spacing).  SH: the tile shape (Shape0 or Shape1).
+// exact for any spacing).  SH: the tile shape (Shape0 or Shape1; Shape2 with the
+// tabulated EOS).
 template <int STAGE, int PM, bool THREED, bool GRAV = false, int SH = 0>
 __global__ void __launch_bounds__(NT, 65536 / (NT * 128)) k_stage(StageArgs a) {
   using S = typename ShapeSel<SH>::type;
@@ -994,11 +1090,17 @@ static cudaError_t launch_stage_g(int pm, bool threed, const StageArgs& a, int n
 }
 
 // a.G set: the step has a gravitational force (instances with the force terms,
-// tile shape 0 only: the batched path, the one that tunes the shape, has no force)
+// tile shape 0 only: the batched path, the one that tunes the shape, has no
+// force, and a grid with the tabulated EOS and a force runs the per-phase
+// kernels).  Shape 2: the tabulated EOS.
 template <int STAGE>
 static cudaError_t launch_stage_s(int pm, bool threed, const StageArgs& a, int ntiles,
                                   cudaStream_t s, int shape) {
-  if (a.G) return launch_stage_g<STAGE, true, 0>(pm, threed, a, ntiles, s);
+  if (a.G) {
+    if (shape != 0) return cudaErrorInvalidValue;
+    return launch_stage_g<STAGE, true, 0>(pm, threed, a, ntiles, s);
+  }
+  if (shape == 2) return launch_stage_g<STAGE, false, 2>(pm, threed, a, ntiles, s);
   return shape == 1 ? launch_stage_g<STAGE, false, 1>(pm, threed, a, ntiles, s)
                     : launch_stage_g<STAGE, false, 0>(pm, threed, a, ntiles, s);
 }
@@ -1011,7 +1113,10 @@ cudaError_t launch_stage(int stage, int pm, bool threed, const StageArgs& a, int
 }
 
 size_t stage_smem_bytes(int shape) {
-  return (shape == 1 ? Shape1::SMEM_DOUBLES : Shape0::SMEM_DOUBLES) * sizeof(double);
+  return (shape == 2   ? Shape2::SMEM_DOUBLES
+          : shape == 1 ? Shape1::SMEM_DOUBLES
+                       : Shape0::SMEM_DOUBLES) *
+         sizeof(double);
 }
 
 // ------------------------------------------------------------------ clock kernels
@@ -1092,46 +1197,6 @@ __device__ __forceinline__ bool is_ghost(const Geom& g, int x, int y, int z) {
 }
 
 // state.f90:29-87, fixed gamma
-// get_gamma2 (eos.f90:653-699): gamma, mu and T from the tables by the specific
-// internal energy eng = eps/rho, linear in eng within the density row irho, then
-// linear in rho towards row irho+1.  eps is clamped like the reference's.
-__device__ void get_gamma2(const EosDev& e, double& eps, double rho, double& tk, double& m,
-                           double& gam) {
-  int irho = min((int)((log10(rho * e.density_unit) - e.log_rho_low) / e.drho) + 1, e.neos_rho);
-  if (irho < 1) irho = 1;
-  int irhop = irho + 1;
-  if (irhop > e.neos_rho) irhop = irho;
-  const long long ne = e.neos;
-  auto at = [&](const double* t, int ie, int ir) { return t[(ie - 1) + (ir - 1) * ne]; };
-  double eng = eps / rho;
-  int ientry = (int)((log10(eng) - log10(at(e.eng2, 1, irho))) / e.deng[irho - 1]) + 1;
-  if (ientry > e.neos - 1) {
-    ientry = e.neos - 1;
-    eng = at(e.eng2, e.neos, irho);
-    eps = eng * rho;
-  }
-  if (ientry < 1 || eng < at(e.eng2, 1, irho)) {
-    ientry = 1;
-    eng = at(e.eng2, 1, irho);
-    eps = eng * rho;
-  }
-  auto lin = [&](const double* t, int ir) {
-    return at(t, ientry, ir) + (at(t, ientry + 1, ir) - at(t, ientry, ir)) /
-                                   (at(e.eng2, ientry + 1, ir) - at(e.eng2, ientry, ir)) *
-                                   (eng - at(e.eng2, ientry, ir));
-  };
-  gam = lin(e.gam2, irho);
-  m = lin(e.muc2, irho);
-  tk = lin(e.tk2, irho);
-  if (!(e.rho[irho - 1] == e.rho[irhop - 1])) {
-    const double gamp = lin(e.gam2, irhop), mp = lin(e.muc2, irhop), tkp = lin(e.tk2, irhop);
-    const double slope = 1.0 / (e.rho[irhop - 1] - e.rho[irho - 1]) * (rho - e.rho[irho - 1]);
-    gam = gam + (gamp - gam) * slope;
-    m = m + (mp - m) * slope;
-    tk = tk + (tkp - tk) * slope;
-  }
-}
-
 __global__ void k_phase_state(Geom g, PhaseArrays a, Ctrl* ctrl) {
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= g.ng) return;
@@ -1963,7 +2028,18 @@ int stage_blocks_per_sm(int stage, int pm, bool threed, int shape) {
   int nb = 0;
   const size_t smem = stage_smem_bytes(shape);
   const void* fn;
-  if (shape == 1) {
+  if (shape == 2) {
+    if (stage == 0)
+      fn = pm == 1 ? (threed ? (const void*)k_stage<0, 1, true, false, 2>
+                             : (const void*)k_stage<0, 1, false, false, 2>)
+                   : (threed ? (const void*)k_stage<0, 0, true, false, 2>
+                             : (const void*)k_stage<0, 0, false, false, 2>);
+    else
+      fn = pm == 1 ? (threed ? (const void*)k_stage<1, 1, true, false, 2>
+                             : (const void*)k_stage<1, 1, false, false, 2>)
+                   : (threed ? (const void*)k_stage<1, 0, true, false, 2>
+                             : (const void*)k_stage<1, 0, false, false, 2>);
+  } else if (shape == 1) {
     if (stage == 0)
       fn = pm == 1 ? (threed ? (const void*)k_stage<0, 1, true, false, 1>
                              : (const void*)k_stage<0, 1, false, false, 1>)

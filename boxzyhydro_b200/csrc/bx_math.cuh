@@ -17,14 +17,16 @@ constexpr double kTheta = 1.25;    // SLOPE_THETA, Makefile:20 / utils.f90:739
 constexpr double kLowRho = 1e-4;   // low-density EOS branch, state.f90:52
 
 // Primitive set used by reconstruction: rho, u1..3, p, eps (internal energy
-// per volume), plus the sound speed c = sqrt(p*gamma/rho) of the cell.
+// per volume), plus the sound speed c = sqrt(p*gamma/rho) of the cell and, with
+// the tabulated EOS, the cell's gamma (adindx), reconstructed like the others.
 struct Prim {
-  double d, u1, u2, u3, p, e, c;
+  double d, u1, u2, u3, p, e, c, g;
 };
 
-// Reconstructed face state (one side of one face); gamma is constant.
+// Reconstructed face state (one side of one face); g: gamma, with the
+// tabulated EOS only (fixed gamma: the grid's).
 struct FaceState {
-  double d, u1, u2, u3, p, e;
+  double d, u1, u2, u3, p, e, g;
 };
 
 // genminmod (utils.f90:696-707) of (theta*d1, half*d2, theta*d3) where
@@ -143,10 +145,10 @@ __device__ __forceinline__ double courant_rate_q(const struct SharedDiv& qd, dou
 // lambda_p = max(u_d+c,0)*dt/ds, lambda_m = min(u_d-c,0)*dt/ds,
 // q- = q + half*(-1-lambda_m)*s, q+ = q + half*(1-lambda_p)*s.
 // The transverse terms of flux.f90:391-479 add zero and are omitted.
-template <bool POW2>
+template <bool POW2, bool TAB = false>
 BX_HD void muscl_states(const Prim& q, double ud, double sd, double su1, double su2,
                         double su3, double sp, double se, double dt, double ds, double ids,
-                        FaceState& mi, FaceState& pl) {
+                        FaceState& mi, FaceState& pl, double sg = 0.0) {
   double lp = fmax(ud + q.c, 0.0) * dt;
   double lm = fmin(ud - q.c, 0.0) * dt;
   if (POW2) {
@@ -170,12 +172,16 @@ BX_HD void muscl_states(const Prim& q, double ud, double sd, double su1, double 
   pl.d = q.d + hp * sd;
   mi.e = q.e + hm * se;
   pl.e = q.e + hp * se;
+  if (TAB) {
+    mi.g = q.g + hm * sg;
+    pl.g = q.g + hp * sg;
+  }
 }
 
 // Face state of a ghost cell: its slopes are zero (flux.f90:53-54), so both
 // sides equal the cell values.
 BX_HD void ghost_states(const Prim& q, FaceState& mi, FaceState& pl) {
-  mi.d = q.d; mi.u1 = q.u1; mi.u2 = q.u2; mi.u3 = q.u3; mi.p = q.p; mi.e = q.e;
+  mi.d = q.d; mi.u1 = q.u1; mi.u2 = q.u2; mi.u3 = q.u3; mi.p = q.p; mi.e = q.e; mi.g = q.g;
   pl = mi;
 }
 
@@ -255,15 +261,16 @@ __device__ __forceinline__ double source_energy_q(const SharedDiv& qd, double m1
 // the cell on the low side (L) and the minus state of the cell on the high side
 // (R): get_fluxes + flux_hll, flux.f90:504-590.  gl=gr=gamma.
 // Returns a nonzero code when ap+am == 0 (the reference divides by zero).
-template <int DIR>
+template <int DIR, bool TAB = false>
 BX_HD void hll_flux(const FaceState& L, const FaceState& R, double gam, double F[5]) {
   // The wave speeds come first, then each component from its own state and
   // flux terms, so only the two face states and the speeds stay live across
   // the components (every expression is the reference's, in its order).
   const double vl = DIR == 0 ? L.u1 : (DIR == 1 ? L.u2 : L.u3);
   const double vr = DIR == 0 ? R.u1 : (DIR == 1 ? R.u2 : R.u3);
-  const double cr = sqrt(gam * R.p / R.d);
-  const double cl = sqrt(gam * L.p / L.d);
+  // gl, gr: the reconstructed gammas with the tabulated EOS (flux.f90:507,521)
+  const double cr = sqrt((TAB ? R.g : gam) * R.p / R.d);
+  const double cl = sqrt((TAB ? L.g : gam) * L.p / L.d);
   const double ap = fmax(fmax(0.0, vr + cr), vl + cl);
   const double am = fmax(fmax(0.0, -(vr - cr)), -(vl - cl));
   const double apam = ap * am;
