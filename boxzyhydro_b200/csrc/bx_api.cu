@@ -570,7 +570,7 @@ int bx_set_eos_table(bx_handle* h, const bx_eos_table* t) {
   const long long n2 = (long long)t->neos * t->neos_rho, nr = t->neos_rho;
   cudaFree(h->d_eos);
   h->d_eos = nullptr;
-  CK(dalloc((void**)&h->d_eos, (4 * n2 + 2 * nr) * sizeof(double)));
+  CK(dalloc((void**)&h->d_eos, (4 * n2 + 3 * nr) * sizeof(double)));
   const double* src[4] = {t->eng_table2, t->gamma_table2, t->muc_table2, t->tk_table2};
   for (int k = 0; k < 4; ++k)
     CK(cudaMemcpy(h->d_eos + k * n2, src[k], n2 * sizeof(double), cudaMemcpyHostToDevice));
@@ -594,6 +594,9 @@ int bx_set_eos_table(bx_handle* h, const bx_eos_table* t) {
   e.tk2 = h->d_eos + 3 * n2;
   e.rho = h->d_eos + 4 * n2;
   e.deng = h->d_eos + 4 * n2 + nr;
+  e.log_eng1 = h->d_eos + 4 * n2 + 2 * nr;
+  CK(eos_log_rows(e.eng2, e.neos, (int)nr, h->d_eos + 4 * n2 + 2 * nr, h->stream));
+  CK(cudaStreamSynchronize(h->stream));
   // the fused kernels read the tables from here on (not while a force is set)
   h->eligible = h->tab_fusable && !h->gforce_set;
   return BX_OK;

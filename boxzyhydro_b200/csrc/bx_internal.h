@@ -161,7 +161,12 @@ struct EosDev {
   double log_rho_low, drho, density_unit, tk_bgrnd;
   const double *eng2, *gam2, *muc2, *tk2;  // (neos, neos_rho), neos fastest
   const double *rho, *deng;                // (neos_rho)
+  const double* log_eng1;                  // (neos_rho): log10 of each row's first energy
 };
+// log10 of the first energy of each density row (the value get_gamma2 needs,
+// computed once with the same device function)
+cudaError_t eos_log_rows(const double* eng2, long long neos, int nr, double* out,
+                         cudaStream_t s);
 
 // ---- kernels (bx_kernels.cu)
 struct StageArgs {

@@ -59,7 +59,8 @@ __device__ void get_gamma2(const EosDev& e, double& eps, double rho, double& tk,
   const long long ne = e.neos;
   auto at = [&](const double* t, int ie, int ir) { return t[(ie - 1) + (ir - 1) * ne]; };
   double eng = eps / rho;
-  int ientry = (int)((log10(eng) - log10(at(e.eng2, 1, irho))) / e.deng[irho - 1]) + 1;
+  // log10 of the row's first energy: precomputed with the same device log10
+  int ientry = (int)((log10(eng) - e.log_eng1[irho - 1]) / e.deng[irho - 1]) + 1;
   if (ientry > e.neos - 1) {
     ientry = e.neos - 1;
     eng = at(e.eng2, e.neos, irho);
@@ -70,16 +71,21 @@ __device__ void get_gamma2(const EosDev& e, double& eps, double rho, double& tk,
     eng = at(e.eng2, 1, irho);
     eps = eng * rho;
   }
-  auto lin = [&](const double* t, int ir) {
-    return at(t, ientry, ir) + (at(t, ientry + 1, ir) - at(t, ientry, ir)) /
-                                   (at(e.eng2, ientry + 1, ir) - at(e.eng2, ientry, ir)) *
-                                   (eng - at(e.eng2, ientry, ir));
+  // t(ientry) + (t(ientry+1) - t(ientry)) / (eng(ientry+1) - eng(ientry)) *
+  // (eng - eng(ientry)) for gamma, mu and T of density row ir: the three
+  // quotients share the denominator, so one exact shared reciprocal
+  auto lin3 = [&](int ir, double& g3, double& m3, double& t3) {
+    const double e0 = at(e.eng2, ientry, ir);
+    const SharedDiv q(at(e.eng2, ientry + 1, ir) - e0);
+    const double de = eng - e0;
+    g3 = at(e.gam2, ientry, ir) + q(at(e.gam2, ientry + 1, ir) - at(e.gam2, ientry, ir)) * de;
+    m3 = at(e.muc2, ientry, ir) + q(at(e.muc2, ientry + 1, ir) - at(e.muc2, ientry, ir)) * de;
+    t3 = at(e.tk2, ientry, ir) + q(at(e.tk2, ientry + 1, ir) - at(e.tk2, ientry, ir)) * de;
   };
-  gam = lin(e.gam2, irho);
-  m = lin(e.muc2, irho);
-  tk = lin(e.tk2, irho);
+  lin3(irho, gam, m, tk);
   if (!(e.rho[irho - 1] == e.rho[irhop - 1])) {
-    const double gamp = lin(e.gam2, irhop), mp = lin(e.muc2, irhop), tkp = lin(e.tk2, irhop);
+    double gamp, mp, tkp;
+    lin3(irhop, gamp, mp, tkp);
     const double slope = 1.0 / (e.rho[irhop - 1] - e.rho[irho - 1]) * (rho - e.rho[irho - 1]);
     gam = gam + (gamp - gam) * slope;
     m = m + (mp - m) * slope;
@@ -1868,6 +1874,15 @@ cudaError_t fused_to_phase(const Geom& g, const double* X, int nsrc, PhaseArrays
   if (nghost > 0)
     k_fill_resolved<<<nblk(nghost), PB, 0, s>>>(nghost, dst, src2, sgn2, a.cons, g.ng);
   k_f2p_prims<<<nblk(g.ng), PB, 0, s>>>(g, a);
+  return cudaGetLastError();
+}
+__global__ void k_log10_rows(const double* eng2, long long neos, int nr, double* out) {
+  const int r = blockIdx.x * blockDim.x + threadIdx.x;
+  if (r < nr) out[r] = log10(eng2[(long long)r * neos]);
+}
+cudaError_t eos_log_rows(const double* eng2, long long neos, int nr, double* out,
+                         cudaStream_t s) {
+  k_log10_rows<<<(nr + 127) / 128, 128, 0, s>>>(eng2, neos, nr, out);
   return cudaGetLastError();
 }
 __global__ void k_fill_const(double* a, long long n, double v) {
