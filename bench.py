@@ -185,14 +185,16 @@ def parity_full_size(st, steps):
 
 def physics_arm(args, rank, world, local):
     """The rows beyond the plain step on the turbulent box: angular-momentum
-    fluxing (fluxangmom, yoffset 0.25), the tabulated EOS (H2STAT >= 0 with
-    synthetic ideal-gas tables of the eos module's layout) and the gravity
+    fluxing (fluxangmom, yoffset 0.75: the rotation axis a quarter box below
+    the box; with the axis inside the box the near-axis pressure terms push
+    velocities past vlimit within a few steps and the limiter's steps run on
+    the per-phase kernels, in the oracle too), the tabulated EOS (H2STAT >= 0
+    with synthetic ideal-gas tables of the eos module's layout) and the gravity
     coupling (a softened point-mass potential handed over from page-locked host
     memory before every step, its upload and calc_gforce inside the timed
-    region).  flux_ang runs on the per-phase kernels, the tabulated EOS and the
-    gravity coupling on the fused stage kernels (the line gives each variant's
-    path).  Device-timed steps and the oracle with the same physics on a
-    bounded sample of the host cores."""
+    region).  All three run on the fused stage kernels (the line gives each
+    variant's path and the status bits of its steps).  Device-timed steps and
+    the oracle with the same physics on a bounded sample of the host cores."""
     import dataclasses
 
     import numpy as np
@@ -212,7 +214,7 @@ def physics_arm(args, rank, world, local):
     phi[:] = -0.1 / np.sqrt(x * x + y * y + z * z + 0.01)
     tab = synthetic_table()
     variants = {
-        "fluxang": dict(params=dataclasses.replace(hp0, fluxangmom=True, yoffset=0.25)),
+        "fluxang": dict(params=dataclasses.replace(hp0, fluxangmom=True, yoffset=0.75)),
         "eostable": dict(params=dataclasses.replace(hp0, h2stat=1), table=tab),
         "gravity": dict(params=hp0, phi=phi),
     }

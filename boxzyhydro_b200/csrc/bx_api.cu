@@ -83,6 +83,19 @@ static std::vector<Tile> make_tiles(const Geom& g, int box, int slots, int zc_fo
 
 static int create_handle(const bx_params* params, bx_handle** out, bool lean);
 
+// whether the steps may run on the fused stage kernels: a grid they take, and
+// the physics they have: fixed gamma or the tabulated EOS with its tables set
+// and nz != 1 (the scale-height branch reads the previous gamma), flux_ang only
+// with fixed gamma, and the tabulated EOS or flux_ang without a force (the
+// force instances have the fixed-gamma tile shape)
+static void update_eligible(bx_handle* h) {
+  const bx_params& P = h->P;
+  bool ok = h->fusable;
+  if (P.h2stat >= 0) ok = ok && !P.fluxangmom && P.nz != 1 && h->d_eos != nullptr;
+  if (h->shape != 0) ok = ok && !h->gforce_set;
+  h->eligible = ok;
+}
+
 extern "C" {
 
 const char* bx_version(void) { return "boxzy-b200 1.0 (sm_100a, FP64)"; }
@@ -124,14 +137,9 @@ static int create_handle(const bx_params* params, bx_handle** out, bool lean) {
   h->P = P;
   fill_geom(P, h->g);
   build_ghost_tables(P, h->T);
-  // flux_ang runs on the per-phase kernels only; the tabulated EOS takes the
-  // fused kernels (tile shape 2) once its tables are set, except with nz == 1,
-  // whose scale-height branch reads the previous gamma
-  const bool fusable = h->T.resolved2 && h->T.face_rule_ok &&
-                       !(P.flags & BX_FLAG_PHASE_ONLY) && !P.fluxangmom;
-  h->eligible = fusable && P.h2stat == -1;
-  h->tab_fusable = fusable && P.h2stat >= 0 && P.nz != 1;
-  h->shape = P.h2stat >= 0 ? 2 : 0;
+  h->fusable = h->T.resolved2 && h->T.face_rule_ok && !(P.flags & BX_FLAG_PHASE_ONLY);
+  h->shape = P.h2stat >= 0 ? 2 : P.fluxangmom ? 3 : 0;
+  update_eligible(h);
   const long long ng = h->g.ng;
   h->nghost = (int)h->T.dst.size();
   auto fail = [&](int code) {
@@ -524,18 +532,14 @@ int bx_save_cons_old(bx_handle* h) {
   return BX_OK;
 }
 
-// a grid with the tabulated EOS takes the fused kernels only without a force
-// (their force instances have the fixed-gamma tile shape): the state goes to
-// the reference arrays when a force is set, and back with the next clean step
-// once it is cleared
+// a grid with the tabulated EOS or flux_ang takes the fused kernels only
+// without a force (their force instances have the fixed-gamma tile shape): the
+// state goes to the reference arrays when a force is set, and back with the
+// next clean step once it is cleared
 static int tab_force_switch(bx_handle* h, bool force) {
-  if (!h->g.tab) return BX_OK;
-  if (force) {
+  if (h->shape == 0) return BX_OK;
+  if (force && h->mode == 1)
     if (int r = to_phase(h)) return r;
-    h->eligible = false;
-  } else {
-    h->eligible = h->tab_fusable && h->d_eos != nullptr;
-  }
   return BX_OK;
 }
 
@@ -545,6 +549,7 @@ int bx_set_gforce(bx_handle* h, const double* gforce) {
   if (int r = tab_force_switch(h, gforce != nullptr)) return r;
   if (!gforce) {
     h->gforce_set = false;
+    update_eligible(h);
     CK(cudaStreamSynchronize(h->stream));
     cudaFree(h->pa.gforce);
     h->pa.gforce = nullptr;
@@ -557,6 +562,7 @@ int bx_set_gforce(bx_handle* h, const double* gforce) {
   CK(aos_to_soa(tmp, h->pa.gforce, n, 3, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   h->gforce_set = true;
+  update_eligible(h);
   return BX_OK;
 }
 
@@ -598,7 +604,7 @@ int bx_set_eos_table(bx_handle* h, const bx_eos_table* t) {
   CK(eos_log_rows(e.eng2, e.neos, (int)nr, h->d_eos + 4 * n2 + 2 * nr, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   // the fused kernels read the tables from here on (not while a force is set)
-  h->eligible = h->tab_fusable && !h->gforce_set;
+  update_eligible(h);
   return BX_OK;
 }
 
@@ -613,6 +619,7 @@ int bx_set_phi(bx_handle* h, const double* phi) {
   CK(phase_calc_gforce(h->g, tmp, h->pa.gforce, h->stream));
   CK(cudaStreamSynchronize(h->stream));
   h->gforce_set = true;
+  update_eligible(h);
   return BX_OK;
 }
 
@@ -1002,7 +1009,7 @@ int bx_step_host(bx_handle* h, const double* cons_in, double* cons_out, double e
   if (ran) *ran = 0;
   if (!cons_in || !cons_out) return set_err(h, BX_ERR_ARG, "cons_in and cons_out are required");
   if (!h->pa.cons) return set_err(h, BX_ERR_STATE, "the handle holds no state (lean handle)");
-  if (!h->eligible || h->g.tab) {
+  if (!h->eligible || h->shape != 0) {
     // not on the fused path: the three calls it stands for
     if (int r = bx_upload_conserved(h, cons_in)) return r;
     if (int r = bx_step(h, endtime, ran)) return r;

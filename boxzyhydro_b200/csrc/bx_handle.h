@@ -39,9 +39,11 @@ struct bx_handle {
   // (kept in pa.cons_old's fourth plane) is the one to give back
   bool p_saved = false;
   bool eligible = false;
-  // the grid would take the fused kernels with the tabulated EOS (tile shape
-  // 2): eligible turns on once the tables are set, and off while a force is set
-  bool tab_fusable = false;
+  // the grid's ghost plan and flags admit the fused kernels; eligible adds the
+  // physics: with the tabulated EOS (tile shape 2) once the tables are set and
+  // nz != 1, with the tabulated EOS or flux_ang (shape 3) not while a force is
+  // set (update_eligible)
+  bool fusable = false;
   int shape = 0;  // stage-kernel tile shape of the single-grid launches
   bool gforce_set = false;
   uint32_t status = 0;

@@ -100,43 +100,49 @@ static_assert(TX * TY <= NT && NT % 32 == 0, "tile larger than the block");
 // primitives of the tile plus a two-cell halo, aliased with the x/y face
 // fluxes; x and y face states; per-thread z-pipeline slots).  Shape 0 is the
 // single-grid path's (TX x TY); the batched path's autotuner may pick shape 1.
-template <int TX_, int TY_, bool TAB_ = false>
+template <int TX_, int TY_, int MODE_ = 0>
 struct TileShape {
   static constexpr int TX = TX_, TY = TY_;
   static constexpr int NT = BX_NT;
-  // TAB: the tabulated EOS, whose gamma is a reconstructed primitive (eight
-  // primitive fields, seven per face state)
-  static constexpr bool TAB = TAB_;
-  static constexpr int NPF = TAB ? 8 : 7;    // primitive fields
-  static constexpr int NSF = TAB ? 7 : 6;    // face-state fields
+  // MODE 1 (TAB): the tabulated EOS, whose gamma is a reconstructed primitive;
+  // MODE 2 (ANG): angular-momentum fluxing, whose radial and angular momenta
+  // are reconstructed primitives and whose x/y face fluxes of the two momentum
+  // components depend on the updated cell (two versions per face)
+  static constexpr bool TAB = MODE_ == 1, ANG = MODE_ == 2;
+  static constexpr int NPF = TAB ? 8 : ANG ? 9 : 7;  // primitive fields
+  static constexpr int NSF = TAB ? 7 : ANG ? 8 : 6;  // face-state fields
+  static constexpr int NFQ = ANG ? 7 : 5;            // x/y face-flux quantities
+  static constexpr int NOWN = TX * TY;               // threads with a column
   static constexpr int PW = TX + 4;          // prim plane width (x halo 2)
   static constexpr int NP = (TY + 4) * PW;   // prim plane cells
   static constexpr int NSX = TY * (TX + 2);  // x-state cells
   static constexpr int NSY = (TY + 2) * TX;  // y-state cells
   static constexpr int NFX = TY * (TX + 1);  // x faces
   static constexpr int NFY = (TY + 1) * TX;  // y faces
-  // per-thread z-pipeline slots (3-D): the z flux below and above the own cell
+  // per-column z-pipeline slots (3-D): the z flux below and above the own cell
   // (5 + 5) and the plus z-state carried to the next plane (NSF), kept in
   // shared memory so the x/y phases have the registers
   static constexpr int NZS = 10 + NSF;
   // the face fluxes of the face and update phases alias the primitives
-  static constexpr int NR0 = (NPF * NP > 5 * (NFX + NFY)) ? NPF * NP : 5 * (NFX + NFY);
-  static constexpr int SMEM_DOUBLES = NR0 + 2 * NSF * NSX + 2 * NSF * NSY + NZS * NT;
+  static constexpr int NR0 = (NPF * NP > NFQ * (NFX + NFY)) ? NPF * NP : NFQ * (NFX + NFY);
+  static constexpr int SMEM_DOUBLES = NR0 + 2 * NSF * NSX + 2 * NSF * NSY + NZS * NOWN;
   static_assert(TX * TY <= NT && NT % 32 == 0, "tile larger than the block");
   static_assert(4 * (TX + TY) <= NT, "one halo cell per thread and plane at most");
 };
 using Shape0 = TileShape<TX, TY>;
 using Shape1 = TileShape<16, 16>;
-// the tabulated EOS (single grids only): 32 x 6 columns, so the larger
-// primitive and face-state sets still fit two blocks per SM
-using Shape2 = TileShape<32, 6, true>;
+// the tabulated EOS and angular-momentum fluxing (single grids only): 32 x 6
+// columns, so the larger primitive and face-state sets still fit two blocks
+// per SM
+using Shape2 = TileShape<32, 6, 1>;
+using Shape3 = TileShape<32, 6, 2>;
 constexpr int kNumShapes = 2;  // the shapes the batched autotuner chooses among
 // the x and y extents of tile shape `shape`
 inline int shape_tx(int shape) {
-  return shape == 2 ? Shape2::TX : shape == 1 ? Shape1::TX : Shape0::TX;
+  return shape == 3 ? Shape3::TX : shape == 2 ? Shape2::TX : shape == 1 ? Shape1::TX : Shape0::TX;
 }
 inline int shape_ty(int shape) {
-  return shape == 2 ? Shape2::TY : shape == 1 ? Shape1::TY : Shape0::TY;
+  return shape == 3 ? Shape3::TY : shape == 2 ? Shape2::TY : shape == 1 ? Shape1::TY : Shape0::TY;
 }
 
 // ghost-fill tables: per ghost (index order), destination cell, source cell and

@@ -332,15 +332,40 @@ __device__ __forceinline__ Prim prim_of(const Geom& g, Raw r, unsigned& flags, i
 //           sources still pending, then source(0) with the force, which kicks
 //           the momenta; state() then reads the velocity array of before the
 //           kick (main.f90:318-319 call state() before velocity()).
-template <int STAGE, bool GRAV = false, bool CG = false, bool TAB = false>
+// the centre of cell (ix, iy) in the x-y plane (flux_ang.f90:44-46 and
+// :571-573, as cell_xy), and its distance from the z axis
+__device__ __forceinline__ void cell_xyr(const Geom& g, int ix, int iy, double& x, double& y,
+                                         double& r) {
+  x = g.dx * ((double)(ix + 1) - ((double)g.nx + 1.0) / 2.0);
+  y = g.dy * ((double)(iy + 1) - ((double)g.ny + 1.0) / 2.0);
+  r = sqrt(x * x + y * y);
+}
+
+// (m1, m2) -> (radial momentum, angular momentum) about the z axis through
+// (0, -yoffset) at cell (ix, iy) (flux_ang.f90:44-62)
+__device__ __forceinline__ void ang_to(const Geom& g, int ix, int iy, double m1, double m2,
+                                       double& rm, double& am) {
+  double x, y, r;
+  cell_xyr(g, ix, iy, x, y, r);
+  y = y + g.yoff;
+  r = sqrt(x * x + y * y);
+  rm = (m1 * x + m2 * y) / r;
+  am = x * m2 - y * m1;
+}
+
+template <int STAGE, bool GRAV = false, bool CG = false, bool TAB = false, bool ANG = false>
 __device__ __forceinline__ Prim load_prim(const StageArgs& a, const Geom& g, int x, int y, int z,
                                           unsigned& flags, int nsrc, double dth,
                                           bool need_c = true, int rs = 0) {
-  return prim_of<STAGE, GRAV, TAB>(g, load_raw<STAGE, GRAV, CG>(a, g, x, y, z, rs), flags, nsrc,
-                                   dth, need_c, rs, &a.eos);
+  const Raw r = load_raw<STAGE, GRAV, CG>(a, g, x, y, z, rs);
+  Prim q = prim_of<STAGE, GRAV, TAB>(g, r, flags, nsrc, dth, need_c, rs, &a.eos);
+  // with flux_ang the momenta reconstructed are the transformed ones (the
+  // sources leave the momenta alone)
+  if (ANG) ang_to(g, x, y, r.c.m1, r.c.m2, q.rm, q.am);
+  return q;
 }
 
-template <bool POW2, bool TAB = false>
+template <bool POW2, bool TAB = false, bool ANG = false>
 __device__ __forceinline__ void dir_states(const Prim& m, const Prim& c, const Prim& p, double ud,
                                            double dt, double ds, double ids, FaceState& mi,
                                            FaceState& pl) {
@@ -352,7 +377,10 @@ __device__ __forceinline__ void dir_states(const Prim& m, const Prim& c, const P
   const double se = slope3(m.e, c.e, p.e);
   // the tabulated EOS's gamma (adindx), reconstructed like the others (flux.f90:293,350)
   const double sg = TAB ? slope3(m.g, c.g, p.g) : 0.0;
-  muscl_states<POW2, TAB>(c, ud, sd, s1, s2, s3, sp, se, dt, ds, ids, mi, pl, sg);
+  // flux_ang's transformed momenta (flux_ang.f90:301-345)
+  const double srm = ANG ? slope3(m.rm, c.rm, p.rm) : 0.0;
+  const double sam = ANG ? slope3(m.am, c.am, p.am) : 0.0;
+  muscl_states<POW2, TAB, ANG>(c, ud, sd, s1, s2, s3, sp, se, dt, ds, ids, mi, pl, sg, srm, sam);
 }
 
 template <int NP, int NPF = 7>
@@ -365,6 +393,10 @@ __device__ __forceinline__ void put_prim(double* SP, int i, const Prim& q) {
   SP[5 * NP + i] = q.e;
   SP[6 * NP + i] = q.c;
   if (NPF == 8) SP[7 * NP + i] = q.g;
+  if (NPF == 9) {
+    SP[7 * NP + i] = q.rm;
+    SP[8 * NP + i] = q.am;
+  }
 }
 template <int NP, int NPF = 7>
 __device__ __forceinline__ Prim get_prim(const double* SP, int i) {
@@ -377,6 +409,10 @@ __device__ __forceinline__ Prim get_prim(const double* SP, int i) {
   q.e = SP[5 * NP + i];
   q.c = SP[6 * NP + i];
   if (NPF == 8) q.g = SP[7 * NP + i];
+  if (NPF == 9) {
+    q.rm = SP[7 * NP + i];
+    q.am = SP[8 * NP + i];
+  }
   return q;
 }
 template <int NSF = 6>
@@ -388,6 +424,10 @@ __device__ __forceinline__ void put_fs(double* S, int n, int i, const FaceState&
   S[4 * n + i] = f.p;
   S[5 * n + i] = f.e;
   if (NSF == 7) S[6 * n + i] = f.g;
+  if (NSF == 8) {
+    S[6 * n + i] = f.rm;
+    S[7 * n + i] = f.am;
+  }
 }
 template <int NSF = 6>
 __device__ __forceinline__ FaceState get_fs(const double* S, int n, int i) {
@@ -399,6 +439,10 @@ __device__ __forceinline__ FaceState get_fs(const double* S, int n, int i) {
   f.p = S[4 * n + i];
   f.e = S[5 * n + i];
   if (NSF == 7) f.g = S[6 * n + i];
+  if (NSF == 8) {
+    f.rm = S[6 * n + i];
+    f.am = S[7 * n + i];
+  }
   return f;
 }
 
@@ -480,15 +524,15 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
                                            double* red_rate, unsigned* red_flags, int rs = 0) {
   const bool is0 = stage_is0<STAGE>(rs);
   constexpr int TX = S::TX, TY = S::TY, NT = S::NT, PW = S::PW, NP = S::NP;
-  constexpr bool TAB = S::TAB;
-  constexpr int NPF = S::NPF, NSF = S::NSF;
+  constexpr bool TAB = S::TAB, ANG = S::ANG;
+  constexpr int NPF = S::NPF, NSF = S::NSF, NFQ = S::NFQ, NOWN = S::NOWN;
   constexpr int NSX = S::NSX, NSY = S::NSY, NFX = S::NFX, NFY = S::NFY, NR0 = S::NR0;
   double* SP = sm;                    // [NPF][TY+4][TX+4] primitives of the plane
   double* SX = sm + NR0;              // [2 NSF][TY][TX+2] x states (minus, then plus)
   double* SY = SX + 2 * NSF * NSX;    // [2 NSF][TY+2][TX] y states
-  double* FX = sm;                    // [5][TY][TX+1] x face fluxes (aliases SP)
-  double* FY = sm + 5 * NFX;          // [5][TY+1][TX] y face fluxes
-  double* ZS = SY + 2 * NSF * NSY;    // [10 + NSF][NT]: Fzm 0-4, Fzp 5-9, plus state 10-
+  double* FX = sm;                    // [NFQ][TY][TX+1] x face fluxes (aliases SP)
+  double* FY = sm + NFQ * NFX;        // [NFQ][TY+1][TX] y face fluxes
+  double* ZS = SY + 2 * NSF * NSY;    // [10 + NSF][NOWN]: Fzm 0-4, Fzp 5-9, plus state 10-
   const double dth = dt * kHalf;  // the sources' half step (main.f90:282,471)
 
   const int tid = threadIdx.x;
@@ -509,28 +553,36 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
 
   // z pipeline of the own column (3-D grids)
   Prim Pk, Pk1;
-  auto zs = [&](int k) -> double& { return ZS[k * NT + threadIdx.x]; };
+  // (columns only: the threads with a column are 0 .. NOWN-1)
+  auto zs = [&](int k) -> double& { return ZS[k * NOWN + threadIdx.x]; };
 
   const int z0 = g.az0 + t.z0, z1 = g.az0 + t.z1;
   if (THREED && own) {
-    const Prim Pm2 = load_prim<STAGE, GRAV, CG, TAB>(a, g, gx, gy, z0 - 2, flags, nsrc, dth, true, rs);
-    const Prim Pm1 = load_prim<STAGE, GRAV, CG, TAB>(a, g, gx, gy, z0 - 1, flags, nsrc, dth, true, rs);
-    Pk = load_prim<STAGE, GRAV, CG, TAB>(a, g, gx, gy, z0, flags, nsrc, dth, true, rs);
-    Pk1 = load_prim<STAGE, GRAV, CG, TAB>(a, g, gx, gy, z0 + 1, flags, nsrc, dth, true, rs);
+    const Prim Pm2 = load_prim<STAGE, GRAV, CG, TAB, ANG>(a, g, gx, gy, z0 - 2, flags, nsrc, dth, true, rs);
+    const Prim Pm1 = load_prim<STAGE, GRAV, CG, TAB, ANG>(a, g, gx, gy, z0 - 1, flags, nsrc, dth, true, rs);
+    Pk = load_prim<STAGE, GRAV, CG, TAB, ANG>(a, g, gx, gy, z0, flags, nsrc, dth, true, rs);
+    Pk1 = load_prim<STAGE, GRAV, CG, TAB, ANG>(a, g, gx, gy, z0 + 1, flags, nsrc, dth, true, rs);
     FaceState mm, pm, m0;
     if (z0 - 1 < g.az0) {
       ghost_states(Pm1, mm, pm);
     } else {
-      dir_states<POW2, TAB>(Pm2, Pm1, Pk, Pm1.u3, dt, g.dz, idz, mm, pm);
+      dir_states<POW2, TAB, ANG>(Pm2, Pm1, Pk, Pm1.u3, dt, g.dz, idz, mm, pm);
     }
     FaceState plusk;
     double Fzm[5];
-    dir_states<POW2, TAB>(Pm1, Pk, Pk1, Pk.u3, dt, g.dz, idz, m0, plusk);
-    hll_flux<2, TAB>(pm, m0, g.gam, Fzm);
+    dir_states<POW2, TAB, ANG>(Pm1, Pk, Pk1, Pk.u3, dt, g.dz, idz, m0, plusk);
+    if (ANG) {
+      double F7[7];
+      hll_flux_ang<2>(pm, m0, g.gam, 0.0, 0.0, 1.0, 0.0, 0.0, 1.0, F7);
+      for (int q = 0; q < 5; ++q) Fzm[q] = F7[q];
+    } else {
+      hll_flux<2, TAB>(pm, m0, g.gam, Fzm);
+    }
     for (int q = 0; q < 5; ++q) zs(q) = Fzm[q];
     zs(10) = plusk.d; zs(11) = plusk.u1; zs(12) = plusk.u2; zs(13) = plusk.u3;
     zs(14) = plusk.p; zs(15) = plusk.e;
     if (TAB) zs(16) = plusk.g;
+    if (ANG) { zs(16) = plusk.rm; zs(17) = plusk.am; }
   }
 
   for (int z = (THREED ? z0 : g.az0 + t.z0); z < (THREED ? z1 : g.az0 + t.z1); ++z) {
@@ -560,9 +612,9 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
     FaceState mz1, pz1;
     if (own) {
       if (THREED) {
-        P2 = load_prim<STAGE, GRAV, CG, TAB>(a, g, gx, gy, z + 2, flags, nsrc, dth, true, rs);
+        P2 = load_prim<STAGE, GRAV, CG, TAB, ANG>(a, g, gx, gy, z + 2, flags, nsrc, dth, true, rs);
       } else {
-        Pk = load_prim<STAGE, GRAV, CG, TAB>(a, g, gx, gy, z, flags, nsrc, dth, true, rs);
+        Pk = load_prim<STAGE, GRAV, CG, TAB, ANG>(a, g, gx, gy, z, flags, nsrc, dth, true, rs);
       }
       put_prim<NP, NPF>(SP, (ty + 2) * PW + (tx + 2), Pk);
       if (is0) {
@@ -593,23 +645,31 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
       const int fx = bx0 + cx, fy = by0 + cy;
       const bool near = cx >= -1 && cx <= w && cy >= -1 && cy <= h;
       const bool inner = fx >= g.ax0 && fx < g.ax1 && fy >= g.ay0 && fy < g.ay1;
-      const Prim q = load_prim<STAGE, GRAV, CG, TAB>(a, g, fx, fy, z, flags, nsrc, dth, near && inner, rs);
+      const Prim q = load_prim<STAGE, GRAV, CG, TAB, ANG>(a, g, fx, fy, z, flags, nsrc, dth, near && inner, rs);
       put_prim<NP, NPF>(SP, (cy + 2) * PW + (cx + 2), q);
     }
     if (THREED && own) {
       if (z + 1 >= g.az1) {
         ghost_states(Pk1, mz1, pz1);
       } else {
-        dir_states<POW2, TAB>(Pk, Pk1, P2, Pk1.u3, dt, g.dz, idz, mz1, pz1);
+        dir_states<POW2, TAB, ANG>(Pk, Pk1, P2, Pk1.u3, dt, g.dz, idz, mz1, pz1);
       }
       const FaceState plusk{zs(10), zs(11), zs(12), zs(13), zs(14), zs(15),
-                            TAB ? zs(16) : 0.0};
+                            TAB ? zs(16) : 0.0,
+                            ANG ? zs(16) : 0.0, ANG ? zs(17) : 0.0};
       double Fzp[5];
-      hll_flux<2, TAB>(plusk, mz1, g.gam, Fzp);
+      if (ANG) {
+        double F7[7];
+        hll_flux_ang<2>(plusk, mz1, g.gam, 0.0, 0.0, 1.0, 0.0, 0.0, 1.0, F7);
+        for (int q = 0; q < 5; ++q) Fzp[q] = F7[q];
+      } else {
+        hll_flux<2, TAB>(plusk, mz1, g.gam, Fzp);
+      }
       for (int q = 0; q < 5; ++q) zs(5 + q) = Fzp[q];
       zs(10) = pz1.d; zs(11) = pz1.u1; zs(12) = pz1.u2; zs(13) = pz1.u3;
       zs(14) = pz1.p; zs(15) = pz1.e;
       if (TAB) zs(16) = pz1.g;
+      if (ANG) { zs(16) = pz1.rm; zs(17) = pz1.am; }
     }
     __syncthreads();
 
@@ -628,7 +688,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         if (fx < g.ax0 || fx >= g.ax1) {
           ghost_states(q, mi, pl);
         } else {
-          dir_states<POW2, TAB>(get_prim<NP, NPF>(SP, c - 1), q, get_prim<NP, NPF>(SP, c + 1), q.u1, dt, g.dx, g.idx, mi,
+          dir_states<POW2, TAB, ANG>(get_prim<NP, NPF>(SP, c - 1), q, get_prim<NP, NPF>(SP, c + 1), q.u1, dt, g.dx, g.idx, mi,
                            pl);
         }
         const int o = cy * (TX + 2) + (cx + 1);
@@ -643,7 +703,7 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         if (fy < g.ay0 || fy >= g.ay1) {
           ghost_states(q, mi, pl);
         } else {
-          dir_states<POW2, TAB>(get_prim<NP, NPF>(SP, c - PW), q, get_prim<NP, NPF>(SP, c + PW), q.u2, dt, g.dy, g.idy,
+          dir_states<POW2, TAB, ANG>(get_prim<NP, NPF>(SP, c - PW), q, get_prim<NP, NPF>(SP, c + PW), q.u2, dt, g.dy, g.idy,
                            mi, pl);
         }
         const int o = (cy + 1) * TX + cx;
@@ -657,26 +717,41 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
     // faces start at a warp boundary as in B
     const int nxf_w = (nxf + 31) & ~31;
     for (int i = tid; i < nxf_w + nyf; i += NT) {
-      double F[5];
+      double F[NFQ];
       if (i < nxf_w) {
         if (i >= nxf) continue;
         const int cy = i / (w + 1), f = i % (w + 1);
         const int base = cy * (TX + 2);
         const FaceState L = get_fs<NSF>(SX + NSF * NSX, NSX, base + f);  // plus state of cell f-1
         const FaceState R = get_fs<NSF>(SX, NSX, base + f + 1);        // minus state of cell f
-        hll_flux<0, TAB>(L, R, g.gam, F);
+        if constexpr (ANG) {
+          // the momentum fluxes for both cells of the face (their own centres)
+          double xl, yl, rl, xh, yh, rh;
+          cell_xyr(g, bx0 + f - 1, by0 + cy, xl, yl, rl);
+          cell_xyr(g, bx0 + f, by0 + cy, xh, yh, rh);
+          hll_flux_ang<0>(L, R, g.gam, xl, yl, rl, xh, yh, rh, F);
+        } else {
+          hll_flux<0, TAB>(L, R, g.gam, F);
+        }
         const int o = cy * (TX + 1) + f;
 #pragma unroll
-        for (int q = 0; q < 5; ++q) FX[q * NFX + o] = F[q];
+        for (int q = 0; q < NFQ; ++q) FX[q * NFX + o] = F[q];
       } else {
         const int k = i - nxf_w;
         const int f = k / w, cx = k % w;
         const FaceState L = get_fs<NSF>(SY + NSF * NSY, NSY, f * TX + cx);
         const FaceState R = get_fs<NSF>(SY, NSY, (f + 1) * TX + cx);
-        hll_flux<1, TAB>(L, R, g.gam, F);
+        if constexpr (ANG) {
+          double xl, yl, rl, xh, yh, rh;
+          cell_xyr(g, bx0 + cx, by0 + f - 1, xl, yl, rl);
+          cell_xyr(g, bx0 + cx, by0 + f, xh, yh, rh);
+          hll_flux_ang<1>(L, R, g.gam, xl, yl, rl, xh, yh, rh, F);
+        } else {
+          hll_flux<1, TAB>(L, R, g.gam, F);
+        }
         const int o = f * TX + cx;
 #pragma unroll
-        for (int q = 0; q < 5; ++q) FY[q * NFY + o] = F[q];
+        for (int q = 0; q < NFQ; ++q) FY[q * NFY + o] = F[q];
       }
     }
     __syncthreads();
@@ -686,8 +761,11 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
       double ft[5];
 #pragma unroll
       for (int q = 0; q < 5; ++q) {
-        const double dfx = FX[q * NFX + ty * (TX + 1) + tx + 1] - FX[q * NFX + ty * (TX + 1) + tx];
-        const double dfy = FY[q * NFY + (ty + 1) * TX + tx] - FY[q * NFY + ty * TX + tx];
+        // with flux_ang the momentum fluxes of this cell's plus faces are the
+        // versions for their low cell (planes 5, 6)
+        const int qp = (ANG && (q == 1 || q == 2)) ? q + 4 : q;
+        const double dfx = FX[qp * NFX + ty * (TX + 1) + tx + 1] - FX[q * NFX + ty * (TX + 1) + tx];
+        const double dfy = FY[qp * NFY + (ty + 1) * TX + tx] - FY[q * NFY + ty * TX + tx];
         double sum = g.ayz * dfx + g.axz * dfy;
         if (THREED) sum = sum + g.axy * (zs(5 + q) - zs(q));
         ft[q] = POW2 ? -sum * dt * g.ivol : cdiv(-sum * dt, g.vol, g.ivol);
@@ -705,6 +783,8 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
           c0.E = source_energy_q(q0, c0.m1, c0.m2, c0.m3, c0.E, g.small_eps);
       }
       double n[5];
+      // flux_ang updates the transformed momenta (flux_ang.f90:44-62, 149-246)
+      if (ANG) ang_to(g, gx, gy, c0.m1, c0.m2, c0.m1, c0.m2);
       if (is0) {
         n[0] = c0.d + ft[0];
         n[1] = c0.m1 + ft[1];
@@ -712,12 +792,22 @@ __device__ __forceinline__ void stage_tile(const StageArgs& a, const Tile& t, co
         n[3] = c0.m3 + ft[3];
         n[4] = c0.E + ft[4];
       } else {
-        const Cons c1 = load_cons<CG>(a.Y, PS, g, gx, gy, z);
+        Cons c1 = load_cons<CG>(a.Y, PS, g, gx, gy, z);
+        if (ANG) ang_to(g, gx, gy, c1.m1, c1.m2, c1.m1, c1.m2);
         n[0] = kHalf * (c0.d + c1.d + ft[0]);
         n[1] = kHalf * (c0.m1 + c1.m1 + ft[1]);
         n[2] = kHalf * (c0.m2 + c1.m2 + ft[2]);
         n[3] = kHalf * (c0.m3 + c1.m3 + ft[3]);
         n[4] = kHalf * (c0.E + c1.E + ft[4]);
+      }
+      if (ANG) {
+        // back to (m1, m2) (flux_ang.f90:247-270)
+        double cxp, cyp, crp;
+        cell_xyr(g, gx, gy, cxp, cyp, crp);
+        const double tyy = cyp + g.yoff, trr = sqrt(cxp * cxp + tyy * tyy);
+        const double rmom = n[1], angmom = n[2];
+        n[1] = (rmom * cxp - angmom * tyy / trr) / trr;
+        n[2] = (rmom * tyy + angmom * cxp / trr) / trr;
       }
       floors(n[0], n[1], n[2], n[3], n[4], g.small_rho, g.small_eps);
       if (!(isfinite(n[0]) && isfinite(n[1]) && isfinite(n[2]) && isfinite(n[3]) &&
@@ -812,11 +902,15 @@ template <>
 struct ShapeSel<2> {
   using type = Shape2;
 };
+template <>
+struct ShapeSel<3> {
+  using type = Shape3;
+};
 
 // PM: 1 = every box of the launch has power-of-two spacings (divisions by the
 // cell sizes are multiplications by exact reciprocals), 0 = otherwise (cdiv,
 // exact for any spacing).  SH: the tile shape (Shape0 or Shape1; Shape2 with the
-// tabulated EOS).
+// tabulated EOS, Shape3 with angular-momentum fluxing).
 template <int STAGE, int PM, bool THREED, bool GRAV = false, int SH = 0>
 __global__ void __launch_bounds__(NT, 65536 / (NT * 128)) k_stage(StageArgs a) {
   using S = typename ShapeSel<SH>::type;
@@ -1097,8 +1191,8 @@ static cudaError_t launch_stage_g(int pm, bool threed, const StageArgs& a, int n
 
 // a.G set: the step has a gravitational force (instances with the force terms,
 // tile shape 0 only: the batched path, the one that tunes the shape, has no
-// force, and a grid with the tabulated EOS and a force runs the per-phase
-// kernels).  Shape 2: the tabulated EOS.
+// force, and a grid with the tabulated EOS or flux_ang and a force runs the
+// per-phase kernels).  Shape 2: the tabulated EOS; shape 3: flux_ang.
 template <int STAGE>
 static cudaError_t launch_stage_s(int pm, bool threed, const StageArgs& a, int ntiles,
                                   cudaStream_t s, int shape) {
@@ -1107,6 +1201,7 @@ static cudaError_t launch_stage_s(int pm, bool threed, const StageArgs& a, int n
     return launch_stage_g<STAGE, true, 0>(pm, threed, a, ntiles, s);
   }
   if (shape == 2) return launch_stage_g<STAGE, false, 2>(pm, threed, a, ntiles, s);
+  if (shape == 3) return launch_stage_g<STAGE, false, 3>(pm, threed, a, ntiles, s);
   return shape == 1 ? launch_stage_g<STAGE, false, 1>(pm, threed, a, ntiles, s)
                     : launch_stage_g<STAGE, false, 0>(pm, threed, a, ntiles, s);
 }
@@ -1119,7 +1214,8 @@ cudaError_t launch_stage(int stage, int pm, bool threed, const StageArgs& a, int
 }
 
 size_t stage_smem_bytes(int shape) {
-  return (shape == 2   ? Shape2::SMEM_DOUBLES
+  return (shape == 3   ? Shape3::SMEM_DOUBLES
+          : shape == 2 ? Shape2::SMEM_DOUBLES
           : shape == 1 ? Shape1::SMEM_DOUBLES
                        : Shape0::SMEM_DOUBLES) *
          sizeof(double);
@@ -2043,7 +2139,18 @@ int stage_blocks_per_sm(int stage, int pm, bool threed, int shape) {
   int nb = 0;
   const size_t smem = stage_smem_bytes(shape);
   const void* fn;
-  if (shape == 2) {
+  if (shape == 3) {
+    if (stage == 0)
+      fn = pm == 1 ? (threed ? (const void*)k_stage<0, 1, true, false, 3>
+                             : (const void*)k_stage<0, 1, false, false, 3>)
+                   : (threed ? (const void*)k_stage<0, 0, true, false, 3>
+                             : (const void*)k_stage<0, 0, false, false, 3>);
+    else
+      fn = pm == 1 ? (threed ? (const void*)k_stage<1, 1, true, false, 3>
+                             : (const void*)k_stage<1, 1, false, false, 3>)
+                   : (threed ? (const void*)k_stage<1, 0, true, false, 3>
+                             : (const void*)k_stage<1, 0, false, false, 3>);
+  } else if (shape == 2) {
     if (stage == 0)
       fn = pm == 1 ? (threed ? (const void*)k_stage<0, 1, true, false, 2>
                              : (const void*)k_stage<0, 1, false, false, 2>)

@@ -18,15 +18,16 @@ constexpr double kLowRho = 1e-4;   // low-density EOS branch, state.f90:52
 
 // Primitive set used by reconstruction: rho, u1..3, p, eps (internal energy
 // per volume), plus the sound speed c = sqrt(p*gamma/rho) of the cell and, with
-// the tabulated EOS, the cell's gamma (adindx), reconstructed like the others.
+// the tabulated EOS, the cell's gamma (adindx), with angular-momentum fluxing
+// the radial and angular momenta (rm, am), reconstructed like the others.
 struct Prim {
-  double d, u1, u2, u3, p, e, c, g;
+  double d, u1, u2, u3, p, e, c, g, rm, am;
 };
 
 // Reconstructed face state (one side of one face); g: gamma, with the
-// tabulated EOS only (fixed gamma: the grid's).
+// tabulated EOS only (fixed gamma: the grid's); rm, am: with flux_ang only.
 struct FaceState {
-  double d, u1, u2, u3, p, e, g;
+  double d, u1, u2, u3, p, e, g, rm, am;
 };
 
 // genminmod (utils.f90:696-707) of (theta*d1, half*d2, theta*d3) where
@@ -145,10 +146,11 @@ __device__ __forceinline__ double courant_rate_q(const struct SharedDiv& qd, dou
 // lambda_p = max(u_d+c,0)*dt/ds, lambda_m = min(u_d-c,0)*dt/ds,
 // q- = q + half*(-1-lambda_m)*s, q+ = q + half*(1-lambda_p)*s.
 // The transverse terms of flux.f90:391-479 add zero and are omitted.
-template <bool POW2, bool TAB = false>
+template <bool POW2, bool TAB = false, bool ANG = false>
 BX_HD void muscl_states(const Prim& q, double ud, double sd, double su1, double su2,
                         double su3, double sp, double se, double dt, double ds, double ids,
-                        FaceState& mi, FaceState& pl, double sg = 0.0) {
+                        FaceState& mi, FaceState& pl, double sg = 0.0, double srm = 0.0,
+                        double sam = 0.0) {
   double lp = fmax(ud + q.c, 0.0) * dt;
   double lm = fmin(ud - q.c, 0.0) * dt;
   if (POW2) {
@@ -176,12 +178,20 @@ BX_HD void muscl_states(const Prim& q, double ud, double sd, double su1, double 
     mi.g = q.g + hm * sg;
     pl.g = q.g + hp * sg;
   }
+  if (ANG) {
+    // flux_ang.f90:349-518: the transformed momenta, without transverse terms
+    mi.rm = q.rm + hm * srm;
+    pl.rm = q.rm + hp * srm;
+    mi.am = q.am + hm * sam;
+    pl.am = q.am + hp * sam;
+  }
 }
 
 // Face state of a ghost cell: its slopes are zero (flux.f90:53-54), so both
 // sides equal the cell values.
 BX_HD void ghost_states(const Prim& q, FaceState& mi, FaceState& pl) {
   mi.d = q.d; mi.u1 = q.u1; mi.u2 = q.u2; mi.u3 = q.u3; mi.p = q.p; mi.e = q.e; mi.g = q.g;
+  mi.rm = q.rm; mi.am = q.am;
   pl = mi;
 }
 
@@ -324,6 +334,69 @@ BX_HD void hll_flux(const FaceState& L, const FaceState& R, double gam, double F
 #else
   for (int i = 0; i < 5; ++i) F[i] = F[i] / den;
 #endif
+}
+
+// HLL flux with angular-momentum fluxing (flux_ang.f90:523-618, gl = gr =
+// gamma): components 1 and 2 are the radial and angular momenta, whose x and y
+// face fluxes carry pressure terms at the centre of the cell being updated
+// (x, y without yoffset, r = sqrt(x^2 + y^2), flux_ang.f90:571-573).  For
+// DIR 0 and 1, F[1], F[2] are those of the high cell (xh, yh, rh: the face is
+// its minus face) and F[5], F[6] of the low cell (xl, yl, rl); z faces have no
+// such terms (F[5], F[6] unset).
+template <int DIR>
+__device__ __forceinline__ void hll_flux_ang(const FaceState& L, const FaceState& R, double gam,
+                                             double xl, double yl, double rl, double xh,
+                                             double yh, double rh, double F[7]) {
+  const double vl = DIR == 0 ? L.u1 : (DIR == 1 ? L.u2 : L.u3);
+  const double vr = DIR == 0 ? R.u1 : (DIR == 1 ? R.u2 : R.u3);
+  const double cr = sqrt(gam * R.p / R.d);
+  const double cl = sqrt(gam * L.p / L.d);
+  const double ap = fmax(fmax(0.0, vr + cr), vl + cl);
+  const double am = fmax(fmax(0.0, -(vr - cr)), -(vl - cl));
+  const double apam = ap * am;
+  const double den = ap + am;
+  auto num = [&](double sl, double sr, double fl, double fr) {
+    return ap * fl + am * fr - apam * (sr - sl);
+  };
+  // mass
+  F[0] = num(L.d, R.d, L.d * vl, R.d * vr);
+  // momentum 3: the pressure on the z faces only
+  {
+    const double sl = L.d * L.u3, sr = R.d * R.u3;
+    F[3] = num(sl, sr, (DIR == 2 ? L.p : 0.0) + sl * vl, (DIR == 2 ? R.p : 0.0) + sr * vr);
+  }
+  // energy
+  {
+    const double sl = L.e + kHalf * L.d * (L.u1 * L.u1 + L.u2 * L.u2 + L.u3 * L.u3);
+    const double sr = R.e + kHalf * R.d * (R.u1 * R.u1 + R.u2 * R.u2 + R.u3 * R.u3);
+    F[4] = num(sl, sr, (sl + L.p) * vl, (sr + R.p) * vr);
+  }
+  // radial and angular momenta, with the pressure terms of the updated cell
+  auto mom = [&](double x, double y, double r, double& f1, double& f2) {
+    double al = 0.0, ar = 0.0, bl = 0.0, br = 0.0;
+    if (DIR == 0) {
+      al = L.p * x / r; ar = R.p * x / r;
+      bl = -(L.p * y); br = -(R.p * y);
+    } else if (DIR == 1) {
+      al = L.p * y / r; ar = R.p * y / r;
+      bl = L.p * x; br = R.p * x;
+    }
+    f1 = num(L.rm, R.rm, al + L.rm * vl, ar + R.rm * vr);
+    f2 = num(L.am, R.am, bl + L.am * vl, br + R.am * vr);
+  };
+  mom(xh, yh, rh, F[1], F[2]);
+  constexpr int NQ = DIR == 2 ? 5 : 7;
+  if (DIR != 2) mom(xl, yl, rl, F[5], F[6]);
+  bool fast = den >= 0x1p-450 && den <= 0x1p+450;
+#pragma unroll
+  for (int i = 0; i < NQ; ++i) fast = fast && quot_fast_ok(F[i]);
+  if (fast) {
+    const double r = __drcp_rn(den);
+#pragma unroll
+    for (int i = 0; i < NQ; ++i) F[i] = quot_fast(F[i], den, r);
+  } else {
+    for (int i = 0; i < NQ; ++i) F[i] = div_ieee(F[i], den);
+  }
 }
 
 // floors after the conservative update (flux.f90:223-230)

@@ -1,6 +1,7 @@
 """Angular-momentum fluxing (fluxangmom=.true., flux_ang.f90) on the per-phase
-kernels against the oracle's restatement: whole steps and single flux calls,
-with and without yoffset, outflow and reflective walls."""
+kernels and on the fused stage kernels against the oracle's restatement: whole
+steps and single flux calls, with and without yoffset, outflow and reflective
+walls, a force switched on and off."""
 import dataclasses
 
 import numpy as np
@@ -21,10 +22,55 @@ def ang_box(dims, walls, yoffset, seed):
                                                 ((16, 10, 8), (1,) * 6, 0.3),
                                                 ((18, 12, 4), (1, 0, 0, 1, 0, 0), -0.45)])
 def test_flux_ang_steps(dims, walls, yoffset):
+    """Steps bit-identical to the oracle; after the first step (per-phase, from
+    the upload) the grids the fused kernels take run them with the transformed
+    momenta (tile shape 3), the reflective 3-D box stays on the per-phase
+    kernels."""
     st = ang_box(dims, walls, yoffset, seed=5)
     o, g = make_pair(st)
     step_both(o, g, 4)
-    assert g.status()[1] == 0  # flux_ang runs on the per-phase kernels
+    reflective_3d = dims[2] >= 6 and any(walls[4:])
+    assert g.status()[1] == (0 if reflective_3d else 1)
+    o.close()
+    g.close()
+
+
+def test_flux_ang_turbulent_box_runs_fused():
+    """The turbulent box with the rotation axis below the box (yoffset 0.75):
+    every step on the fused kernels with no guard fired, bit-identical to the
+    oracle."""
+    from boxzyhydro_b200 import ic
+    st = ic.turbulent_box(n=40, seed=3)
+    st.params = dataclasses.replace(st.params, fluxangmom=True, yoffset=0.75)
+    o, g = make_pair(st)
+    step_both(o, g, 1)
+    g.status()
+    step_both(o, g, 4)
+    assert g.status() == (0, 1)
+    o.close()
+    g.close()
+
+
+def test_flux_ang_fused_with_a_force_leaves_and_returns():
+    """A force moves a flux_ang grid to the per-phase kernels (the force
+    instances have the fixed-gamma, fixed-frame tile shape); clearing it lets
+    the next clean step return to the fused kernels, bit-identical throughout."""
+    from boxzyhydro_b200 import grid as G
+    st = ang_box((20, 18, 14), (0,) * 6, 0.25, seed=9)
+    o, g = make_pair(st)
+    step_both(o, g, 2)
+    assert g.status()[1] == 1
+    hp = st.params
+    x, y, z = G.cell_centres(hp.nx, hp.ny, hp.nz, hp.dx, hp.dy, hp.dz)
+    phi = -0.05 / np.sqrt(x * x + y * y + z * z + 0.01)
+    g.set_phi(phi)
+    o.set_gforce(o.calc_gforce(phi))
+    step_both(o, g, 2)
+    assert g.status()[1] == 0
+    g.set_phi(None)
+    o.set_gforce(None)
+    step_both(o, g, 3)
+    assert g.status()[1] == 1
     o.close()
     g.close()
 
