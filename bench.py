@@ -1000,7 +1000,7 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu and args.parity_steps > 0:
         parity = parity_full_size(st, args.parity_steps)
 
-    # ---- the other two BASELINE figures at their configurations (one GPU):
+    # ---- the other two headline figures at their configurations (one GPU):
     # the adjoint/forward time ratio (C4: 128^3, 200 steps, 15 snapshots) and
     # the batched ensemble's boxes/s against the looped plain path (C3: 4096 boxes)
     adjoint_c4 = batched_c3 = None

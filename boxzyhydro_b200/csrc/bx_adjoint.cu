@@ -290,14 +290,19 @@ k_rdir(Geom g, const double* P, const double* lamL, double lscale, double dt, do
   const long long st = DIR == 0 ? 1 : DIR == 1 ? g.sy : g.sz;
   const long long nlines = DIR == 0 ? (long long)nyi * nzi : DIR == 1 ? (long long)nxi * nzi
                                                                        : (long long)nxi * nyi;
-  const int s0 = lo - 1 + (int)blockIdx.y * W;
+  // the segments of a line group are consecutive blocks, so the cells that
+  // neighbouring segments both load (their halos) are read while the other
+  // segment's block still has them in L2
+  const int seg = (int)(blockIdx.x % (unsigned)sh.nseg);
+  const long long grp = (long long)(blockIdx.x / (unsigned)sh.nseg);
+  const int s0 = lo - 1 + seg * W;
   const double ds = DIR == 0 ? g.dx : DIR == 1 ? g.dy : g.dz;
   const double ids = DIR == 0 ? g.idx : DIR == 1 ? g.idy : g.idz;
   const double area = DIR == 0 ? g.ayz : DIR == 1 ? g.axz : g.axy;
   const double coef = -(dt / g.vol) * area;
   const double rr = dt / ds;
   auto line_base = [&](int l, bool& ok) -> long long {
-    const long long L = (long long)blockIdx.x * NL + l;
+    const long long L = grp * NL + l;
     ok = L < nlines;
     if (!ok) return 0;
     if (DIR == 0) return (g.ay0 + L % nyi) * g.sy + (zlo + L / nyi) * g.sz;
@@ -1169,7 +1174,8 @@ static cudaError_t launch_rdir(const Geom& g, const double* P, const double* lam
   const RShape sh = DIR == 0 ? rshape(hi - lo + 2, 60, 128) : rshape(hi - lo + 2, 28, 256);
   cudaError_t e = ensure_dyn_smem((const void*)k_rdir<DIR, POW2>, sh.smem);
   if (e != cudaSuccess) return e;
-  dim3 grid((unsigned)((nlines + sh.NL - 1) / sh.NL), (unsigned)sh.nseg);
+  const long long ngrp = (nlines + sh.NL - 1) / sh.NL;
+  const dim3 grid((unsigned)(ngrp * sh.nseg));
   k_rdir<DIR, POW2><<<grid, sh.threads, sh.smem, s>>>(g, P, lamL, lscale, dt, PA, sh);
   return cudaGetLastError();
 }
