@@ -587,7 +587,8 @@ def adjoint_measure(args, local):
     m = torch.tensor(G.boundary_flags(hp.nx, hp.ny, hp.nz) == 0, device=dev)
     c0 = torch.tensor(np.ascontiguousarray(st.cons.T), device=dev)
     del st
-    snaps = args.snapshots
+    # the automatic host level sizes the device snapshots too
+    snaps = 0 if args.host_stride < 0 else args.snapshots
     # stage-0 cache entries: 8 beside a given snapshot count; when the snapshots
     # fill HBM, about a third of the free state sets (a schedule simulation of
     # 400 steps in 17 sets: 11 snapshots + 6 entries recompute least)
@@ -775,7 +776,8 @@ def main():
     ap.add_argument("--stage0-cache", type=int, default=0, dest="stage0_cache")
     ap.add_argument("--host-stride", type=int, default=0, dest="host_stride",
                     help="adjoint: every stride-th state in pinned host memory (0: off; "
-                         "-1 with --snapshots 0: chosen from the free device and host memory)")
+                         "-1: the stride and the device snapshots chosen from the free "
+                         "device and host memory)")
     ap.add_argument("--nbox", type=int, default=4096)
     ap.add_argument("--check-boxes", type=int, default=16, dest="check_boxes")
     ap.add_argument("--no-autotune", action="store_true", dest="no_autotune")
