@@ -17,11 +17,13 @@
  *    arrays directly (assumed-size dummies of a bind(c) interface).
  *  - Calls on one handle are single-threaded (outside OpenMP parallel regions or
  *    under !$OMP MASTER).  Each handle owns one CUDA stream unless one is given.
- *  - Grids with the fixed-gamma EOS (H2STAT=-1) and Cartesian fluxing step on
- *    the fused stage kernels, with or without a gravitational force
- *    (bx_set_gforce, bx_set_phi); the tabulated EOS (H2STAT>=0,
- *    bx_set_eos_table) and angular-momentum fluxing (fluxangmom=1) step on the
- *    per-phase kernels, with the same results as the reference's subroutines.
+ *  - Steps run on the fused stage kernels: the fixed-gamma EOS (H2STAT=-1)
+ *    with or without a gravitational force (bx_set_gforce, bx_set_phi), and,
+ *    without a force, the tabulated EOS (H2STAT>=0 with nz != 1,
+ *    bx_set_eos_table) and angular-momentum fluxing (fluxangmom=1).  The other
+ *    combinations, grids whose ghost rule the fused kernels do not take, and
+ *    steps in which the velocity limiter or the low-density branch fires run on
+ *    the per-phase kernels.  Both give the reference's results bit for bit.
  */
 #ifndef BOXZY_GPU_H
 #define BOXZY_GPU_H
@@ -63,7 +65,7 @@ typedef struct bx_params {
   double rgas;            /* scale%rgas of get_units, units.f90:17 */
   int32_t no_outflow[6];  /* grid_params no_outflow_xl,xr,yl,yr,zl,zr (reflective walls) */
   int32_t fluxangmom;     /* grid_params fluxangmom: 1 = flux_ang.f90 in place of flux.f90
-                             (angular-momentum fluxing, per-phase kernels) */
+                             (angular-momentum fluxing) */
   int32_t flags;          /* BX_FLAG_* */
   double yoffset;         /* grid_params yoffset (flux_ang.f90:46,251) */
 } bx_params;
@@ -123,8 +125,8 @@ int bx_step(bx_handle *h, double endtime, int32_t *ran);
  * the (5, ngrid) layout and copied back.  cons_in and cons_out may be the same
  * array; pinned (page-locked) host memory lets the copies run asynchronously.
  * A force set with bx_set_phi or bx_set_gforce applies to the step.  States the
- * fused path does not take (see bx_upload_conserved; tabulated EOS) run the
- * three calls in sequence.  Uses the handle's reference cons array as
+ * fused path does not take (see bx_upload_conserved), and the tabulated EOS and
+ * angular-momentum fluxing, run the three calls in sequence.  Uses the handle's reference cons array as
  * staging; returns after the result is in cons_out. */
 int bx_step_host(bx_handle *h, const double *cons_in, double *cons_out, double endtime,
                  int32_t *ran);
@@ -154,7 +156,8 @@ int bx_read_celldump(bx_handle *h, const char *path, double *phi, double *time, 
  * (eos.f90:30-51), in Fortran order (energy index fastest).  state() then takes
  * gamma, mu and T from them by get_gamma2 (eos.f90:653-699) as state.f90:60-79
  * does (including the disk scale-height branch for nz == 1).  Such grids run the
- * per-phase kernels; bx_set_eos_table must come before the first step. */
+ * fused stage kernels (nz != 1, no force) or the per-phase kernels;
+ * bx_set_eos_table must come before the first step. */
 typedef struct bx_eos_table {
   int32_t neos;            /* NEOS = NEOS_T: entries per density (eng_table2 rows) */
   int32_t neos_rho;        /* NEOS_RHO */
